@@ -1,0 +1,116 @@
+"""Synthetic zincblende structures with the shapes of the benchmark configurations.
+
+A structure is a dense grid of conventional cubic cells (cell (i,j,k) row-major,
+k fastest -- the order in which ``geo_struct::FillFirstShape``
+(base/ham3d.c:745-900) enumerates cells) with eight sites per cell (sites 0..3
+cations, 4..7 anions, positions from ``Cell::Initialize``, base/Cell.c:185-210).
+Each site holds a species id (``materials.SPECIES``, 0 = empty) and optionally
+a displacement in nm, the seam through which the reference receives strain
+(``geo_struct::l_m_2_atomdsp``, base/geo_struct.c:2224-2297).
+
+These generators stand in for the reference's XML shape decks and its Keating
+strain solver, which are out of scope; they are inputs, not parity targets.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .materials import SPECIES
+
+# in-cell site positions in units of the lattice constant (Cell.c:185-210)
+SITE_POS = np.array([
+    [0, 0, 0], [0, -0.5, -0.5], [-0.5, -0.5, 0], [-0.5, 0, -0.5],
+    [-0.25, -0.25, -0.25], [-0.25, -0.75, -0.75], [-0.75, -0.75, -0.25],
+    [-0.75, -0.25, -0.75]], dtype=np.float64)
+
+A_GAAS = 0.56532  # GaAs lattice constant of the shipped parameter set (nm)
+
+
+@dataclass
+class Structure:
+    nx: int
+    ny: int
+    nz: int
+    lattice: tuple = (A_GAAS, A_GAAS, A_GAAS)
+    periodic: tuple = (False, False, False)
+    types: np.ndarray = None          # uint8 [nx, ny, nz, 8]
+    dsp: np.ndarray | None = None     # float64 [nx, ny, nz, 8, 3] (nm) or None
+    name: str = ""
+    info: dict = field(default_factory=dict)
+
+    @property
+    def nsites(self) -> int:
+        return self.nx * self.ny * self.nz * 8
+
+    def site_positions(self) -> np.ndarray:
+        """Unstrained site positions (nm), shape [nx, ny, nz, 8, 3]."""
+        ijk = np.stack(np.meshgrid(np.arange(self.nx), np.arange(self.ny),
+                                   np.arange(self.nz), indexing="ij"), -1)
+        pos = ijk[:, :, :, None, :] + SITE_POS[None, None, None]
+        return pos * np.asarray(self.lattice)
+
+
+def _binary(nx, ny, nz, cation="Ga", anion="As"):
+    t = np.zeros((nx, ny, nz, 8), dtype=np.uint8)
+    t[..., :4] = SPECIES[cation]
+    t[..., 4:] = SPECIES[anion]
+    return t
+
+
+def bulk_cell(cation="Ga", anion="As", a=A_GAAS) -> Structure:
+    """One periodic conventional cell (the reference's bulk decks)."""
+    return Structure(1, 1, 1, (a, a, a), (True, True, True),
+                     _binary(1, 1, 1, cation, anion), None, f"{cation}{anion}_bulk")
+
+
+def gaas_cube(n: int = 8, a: float = A_GAAS) -> Structure:
+    """Closed GaAs cube of n x n x n conventional cells (4096 atoms for n=8)."""
+    return Structure(n, n, n, (a, a, a), (False, False, False),
+                     _binary(n, n, n), None, f"GaAs_cube_{n}")
+
+
+def dome_in_box(cells=(58, 58, 38), base_nm: float = 20.0, height_nm: float = 5.0,
+                wl_z_nm: float | None = None, sigma_frac: float = 0.005,
+                seed: int = 1, a: float = A_GAAS) -> Structure:
+    """InAs lens (dome) on a one-monolayer InAs wetting layer in a GaAs box.
+
+    The dome is the half-ellipsoid of ``isNotInDome`` (base/ham3d.c:233-256):
+    centred in x,y on the wetting layer, semi-axes base/2, base/2, height.
+    Displacements are i.i.d. Gaussian per component with sigma equal to
+    ``sigma_frac`` times the ideal GaAs bond length, drawn from ``seed``
+    (a stand-in for the Keating strain field).
+    """
+    nx, ny, nz = cells
+    t = _binary(nx, ny, nz)
+    st = Structure(nx, ny, nz, (a, a, a), (False, False, False), t, None,
+                   f"InAs_dome_{nx}x{ny}x{nz}")
+    pos = st.site_positions()
+    lx, ly, lz = nx * a, ny * a, nz * a
+    z0 = wl_z_nm if wl_z_nm is not None else 0.3 * lz
+    cx, cy = 0.5 * lx - 0.5 * a, 0.5 * ly - 0.5 * a
+    cat = pos[..., :4, :]
+    # wetting layer: the cation plane(s) within one monolayer (a/2) below z0
+    wl = (cat[..., 2] >= z0 - 0.5 * a) & (cat[..., 2] < z0)
+    rb, h = 0.5 * base_nm, height_nm
+    dome = (cat[..., 2] >= z0) & (((cat[..., 0] - cx) / rb) ** 2 +
+                                  ((cat[..., 1] - cy) / rb) ** 2 +
+                                  ((cat[..., 2] - z0) / h) ** 2 <= 1.0)
+    sub = t[..., :4]
+    sub[wl | dome] = SPECIES["In"]
+    if sigma_frac > 0:
+        rng = np.random.default_rng(seed)
+        sigma = sigma_frac * np.sqrt(3.0) / 4.0 * a
+        st.dsp = rng.normal(0.0, sigma, size=(nx, ny, nz, 8, 3))
+    st.info = dict(base_nm=base_nm, height_nm=height_nm, wl_z_nm=z0,
+                   sigma_nm=sigma_frac * np.sqrt(3.0) / 4.0 * a, seed=seed,
+                   n_in=int((sub == SPECIES["In"]).sum()))
+    return st
+
+
+def random_start(n_complex: int, seed: int = 0) -> np.ndarray:
+    """Start vector with real and imaginary parts uniform in [-1, 1]."""
+    rng = np.random.default_rng(seed)
+    return rng.uniform(-1.0, 1.0, size=2 * n_complex)

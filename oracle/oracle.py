@@ -1,0 +1,208 @@
+"""ctypes front end of the CPU oracle (oracle/tb_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by ``__graft_entry__.smoke`` as
+the checker and by the CPU-baseline leg of ``bench.py``.  The product never
+imports it.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+NPV, NSTR = 35, 33
+NPAR = NPV + NSTR
+
+
+def build(force: bool = False) -> str:
+    src = os.path.join(HERE, "tb_oracle.c")
+    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(src):
+        subprocess.check_call(["gcc", "-O2", "-fopenmp", "-fPIC", "-shared", "-o", LIB,
+                               src, "-lm"], cwd=HERE)
+    return LIB
+
+
+class _Geom(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+                ("periodic", C.c_int * 3), ("lattice", C.c_double * 3),
+                ("type", C.c_void_p), ("dsp", C.c_void_p)]
+
+
+class _Model(C.Structure):
+    _fields_ = [("norb", C.c_int), ("nspin", C.c_int), ("include_strain", C.c_int),
+                ("passivate", C.c_int), ("dangling_shift", C.c_double),
+                ("nspecies", C.c_int), ("par", C.c_void_p), ("par_ok", C.c_void_p)]
+
+
+class _Opts(C.Structure):
+    _fields_ = [("conv_start", C.c_int), ("conv_skip", C.c_int), ("imax", C.c_int),
+                ("req1", C.c_int), ("req2", C.c_int),
+                ("emin1", C.c_double), ("emax1", C.c_double),
+                ("emin2", C.c_double), ("emax2", C.c_double),
+                ("tolerance", C.c_double), ("seed", C.c_uint)]
+
+
+class _Ham(C.Structure):
+    _fields_ = [("norb", C.c_int), ("nspin", C.c_int), ("natoms", C.c_long),
+                ("atom_slot", C.c_void_p), ("nbr", C.c_void_p), ("wrap", C.c_void_p),
+                ("kvec", C.c_void_p), ("onsite", C.c_void_p), ("blocks", C.c_void_p),
+                ("shift", C.c_double)]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = C.CDLL(build())
+        L = _lib
+        L.orc_prepare_params.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                         C.c_double, C.c_double, C.c_void_p]
+        L.orc_topology.restype = C.c_long
+        L.orc_topology.argtypes = [C.POINTER(_Geom), C.c_long, C.c_void_p, C.c_void_p,
+                                   C.c_void_p, C.c_void_p]
+        L.orc_build.argtypes = [C.POINTER(_Geom), C.POINTER(_Model), C.c_long,
+                                C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                C.c_void_p, C.c_void_p]
+        L.orc_hx.argtypes = [C.c_int, C.c_int, C.c_long] + [C.c_void_p] * 6 + \
+            [C.c_double, C.c_void_p, C.c_void_p]
+        L.orc_dense.argtypes = [C.c_int, C.c_int, C.c_long] + [C.c_void_p] * 7
+        L.orc_tridiag_eigs.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_double,
+                                       C.c_double, C.c_double, C.c_void_p]
+        L.orc_eigensolve_lanczos.argtypes = [C.c_void_p, C.c_void_p, C.c_long,
+                                             C.c_void_p, C.POINTER(_Opts), C.c_void_p,
+                                             C.c_void_p, C.c_void_p, C.c_void_p,
+                                             C.c_void_p, C.c_void_p]
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None else None
+
+
+def prepare_params(mat: dict, include_strain: bool = True) -> np.ndarray:
+    out = np.zeros(NPAR)
+    pv = np.zeros(NPV)
+    pv[:len(mat["pv"])] = mat["pv"]
+    st = np.asarray(mat["strain"], dtype=np.float64)
+    lib().orc_prepare_params(int(mat["family"] == "sp3s*"), int(include_strain),
+                             _p(pv), _p(st), float(mat["ev_offset"]),
+                             float(mat["a0"]), _p(out))
+    return out
+
+
+def param_table(materials, include_strain=True, nspecies=8):
+    """[ns, ns, NPAR] table indexed (cation species, anion species)."""
+    from nemo3d_b200.materials import SPECIES
+    par = np.zeros((nspecies, nspecies, NPAR))
+    ok = np.zeros((nspecies, nspecies), dtype=np.uint8)
+    for m in materials:
+        c, a = SPECIES[m["cation"]], SPECIES[m["anion"]]
+        par[c, a] = prepare_params(m, include_strain)
+        ok[c, a] = 1
+    return par, ok
+
+
+class OracleHamiltonian:
+    """Topology + assembled stored Hamiltonian of a structure."""
+
+    def __init__(self, st, norb, nspin, materials, include_strain=True,
+                 passivate=True, dangling_shift=30.0, kvec=None):
+        self.st, self.norb, self.nspin = st, norb, nspin
+        self.nb = norb * nspin
+        self.types = np.ascontiguousarray(st.types, dtype=np.uint8).reshape(-1)
+        self.dsp = None if st.dsp is None else np.ascontiguousarray(st.dsp, np.float64).reshape(-1)
+        g = _Geom()
+        g.nx, g.ny, g.nz = st.nx, st.ny, st.nz
+        g.periodic[:] = [int(bool(x)) for x in st.periodic]
+        g.lattice[:] = list(st.lattice)
+        g.type = _p(self.types)
+        g.dsp = _p(self.dsp)
+        self._g = g
+        ns = st.nsites
+        slot = np.zeros(ns, np.int32)
+        nbr = np.zeros(ns * 4, np.int32)
+        wrap = np.zeros(ns * 12, np.int8)
+        surf = np.zeros(ns, np.uint8)
+        na = lib().orc_topology(C.byref(g), ns, _p(slot), _p(nbr), _p(wrap), _p(surf))
+        self.natoms = int(na)
+        self.atom_slot = slot[:na].copy()
+        self.nbr = nbr[:na * 4].copy()
+        self.wrap = wrap[:na * 12].copy()
+        self.surface = surf[:na].copy()
+        self.par, self.par_ok = param_table(materials, include_strain)
+        m = _Model()
+        m.norb, m.nspin, m.include_strain = norb, nspin, int(include_strain)
+        m.passivate, m.dangling_shift = int(passivate), float(dangling_shift)
+        m.nspecies = self.par.shape[0]
+        m.par, m.par_ok = _p(self.par), _p(self.par_ok)
+        self._m = m
+        self.onsite = np.zeros(self.natoms * self.nb * self.nb * 2)
+        self.blocks = np.zeros(self.natoms * 4 * norb * norb)
+        rc = lib().orc_build(C.byref(g), C.byref(m), self.natoms, _p(self.atom_slot),
+                             _p(self.nbr), _p(self.wrap), _p(self.surface),
+                             _p(self.onsite), _p(self.blocks))
+        if rc != 0:
+            raise ValueError(f"orc_build failed ({rc}): missing material set")
+        self.kvec = None if kvec is None else np.asarray(kvec, np.float64)
+        self.n = self.natoms * self.nb
+
+    def hx(self, x, shift=0.0):
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.empty_like(x)
+        lib().orc_hx(self.norb, self.nspin, self.natoms, _p(self.atom_slot), _p(self.nbr),
+                     _p(self.wrap), _p(self.kvec), _p(self.onsite), _p(self.blocks),
+                     float(shift), _p(x), _p(y))
+        return y
+
+    def dense(self, kvec=None):
+        k = None if kvec is None else np.asarray(kvec, np.float64)
+        h = np.zeros(self.n * self.n * 2)
+        lib().orc_dense(self.norb, self.nspin, self.natoms, _p(self.atom_slot), _p(self.nbr),
+                        _p(self.wrap), _p(k), _p(self.onsite), _p(self.blocks), _p(h))
+        h = h.reshape(self.n, self.n, 2)
+        return h[..., 0] + 1j * h[..., 1]
+
+    def lanczos(self, r0, imax=2000, req=(1, 1), erange1=(-1, 0), erange2=(1, 2),
+                tol=1e-7, conv_start=200, conv_skip=50, eigvecs=False, seed=1,
+                shift=0.0):
+        """eigensolve_lanczos with this Hamiltonian; returns a dict."""
+        ham = _Ham()
+        ham.norb, ham.nspin, ham.natoms = self.norb, self.nspin, self.natoms
+        ham.atom_slot, ham.nbr, ham.wrap = _p(self.atom_slot), _p(self.nbr), _p(self.wrap)
+        ham.kvec, ham.onsite, ham.blocks = _p(self.kvec), _p(self.onsite), _p(self.blocks)
+        ham.shift = float(shift)
+        o = _Opts(conv_start, conv_skip, imax, req[0], req[1], erange1[0], erange1[1],
+                  erange2[0], erange2[1], tol, seed)
+        r0 = np.ascontiguousarray(r0, np.float64)
+        ev = np.zeros(imax)
+        cit = np.zeros(imax, np.int32)
+        its = np.zeros(1, np.int32)
+        al = np.zeros(imax)
+        be = np.zeros(imax)
+        nev_max = imax
+        vec = np.zeros(2 * self.n * min(nev_max, 64)) if eigvecs else None
+        fn = C.cast(lib().orc_ham_matvec, C.c_void_p)
+        ne = lib().orc_eigensolve_lanczos(fn, C.byref(ham), self.n, _p(r0), C.byref(o),
+                                          _p(ev), _p(cit), _p(its), _p(vec), _p(al), _p(be))
+        it = int(its[0])
+        out = dict(evals=ev[:ne].copy(), conv_it=cit[:ne].copy(), iterations=it,
+                   alpha=al[:it].copy(), beta=be[:it].copy())
+        if eigvecs:
+            v = vec[:2 * self.n * ne].reshape(ne, self.n, 2)
+            out["evecs"] = v[..., 0] + 1j * v[..., 1]
+        return out
+
+
+def tridiag_eigs(d, e, vl, vu, abstol=1e-13):
+    d = np.ascontiguousarray(d, np.float64)
+    e = np.ascontiguousarray(e, np.float64)
+    w = np.zeros(len(d))
+    n = lib().orc_tridiag_eigs(len(d), _p(d), _p(e), vl, vu, abstol, _p(w))
+    return w[:n].copy()
