@@ -1,0 +1,190 @@
+/*
+ * tbgpu.h -- C ABI of the B200 tight-binding eigensolver (libtbgpu.so).
+ *
+ * The three seams of NEMO-3D's electronic-structure hot path are replaced:
+ *
+ *   Hamiltonian build   setup_hamiltonian + first Hmult_spds_complete
+ *                       (nemo3d/src/base/ham3d_final.c:731,
+ *                        nemo3d/src/base/h_cvectr_mult.c:1194-1196)
+ *                       -> tbgpu_ctx_create + tbgpu_build_hamiltonian
+ *   H*x                 matvect_mult, the "matmul" function pointer
+ *                       (nemo3d/src/base/h_cvectr_mult.c:205-258,
+ *                        eigen/include/lanczos.h:287,336,389)
+ *                       -> tbgpu_matvect_mult (same signature)
+ *   Lanczos driver      eigensolve_lanczos (eigen/src/lanczos.c:1823-2089,
+ *                        eigen/include/lanczos.h:365-391)
+ *                       -> tbgpu_eigensolve_lanczos
+ *
+ * All pointers are plain host pointers unless the name ends in _dev (device
+ * pointers on the context's CUDA device).  Complex vectors are interleaved
+ * (re, im) doubles, layout-compatible with nml_dcscalar {double r, i}, in the
+ * reference's order: index = atom * NBasisStates + orbital, spin-up orbitals
+ * first (nemo3d/src/base/ham3d_final.c:547-620).
+ *
+ * Error convention: functions return TBGPU_OK (0) or a negative TBGPU_E_*
+ * code; a positive return of tbgpu_eigensolve_lanczos is the number of
+ * eigenvalues found.  tbgpu_last_error() repeats the last failure code of the
+ * calling thread and tbgpu_error_string() describes it.  The reference aborts
+ * via die()/error() instead (eigen/src/lanczos.c:270-296); nothing here exits
+ * the process.  A context is not re-entrant; distinct contexts are
+ * independent.  Every call runs on the context's CUDA stream.
+ */
+#ifndef TBGPU_H
+#define TBGPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TBGPU_OK 0
+#define TBGPU_E_ARG (-1)          /* invalid argument or size                */
+#define TBGPU_E_CUDA (-2)         /* a CUDA call failed                       */
+#define TBGPU_E_NOMEM (-3)        /* device allocation failed                 */
+#define TBGPU_E_MATERIAL (-4)     /* a bond has no material parameter set     */
+#define TBGPU_E_STATE (-5)        /* call out of order (e.g. H not built)     */
+#define TBGPU_E_UNSUPPORTED (-6)  /* option not supported by this build       */
+#define TBGPU_E_NUMERIC (-7)      /* breakdown (beta = 0, zero pivot, NaN)    */
+
+/* band models: orbitals per spin x spins (mb_ham_spds_micro2.h:43-48) */
+#define TBGPU_SP3S 1          /* 5 x 1: spin-up block of Bands_10_sp3ss_spin   */
+#define TBGPU_SP3S_SO 2       /* 5 x 2: Bands_10_sp3ss_spin                    */
+#define TBGPU_SP3D5S 3        /* 10 x 1: Bands_10_sp3d5ss_nospin               */
+#define TBGPU_SP3D5S_SO 4     /* 10 x 2: Bands_20_sp3d5ss_spin                 */
+
+#define TBGPU_NPAR 68         /* 35 mb_pv + 33 mb_strain after param_init      */
+
+typedef struct {
+  double r, i;
+} tbgpu_dcomplex; /* layout of nml_dcscalar */
+
+typedef struct tbgpu_ctx tbgpu_ctx;
+
+/* Geometry: a dense grid of zincblende conventional cells, cell (i,j,k)
+ * row-major with k fastest (the cell order of geo_struct::FillFirstShape,
+ * nemo3d/src/base/ham3d.c:745-900), 8 sites per cell (sites 0..3 cations,
+ * 4..7 anions, nemo3d/src/base/Cell.c:185-210).  Replaces geo_struct's
+ * AtomType / l_m_2_atomdsp (nemo3d/src/base/geo_struct.c:2109-2131). */
+typedef struct {
+  int nx, ny, nz;
+  int periodic[3];            /* periodic axes (Gamma point only)            */
+  double lattice[3];          /* a_x, a_y, a_z of the device (nm)            */
+  const unsigned char *type;  /* [nx*ny*nz*8] species id, 0 = no atom        */
+  const double *dsp;          /* [nx*ny*nz*8*3] displacement (nm) or NULL    */
+} tbgpu_geom;
+
+/* Physics options and parameters (ExecParam.Phys / ElCalc of the XML deck). */
+typedef struct {
+  int band_model;             /* TBGPU_SP3S ... TBGPU_SP3D5S_SO              */
+  int include_strain;         /* include_strain_in_Hamiltonian               */
+  int passivate;              /* SurfacePassivation == PassivateDanglingBond */
+  double dangling_shift;      /* DanglingBondEnergyShift (eV)                */
+  int nspecies;               /* species ids 0..nspecies-1                   */
+  const double *par;          /* [nspecies][nspecies][TBGPU_NPAR], (c, a)    */
+  const unsigned char *par_ok;/* [nspecies][nspecies]                        */
+} tbgpu_model;
+
+/* param_init for one material set (nemo3d/src/base/mat3d.c:133-307 with
+ * param_sp3s_2_sp3d5s, nemo3d/src/ham/mb_ham_spds_micro.c:2984-3026):
+ * sp3s_family = 1 for a 15-entry sp3s* mb_pv.  out[TBGPU_NPAR]. */
+int tbgpu_prepare_params(int sp3s_family, int include_strain,
+                         const double *mb_pv, const double *mb_strain,
+                         double ev_offset, double a0, double *out);
+
+/* Create a context on the current CUDA device; geometry and tables are copied
+ * (host pointers).  tbgpu_ctx_create_dev takes device pointers for type/dsp. */
+int tbgpu_ctx_create(const tbgpu_geom *geom, const tbgpu_model *model,
+                     tbgpu_ctx **out);
+int tbgpu_ctx_create_dev(const tbgpu_geom *geom_dev, const tbgpu_model *model,
+                         tbgpu_ctx **out);
+int tbgpu_ctx_destroy(tbgpu_ctx *ctx);
+
+/* Use a caller-owned CUDA stream (cudaStream_t passed as void*). */
+int tbgpu_set_stream(tbgpu_ctx *ctx, void *stream);
+
+/* Topology + Slater-Koster assembly on the GPU (replaces Hmult_spds_col's
+ * store pass, nemo3d/src/base/h_cvectr_mult.c:1134-1886). */
+int tbgpu_build_hamiltonian(tbgpu_ctx *ctx);
+
+long tbgpu_num_atoms(const tbgpu_ctx *ctx);
+long tbgpu_dimension(const tbgpu_ctx *ctx); /* complex length n_atoms * nb */
+
+/* Drop-in for the reference's matmul pointer (h_cvectr_mult.c:205):
+ * argList[0] = (int*)ctx, argList[1] = (int*)&shift (double), y = (H-shift)x
+ * over host vectors of length tbgpu_dimension(ctx).  On failure y is left
+ * unspecified and tbgpu_last_error() is set. */
+void tbgpu_matvect_mult(const int **argList, tbgpu_dcomplex *y,
+                        const tbgpu_dcomplex *x);
+
+/* y = (H - shift) x on device vectors (asynchronous on the context stream). */
+int tbgpu_hx_dev(tbgpu_ctx *ctx, double shift, const double *x_dev,
+                 double *y_dev);
+
+/* Lanczos eigensolver with the semantics of eigensolve_lanczos
+ * (eigen/src/lanczos.c:1823-2089): plain Lanczos, convergence test every
+ * ConvCheckSkipRate iterations after ConvCheckStartIter on the last two
+ * components of the tridiagonal eigenvector (lanczos.c:764-996), degenerate
+ * and ghost values dropped at resolution 100*tolerance, windows
+ * (emin1,emax1] and (emin2,emax2].  r_0: host start vector (normalised here,
+ * as lanczos_initialize does, eigsys3d_par.c:113-215).  values[>= imax]
+ * receives the eigenvalues ascending; conv_iterations (optional) the
+ * iteration at which each converged; *iterations the iteration count.  If
+ * vectors != NULL, the eigenvectors of the first max_vectors eigenvalues are
+ * rebuilt by a second Lanczos pass (eigenvectorsLanczos, lanczos.c:1364-1689)
+ * into vectors[max_vectors][dimension].  Returns the number of eigenvalues
+ * found or a negative error code. */
+int tbgpu_eigensolve_lanczos(tbgpu_ctx *ctx, int ConvCheckStartIter,
+                             int ConvCheckSkipRate, int imax, int requested1,
+                             int requested2, double emin1, double emax1,
+                             double emin2, double emax2, double tolerance,
+                             const tbgpu_dcomplex *r_0, double *values,
+                             int *conv_iterations, int *iterations,
+                             tbgpu_dcomplex *vectors, int max_vectors);
+
+/* Same with the start vector and the eigenvectors in device memory. */
+int tbgpu_eigensolve_lanczos_dev(tbgpu_ctx *ctx, int ConvCheckStartIter,
+                                 int ConvCheckSkipRate, int imax,
+                                 int requested1, int requested2, double emin1,
+                                 double emax1, double emin2, double emax2,
+                                 double tolerance, const double *r0_dev,
+                                 double *values, int *conv_iterations,
+                                 int *iterations, double *vectors_dev,
+                                 int max_vectors);
+
+/* Tridiagonal matrix of the last solve: alpha[n], beta[n] (n <= cap). */
+int tbgpu_get_tridiagonal(const tbgpu_ctx *ctx, double *alpha, double *beta,
+                          int cap);
+
+/* Export for parity tests (tbgpu_export_pattern mirrors the topology of
+ * get_total_hamiltonian_dimension_and_offsets / remove_few_bonded_atoms /
+ * FindSurfaceAtoms): atom_site[n_atoms] site index of each atom,
+ * nbr[n_atoms*4] neighbour atom or -1 in Cell.c nnmap order,
+ * surface[n_atoms] 1 for atoms with fewer than four neighbours. */
+int tbgpu_export_pattern(const tbgpu_ctx *ctx, int *atom_site, int *nbr,
+                         unsigned char *surface);
+
+/* Export the assembled H: onsite[n_atoms][nb][nb] complex (interleaved) and
+ * blocks[n_atoms][4][norb][norb] real, nonzero for cation atoms only,
+ * blocks[c][a] = <anion orbital a | H | cation orbital c>. */
+int tbgpu_export_hamiltonian(const tbgpu_ctx *ctx, double *onsite,
+                             double *blocks);
+
+/* Timing of the last solve / build (ms, CUDA events on the context stream). */
+typedef struct {
+  double build_ms;            /* topology + assembly                          */
+  double solve_ms;            /* eigensolve_lanczos, first pass               */
+  double vectors_ms;          /* second pass (eigenvectors)                   */
+  double spmv_ms;             /* sum over H*x launches (when profiling on)    */
+  long spmv_launches;
+  long lanczos_iterations;
+  long kernel_launches;       /* all kernels launched by the last solve       */
+} tbgpu_stats;
+int tbgpu_set_profiling(tbgpu_ctx *ctx, int on);
+int tbgpu_get_stats(const tbgpu_ctx *ctx, tbgpu_stats *out);
+
+int tbgpu_last_error(void);
+const char *tbgpu_error_string(int code);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

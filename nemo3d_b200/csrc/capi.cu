@@ -1,0 +1,344 @@
+// C ABI entry points of libtbgpu.so (declared in include/tbgpu.h).
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "tbgpu_internal.cuh"
+
+namespace tbgpu {
+
+static thread_local int g_last_error = TBGPU_OK;
+
+int set_error(int code) {
+  g_last_error = code;
+  return code;
+}
+
+
+static int model_dims(int bm, int *norb, int *nspin) {
+  switch (bm) {
+    case TBGPU_SP3S: *norb = 5; *nspin = 1; return TBGPU_OK;
+    case TBGPU_SP3S_SO: *norb = 5; *nspin = 2; return TBGPU_OK;
+    case TBGPU_SP3D5S: *norb = 10; *nspin = 1; return TBGPU_OK;
+    case TBGPU_SP3D5S_SO: *norb = 10; *nspin = 2; return TBGPU_OK;
+    default: return TBGPU_E_ARG;
+  }
+}
+
+static void free_ctx(Ctx *c) {
+  if (!c) return;
+  void *ptrs[] = {c->d_type, c->d_dsp, c->d_par, c->d_par_ok, c->d_site_index, c->d_atom_site,
+                  c->d_nbr, c->d_site_m, c->d_surface, c->d_onsite, c->d_blocks, c->d_partial,
+                  c->d_counter, c->d_status, c->d_x, c->d_y};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+static int create(const tbgpu_geom *g, const tbgpu_model *m, bool dev, tbgpu_ctx **out) {
+  if (!g || !m || !out || !g->type || !m->par || !m->par_ok) return set_error(TBGPU_E_ARG);
+  *out = nullptr;
+  if (g->nx <= 0 || g->ny <= 0 || g->nz <= 0 || m->nspecies <= 0 || m->nspecies > 255)
+    return set_error(TBGPU_E_ARG);
+  Ctx *c = new (std::nothrow) Ctx();
+  if (!c) return set_error(TBGPU_E_NOMEM);
+  if (model_dims(m->band_model, &c->norb, &c->nspin)) {
+    delete c;
+    return set_error(TBGPU_E_ARG);
+  }
+  c->band_model = m->band_model;
+  c->nb = c->norb * c->nspin;
+  c->ons = onsite_len(c->nb);
+  c->include_strain = m->include_strain;
+  c->passivate = m->passivate;
+  c->dangling_shift = m->dangling_shift;
+  c->nspecies = m->nspecies;
+  c->nx = g->nx; c->ny = g->ny; c->nz = g->nz;
+  for (int d = 0; d < 3; d++) {
+    c->periodic[d] = g->periodic[d] ? 1 : 0;
+    c->lattice[d] = g->lattice[d];
+  }
+  c->nsites = long(g->nx) * g->ny * g->nz * 8;
+  cudaGetDevice(&c->device);
+  auto fail = [&](int code) {
+    free_ctx(c);
+    return set_error(code);
+  };
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return fail(TBGPU_E_CUDA);
+  c->own_stream = true;
+  const size_t ns = size_t(c->nsites);
+  const size_t npar = size_t(m->nspecies) * m->nspecies;
+  if (cudaMalloc(&c->d_type, ns) != cudaSuccess) return fail(TBGPU_E_NOMEM);
+  if (g->dsp && cudaMalloc(&c->d_dsp, ns * 3 * sizeof(double)) != cudaSuccess)
+    return fail(TBGPU_E_NOMEM);
+  if (cudaMalloc(&c->d_par, npar * kNPAR * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&c->d_par_ok, npar) != cudaSuccess ||
+      cudaMalloc(&c->d_counter, sizeof(unsigned)) != cudaSuccess ||
+      cudaMalloc(&c->d_status, sizeof(int)) != cudaSuccess)
+    return fail(TBGPU_E_NOMEM);
+  if (!dev) {  // species ids index the parameter table
+    for (size_t i = 0; i < ns; i++)
+      if (g->type[i] >= m->nspecies) return fail(TBGPU_E_ARG);
+  }
+  const cudaMemcpyKind kind = dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  if (cudaMemcpy(c->d_type, g->type, ns, kind) != cudaSuccess) return fail(TBGPU_E_CUDA);
+  if (g->dsp && cudaMemcpy(c->d_dsp, g->dsp, ns * 3 * sizeof(double), kind) != cudaSuccess)
+    return fail(TBGPU_E_CUDA);
+  if (cudaMemcpy(c->d_par, m->par, npar * kNPAR * sizeof(double), cudaMemcpyHostToDevice) !=
+          cudaSuccess ||
+      cudaMemcpy(c->d_par_ok, m->par_ok, npar, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemset(c->d_counter, 0, sizeof(unsigned)) != cudaSuccess ||
+      cudaMemset(c->d_status, 0, sizeof(int)) != cudaSuccess)
+    return fail(TBGPU_E_CUDA);
+  *out = reinterpret_cast<tbgpu_ctx *>(c);
+  return TBGPU_OK;
+}
+
+static Ctx *C(tbgpu_ctx *p) { return reinterpret_cast<Ctx *>(p); }
+static const Ctx *C(const tbgpu_ctx *p) { return reinterpret_cast<const Ctx *>(p); }
+
+}  // namespace tbgpu
+
+using namespace tbgpu;
+
+extern "C" {
+
+int tbgpu_ctx_create(const tbgpu_geom *geom, const tbgpu_model *model, tbgpu_ctx **out) {
+  return create(geom, model, false, out);
+}
+
+int tbgpu_ctx_create_dev(const tbgpu_geom *geom, const tbgpu_model *model, tbgpu_ctx **out) {
+  return create(geom, model, true, out);
+}
+
+int tbgpu_ctx_destroy(tbgpu_ctx *ctx) {
+  if (!ctx) return set_error(TBGPU_E_ARG);
+  Ctx *c = C(ctx);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  free_ctx(c);
+  return TBGPU_OK;
+}
+
+int tbgpu_set_stream(tbgpu_ctx *ctx, void *stream) {
+  if (!ctx) return set_error(TBGPU_E_ARG);
+  Ctx *c = C(ctx);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  c->stream = reinterpret_cast<cudaStream_t>(stream);
+  c->own_stream = false;
+  return TBGPU_OK;
+}
+
+int tbgpu_build_hamiltonian(tbgpu_ctx *ctx) {
+  if (!ctx) return set_error(TBGPU_E_ARG);
+  Ctx &c = *C(ctx);
+  if (c.built) return set_error(TBGPU_E_STATE);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, c.stream);
+  int rc = build_topology(c);
+  if (rc == TBGPU_OK) rc = assemble(c);
+  if (rc == TBGPU_OK) rc = ensure_partials(c, int(c.natoms / 8 + 65536));
+  cudaEventRecord(e1, c.stream);
+  if (cudaStreamSynchronize(c.stream) != cudaSuccess && rc == TBGPU_OK) rc = set_error(TBGPU_E_CUDA);
+  int st = 0;
+  if (rc == TBGPU_OK && cudaMemcpy(&st, c.d_status, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+    rc = set_error(TBGPU_E_CUDA);
+  if (rc == TBGPU_OK && st != 0) rc = set_error(st);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  c.stats.build_ms = ms;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc == TBGPU_OK) c.built = true;
+  return rc;
+}
+
+long tbgpu_num_atoms(const tbgpu_ctx *ctx) { return ctx ? C(ctx)->natoms : -1; }
+
+long tbgpu_dimension(const tbgpu_ctx *ctx) {
+  return ctx ? C(ctx)->natoms * C(ctx)->nb : -1;
+}
+
+int tbgpu_hx_dev(tbgpu_ctx *ctx, double shift, const double *x_dev, double *y_dev) {
+  if (!ctx || !x_dev || !y_dev) return set_error(TBGPU_E_ARG);
+  Ctx &c = *C(ctx);
+  if (!c.built) return set_error(TBGPU_E_STATE);
+  return launch_spmv(c, x_dev, y_dev, shift, nullptr, 0, nullptr, 0, c.stream);
+}
+
+void tbgpu_matvect_mult(const int **argList, tbgpu_dcomplex *y, const tbgpu_dcomplex *x) {
+  if (!argList || !argList[0] || !x || !y) {
+    set_error(TBGPU_E_ARG);
+    return;
+  }
+  Ctx &c = *reinterpret_cast<Ctx *>(const_cast<int *>(argList[0]));
+  const double shift = argList[1] ? *reinterpret_cast<const double *>(argList[1]) : 0.0;
+  if (!c.built) {
+    set_error(TBGPU_E_STATE);
+    return;
+  }
+  const size_t bytes = sizeof(double) * 2 * size_t(c.natoms) * c.nb;
+  if (!c.d_x) {
+    if (cudaMalloc(&c.d_x, bytes) != cudaSuccess || cudaMalloc(&c.d_y, bytes) != cudaSuccess) {
+      set_error(TBGPU_E_NOMEM);
+      return;
+    }
+  }
+  if (cudaMemcpyAsync(c.d_x, x, bytes, cudaMemcpyHostToDevice, c.stream) != cudaSuccess) {
+    set_error(TBGPU_E_CUDA);
+    return;
+  }
+  if (launch_spmv(c, c.d_x, c.d_y, shift, nullptr, 0, nullptr, 0, c.stream)) return;
+  if (cudaMemcpyAsync(y, c.d_y, bytes, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
+      cudaStreamSynchronize(c.stream) != cudaSuccess)
+    set_error(TBGPU_E_CUDA);
+}
+
+int tbgpu_eigensolve_lanczos_dev(tbgpu_ctx *ctx, int ConvCheckStartIter, int ConvCheckSkipRate,
+                                 int imax, int requested1, int requested2, double emin1,
+                                 double emax1, double emin2, double emax2, double tolerance,
+                                 const double *r0_dev, double *values, int *conv_iterations,
+                                 int *iterations, double *vectors_dev, int max_vectors) {
+  if (!ctx) return set_error(TBGPU_E_ARG);
+  SolveArgs A{ConvCheckStartIter, ConvCheckSkipRate, imax, requested1, requested2,
+              emin1, emax1, emin2, emax2, tolerance};
+  return solve(*C(ctx), A, r0_dev, values, conv_iterations, iterations, vectors_dev,
+               max_vectors);
+}
+
+int tbgpu_eigensolve_lanczos(tbgpu_ctx *ctx, int ConvCheckStartIter, int ConvCheckSkipRate,
+                             int imax, int requested1, int requested2, double emin1,
+                             double emax1, double emin2, double emax2, double tolerance,
+                             const tbgpu_dcomplex *r_0, double *values, int *conv_iterations,
+                             int *iterations, tbgpu_dcomplex *vectors, int max_vectors) {
+  if (!ctx || !r_0) return set_error(TBGPU_E_ARG);
+  Ctx &c = *C(ctx);
+  if (!c.built) return set_error(TBGPU_E_STATE);
+  const size_t bytes = sizeof(double) * 2 * size_t(c.natoms) * c.nb;
+  double *r0 = nullptr, *V = nullptr;
+  if (cudaMalloc(&r0, bytes) != cudaSuccess) return set_error(TBGPU_E_NOMEM);
+  int nv = (vectors && max_vectors > 0) ? max_vectors : 0;
+  if (nv && cudaMalloc(&V, bytes * nv) != cudaSuccess) {
+    cudaFree(r0);
+    return set_error(TBGPU_E_NOMEM);
+  }
+  int rc = TBGPU_OK;
+  if (cudaMemcpyAsync(r0, r_0, bytes, cudaMemcpyHostToDevice, c.stream) != cudaSuccess)
+    rc = set_error(TBGPU_E_CUDA);
+  int ne = rc;
+  if (rc == TBGPU_OK)
+    ne = tbgpu_eigensolve_lanczos_dev(ctx, ConvCheckStartIter, ConvCheckSkipRate, imax,
+                                      requested1, requested2, emin1, emax1, emin2, emax2,
+                                      tolerance, r0, values, conv_iterations, iterations, V, nv);
+  if (ne > 0 && nv) {
+    const int got = ne < nv ? ne : nv;
+    if (cudaMemcpyAsync(vectors, V, bytes * got, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
+        cudaStreamSynchronize(c.stream) != cudaSuccess)
+      ne = set_error(TBGPU_E_CUDA);
+  }
+  cudaFree(r0);
+  if (V) cudaFree(V);
+  return ne;
+}
+
+int tbgpu_get_tridiagonal(const tbgpu_ctx *ctx, double *alpha, double *beta, int cap) {
+  if (!ctx || !alpha || !beta) return set_error(TBGPU_E_ARG);
+  const Ctx &c = *C(ctx);
+  const int n = int(c.alpha.size()) < cap ? int(c.alpha.size()) : cap;
+  for (int i = 0; i < n; i++) {
+    alpha[i] = c.alpha[i];
+    beta[i] = c.beta[i];
+  }
+  return n;
+}
+
+int tbgpu_export_pattern(const tbgpu_ctx *ctx, int *atom_site, int *nbr, unsigned char *surface) {
+  if (!ctx) return set_error(TBGPU_E_ARG);
+  const Ctx &c = *C(ctx);
+  if (!c.built) return set_error(TBGPU_E_STATE);
+  const size_t n = size_t(c.natoms);
+  if ((atom_site && cudaMemcpy(atom_site, c.d_atom_site, n * sizeof(int), cudaMemcpyDeviceToHost)) ||
+      (nbr && cudaMemcpy(nbr, c.d_nbr, n * sizeof(int4), cudaMemcpyDeviceToHost)) ||
+      (surface && cudaMemcpy(surface, c.d_surface, n, cudaMemcpyDeviceToHost)))
+    return set_error(TBGPU_E_CUDA);
+  return TBGPU_OK;
+}
+
+int tbgpu_export_hamiltonian(const tbgpu_ctx *ctx, double *onsite, double *blocks) {
+  if (!ctx) return set_error(TBGPU_E_ARG);
+  const Ctx &c = *C(ctx);
+  if (!c.built) return set_error(TBGPU_E_STATE);
+  const size_t n = size_t(c.natoms);
+  const int nb = c.nb, norb = c.norb;
+  if (blocks && cudaMemcpy(blocks, c.d_blocks, n * 4 * norb * norb * sizeof(double),
+                           cudaMemcpyDeviceToHost) != cudaSuccess)
+    return set_error(TBGPU_E_CUDA);
+  if (!onsite) return TBGPU_OK;
+  std::vector<double> rec(n * c.ons);
+  if (cudaMemcpy(rec.data(), c.d_onsite, rec.size() * sizeof(double), cudaMemcpyDeviceToHost) !=
+      cudaSuccess)
+    return set_error(TBGPU_E_CUDA);
+  std::memset(onsite, 0, sizeof(double) * n * nb * nb * 2);
+  for (size_t a = 0; a < n; a++) {
+    const double *r = rec.data() + a * c.ons;
+    double *h = onsite + a * nb * nb * 2;
+    auto re = [&](int i, int j) -> double & { return h[(i * nb + j) * 2]; };
+    auto im = [&](int i, int j) -> double & { return h[(i * nb + j) * 2 + 1]; };
+    for (int i = 0; i < nb; i++) re(i, i) = r[i];
+    for (int sp = 0; sp < c.nspin; sp++) {
+      const int o = sp * norb;
+      re(o + 1, o + 2) += r[nb + 2]; re(o + 2, o + 1) += r[nb + 2];
+      re(o + 1, o + 3) += r[nb + 3]; re(o + 3, o + 1) += r[nb + 3];
+      re(o + 1, o + 4) += r[nb + 4]; re(o + 4, o + 1) += r[nb + 4];
+      re(o + 2, o + 3) += r[nb + 5]; re(o + 3, o + 2) += r[nb + 5];
+      re(o + 2, o + 4) += r[nb + 6]; re(o + 4, o + 2) += r[nb + 6];
+      re(o + 3, o + 4) += r[nb + 7]; re(o + 4, o + 3) += r[nb + 7];
+    }
+    if (c.nspin == 2) {  // spin-orbit (mb_ham_spds_so.h)
+      const double L = r[nb];
+      const int u = 0, d = norb;
+      im(u + 2, u + 3) += -L; im(u + 3, u + 2) += L;
+      im(d + 2, d + 3) += L;  im(d + 3, d + 2) += -L;
+      re(u + 2, d + 4) += L;  im(u + 3, d + 4) += -L;
+      re(u + 4, d + 2) += -L; im(u + 4, d + 3) += L;
+      re(d + 2, u + 4) += -L; im(d + 3, u + 4) += -L;
+      re(d + 4, u + 2) += L;  im(d + 4, u + 3) += L;
+    }
+  }
+  return TBGPU_OK;
+}
+
+int tbgpu_set_profiling(tbgpu_ctx *ctx, int on) {
+  if (!ctx) return set_error(TBGPU_E_ARG);
+  C(ctx)->profiling = on != 0;
+  return TBGPU_OK;
+}
+
+int tbgpu_get_stats(const tbgpu_ctx *ctx, tbgpu_stats *out) {
+  if (!ctx || !out) return set_error(TBGPU_E_ARG);
+  *out = C(ctx)->stats;
+  return TBGPU_OK;
+}
+
+int tbgpu_last_error(void) { return g_last_error; }
+
+const char *tbgpu_error_string(int code) {
+  switch (code) {
+    case TBGPU_OK: return "ok";
+    case TBGPU_E_ARG: return "invalid argument";
+    case TBGPU_E_CUDA: return "CUDA call failed";
+    case TBGPU_E_NOMEM: return "device allocation failed";
+    case TBGPU_E_MATERIAL: return "no material parameter set for a bond";
+    case TBGPU_E_STATE: return "call out of order";
+    case TBGPU_E_UNSUPPORTED: return "unsupported option";
+    case TBGPU_E_NUMERIC: return "numerical breakdown";
+    default: return "unknown error";
+  }
+}
+
+}  // extern "C"

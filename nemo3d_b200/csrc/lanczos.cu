@@ -1,0 +1,580 @@
+// Lanczos eigensolver driver with the semantics of the reference's
+// eigensolve_lanczos (eigen/src/lanczos.c:1823-2089).
+//
+// Device side, per iteration n (single_lanczos_iteration, lanczos.c:421-757):
+//   k_spmv (fused):  w = H q_n with q_n = r_{n-1} / beta_{n-1} formed on the
+//                    fly, alpha_n = Re<q_n, w>            (spmv.cu)
+//   k_update:        r_n = w - (alpha_n q_n + beta_{n-1} q_{n-1}),
+//                    beta_n = ||r_n||
+// Vectors are kept as the unnormalised r's in a ring of buffers; q's are
+// formed on the fly, so an iteration moves the Hamiltonian once and six
+// vector-lengths of data.  alpha/beta live in device memory; the host never
+// waits inside the recurrence.
+//
+// Host side: the convergence test (find_converged_eigval, lanczos.c:764-996)
+// runs on a copy of the tridiagonal matrix while the GPU continues with the
+// next batch of iterations; the iteration count and the tridiagonal matrix
+// used are those of the check that declared convergence, as in the
+// reference.  Eigenvectors: second pass (eigenvectorsLanczos, method 3,
+// lanczos.c:1364-1689) with the Ritz combination accumulated in chunks of
+// iterations (k_accum) rather than one axpy per eigenvector per iteration.
+#include <algorithm>
+#include <atomic>
+#include <thread>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "tbgpu_internal.cuh"
+#include "reduce.cuh"
+
+namespace tbgpu {
+
+constexpr int kRedThreads = 256;
+
+int ensure_partials(Ctx &c, int nblocks) {
+  if (nblocks <= c.partial_cap) return TBGPU_OK;
+  if (c.d_partial) cudaFree(c.d_partial);
+  c.d_partial = nullptr;
+  c.partial_cap = 0;
+  if (cudaMalloc(&c.d_partial, sizeof(double) * nblocks) != cudaSuccess)
+    return set_error(TBGPU_E_NOMEM);
+  c.partial_cap = nblocks;
+  return TBGPU_OK;
+}
+
+static unsigned red_grid(const Ctx &c, long n2) {
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device);
+  long want = (n2 + kRedThreads - 1) / kRedThreads;
+  long g = std::min<long>(want, long(sms) * 8);
+  return unsigned(std::max<long>(g, 1));
+}
+
+// out[idx] = sqrt(sum |x|^2)
+__global__ void __launch_bounds__(kRedThreads)
+    k_norm(long n2, const double2 *__restrict__ x, double *partial, unsigned *counter,
+           double *out, int idx) {
+  double s = 0.0;
+  for (long j = blockIdx.x * (long)blockDim.x + threadIdx.x; j < n2;
+       j += (long)gridDim.x * blockDim.x) {
+    const double2 v = x[j];
+    s += v.x * v.x + v.y * v.y;
+  }
+  grid_reduce<kRedThreads>(s, partial, counter, out, idx, true);
+}
+
+// y = x / (*den)   (lanczos_initialize divides by the norm, eigsys3d_par.c:199-211)
+__global__ void k_divide(long n2, const double2 *__restrict__ x, const double *den,
+                         double2 *__restrict__ y) {
+  const double d = *den;
+  for (long j = blockIdx.x * (long)blockDim.x + threadIdx.x; j < n2;
+       j += (long)gridDim.x * blockDim.x) {
+    const double2 v = x[j];
+    y[j] = make_double2(v.x / d, v.y / d);
+  }
+}
+
+// r_n = w - (alpha q + beta_prev q_prev), q = rc/bet[it], q_prev = rp/bet[it-1];
+// bet[it+1] = ||r_n||.  bet[0] is the norm of the start vector.
+__global__ void __launch_bounds__(kRedThreads)
+    k_update(long n2, const double2 *__restrict__ w, const double2 *__restrict__ rc,
+             const double2 *__restrict__ rp, double2 *__restrict__ rout,
+             const double *alpha, double *bet, int it, double *partial, unsigned *counter) {
+  const double al = alpha[it], bprev = bet[it];
+  const double iq = 1.0 / bprev;
+  const double ip = it > 0 ? 1.0 / bet[it - 1] : 0.0;
+  double s = 0.0;
+  for (long j = blockIdx.x * (long)blockDim.x + threadIdx.x; j < n2;
+       j += (long)gridDim.x * blockDim.x) {
+    const double2 wv = w[j], cv = rc[j];
+    const double2 q = make_double2(cv.x * iq, cv.y * iq);
+    double2 p = make_double2(0.0, 0.0);
+    if (it > 0) {
+      const double2 pv = rp[j];
+      p = make_double2(pv.x * ip, pv.y * ip);
+    }
+    double2 r;
+    r.x = wv.x - (al * q.x + bprev * p.x);
+    r.y = wv.y - (al * q.y + bprev * p.y);
+    rout[j] = r;
+    s += r.x * r.x + r.y * r.y;
+  }
+  grid_reduce<kRedThreads>(s, partial, counter, bet, it + 1, true);
+}
+
+constexpr int kMaxChunk = 32;
+constexpr int kVecGroup = 16;
+struct ChunkPtrs {
+  const double2 *r[kMaxChunk];
+};
+
+// V[e] += sum_k coef[k][e] * R_k for one group of up to kVecGroup vectors
+__global__ void __launch_bounds__(256)
+    k_accum(long n2, int nk, int nv, ChunkPtrs R, const double *__restrict__ coef, int ldc,
+            double2 *__restrict__ V) {
+  __shared__ double cs[kMaxChunk * kVecGroup];
+  for (int t = threadIdx.x; t < nk * nv; t += blockDim.x)
+    cs[t] = coef[(t / nv) * ldc + (t % nv)];
+  __syncthreads();
+  for (long j = blockIdx.x * (long)blockDim.x + threadIdx.x; j < n2;
+       j += (long)gridDim.x * blockDim.x) {
+    double2 acc[kVecGroup];
+#pragma unroll
+    for (int e = 0; e < kVecGroup; e++)
+      if (e < nv) acc[e] = V[e * n2 + j];
+    for (int k = 0; k < nk; k++) {
+      const double2 r = R.r[k][j];
+#pragma unroll
+      for (int e = 0; e < kVecGroup; e++)
+        if (e < nv) {
+          const double cf = cs[k * nv + e];
+          acc[e].x = fma(cf, r.x, acc[e].x);
+          acc[e].y = fma(cf, r.y, acc[e].y);
+        }
+    }
+#pragma unroll
+    for (int e = 0; e < kVecGroup; e++)
+      if (e < nv) V[e * n2 + j] = acc[e];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host: tridiagonal eigenvalues (Sturm bisection in place of LAPACK dstebz,
+// lanczos.c:793-811) and inverse iteration (originalInverseIteration,
+// lanczos.c:378-418; solve_rtridiag_ii, lanczos.c:249-308).
+
+static int sturm_below(int n, const double *d, const double *e2, double x) {
+  int cnt = 0;
+  double q = d[0] - x;
+  if (q < 0) cnt++;
+  for (int i = 1; i < n; i++) {
+    if (std::fabs(q) < 1e-300) q = q < 0 ? -1e-300 : 1e-300;
+    q = d[i] - x - e2[i - 1] / q;
+    if (q < 0) cnt++;
+  }
+  return cnt;
+}
+
+// run f(i) for i in [0, n) on up to hardware_concurrency host threads
+template <class F>
+static void parallel_for(int n, F f) {
+  int nt = int(std::thread::hardware_concurrency());
+  nt = std::max(1, std::min({nt, 32, n}));
+  if (nt <= 1) {
+    for (int i = 0; i < n; i++) f(i);
+    return;
+  }
+  std::atomic<int> next{0};
+  std::vector<std::thread> th;
+  for (int t = 0; t < nt; t++)
+    th.emplace_back([&]() {
+      for (int i = next++; i < n; i = next++) f(i);
+    });
+  for (auto &x : th) x.join();
+}
+
+// eigenvalues of T (diag d, off-diagonal e) in (vl, vu], ascending
+static std::vector<double> tri_eigs(int n, const double *d, const double *e, double vl,
+                                    double vu) {
+  std::vector<double> e2(std::max(n - 1, 1));
+  double lo = d[0], hi = d[0];
+  for (int i = 0; i < n - 1; i++) e2[i] = e[i] * e[i];
+  for (int i = 0; i < n; i++) {
+    const double r = (i > 0 ? std::fabs(e[i - 1]) : 0.0) + (i < n - 1 ? std::fabs(e[i]) : 0.0);
+    lo = std::min(lo, d[i] - r);
+    hi = std::max(hi, d[i] + r);
+  }
+  const int c0 = sturm_below(n, d, e2.data(), vl), c1 = sturm_below(n, d, e2.data(), vu);
+  std::vector<double> w(std::max(c1 - c0, 0));
+  parallel_for(c1 - c0, [&](int k) {
+    const int idx = c0 + k;
+    double a = std::max(vl, lo), b = std::min(vu, hi);
+    for (int it = 0; it < 200; it++) {
+      const double tol = 1e-13 + 2.2e-16 * std::max(std::fabs(a), std::fabs(b));
+      if (b - a <= tol) break;
+      const double mid = 0.5 * (a + b);
+      if (sturm_below(n, d, e2.data(), mid) > idx) b = mid;
+      else a = mid;
+    }
+    w[k] = 0.5 * (a + b);
+  });
+  return w;
+}
+
+struct Rng {  // uniform [0,1] starts for inverse iteration
+  unsigned long long s;
+  double next() {
+    s = s * 6364136223846793005ULL + 1442695040888963407ULL;
+    return double(s >> 11) * (1.0 / 9007199254740992.0);
+  }
+};
+
+// 20 solves with T - (lambda + 1e-8) on the leading m x m block; x out
+static bool inverse_iteration(int m, const double *d, const double *e, double lambda,
+                              Rng &rng, std::vector<double> &x) {
+  std::vector<double> ds(m), g(m), y(m);
+  x.assign(m, 0.0);
+  for (int i = 0; i < m; i++) ds[i] = d[i] - (lambda + 1e-8);
+  double nrm = 0.0;
+  for (int i = 0; i < m; i++) {
+    y[i] = rng.next();
+    nrm += y[i] * y[i];
+  }
+  nrm = std::sqrt(nrm);
+  for (int i = 0; i < m; i++) y[i] /= nrm;
+  for (int it = 0; it < 20; it++) {
+    double piv = ds[0];
+    if (piv == 0.0) return false;
+    x[0] = y[0] / piv;
+    for (int j = 1; j < m; j++) {
+      g[j] = e[j - 1] / piv;
+      piv = ds[j] - e[j - 1] * g[j];
+      if (piv == 0.0) return false;
+      x[j] = (y[j] - e[j - 1] * x[j - 1]) / piv;
+    }
+    for (int j = m - 1; j > 0; j--) x[j - 1] -= g[j] * x[j];
+    nrm = 0.0;
+    for (int i = 0; i < m; i++) nrm += x[i] * x[i];
+    nrm = std::sqrt(nrm);
+    for (int i = 0; i < m; i++) y[i] = x[i] / nrm;
+  }
+  x = y;
+  return true;
+}
+
+// find_converged_eigval, method 2 (lanczos.c:764-996).  The inverse
+// iterations of the candidates run in parallel; the acceptance pass then
+// walks the candidates in ascending order exactly as the reference does.
+static void check_window(int it, const double *al, const double *be, double emin,
+                         double emax, double tol, double res, std::vector<double> &conv,
+                         std::vector<int> &conv_it, unsigned long long seed) {
+  const std::vector<double> ev = tri_eigs(it, al, be, emin, emax);
+  const int ne = int(ev.size());
+  std::vector<char> cand(ne, 0), ok(ne, 0);
+  for (int i = 0; i < ne; i++) {
+    if (i > 0 && std::fabs(ev[i - 1] - ev[i]) < std::fabs(1e-80 + ev[i]) * res) continue;
+    bool done = false;
+    for (double c : conv)
+      if (std::fabs(c - ev[i]) < res) done = true;
+    cand[i] = !done;
+  }
+  parallel_for(ne, [&](int i) {
+    if (!cand[i]) return;
+    Rng rng{seed ^ (0x9E3779B97F4A7C15ULL * (unsigned long long)(i + 1))};
+    std::vector<double> x;
+    if (!inverse_iteration(it, al, be, ev[i], rng, x)) return;
+    bool flag = true;
+    for (int k = std::max(it - 2, 0); k < it; k++)
+      if (std::fabs(x[k]) > tol) flag = false;
+    ok[i] = flag;
+  });
+  for (int i = 0; i < ne; i++) {
+    if (!cand[i] || !ok[i]) continue;
+    bool done = false;  // may have converged earlier in this same pass
+    for (double c : conv)
+      if (std::fabs(c - ev[i]) < res) done = true;
+    if (done) continue;
+    conv.push_back(ev[i]);
+    conv_it.push_back(it);
+  }
+}
+
+struct Timers {
+  cudaEvent_t t0, t1, t2, t3;
+};
+
+int solve(Ctx &c, const SolveArgs &A, const double *r0_dev, double *values, int *conv_iters,
+          int *iterations, double *V_dev, int maxvec) {
+  if (!c.built) return set_error(TBGPU_E_STATE);
+  if (A.imax < 2 || A.conv_skip < 1 || !values || !r0_dev) return set_error(TBGPU_E_ARG);
+  const long n2 = c.natoms * c.nb;  // complex entries
+  const size_t vbytes = sizeof(double2) * n2;
+  cudaStream_t s = c.stream;
+  const unsigned rg = red_grid(c, n2);
+  int rc = ensure_partials(c, int(rg));
+  if (rc) return rc;
+  long launches = 0;
+  c.stats.spmv_ms = 0.0;
+  c.stats.spmv_launches = 0;
+
+  // device state
+  const int S1 = 3;  // ring of r's for the first pass
+  double2 *ring[kMaxChunk + 1] = {nullptr};
+  double2 *W = nullptr;
+  double *d_alpha = nullptr, *d_bet = nullptr, *d_tmp = nullptr;
+  double *h_alpha = nullptr, *h_bet = nullptr;
+  std::vector<cudaEvent_t> spmv_ev;
+  auto cleanup = [&]() {
+    for (int i = 0; i <= kMaxChunk; i++)
+      if (ring[i]) cudaFree(ring[i]);
+    if (W) cudaFree(W);
+    if (d_alpha) cudaFree(d_alpha);
+    if (d_bet) cudaFree(d_bet);
+    if (d_tmp) cudaFree(d_tmp);
+    if (h_alpha) cudaFreeHost(h_alpha);
+    if (h_bet) cudaFreeHost(h_bet);
+    for (auto e : spmv_ev) cudaEventDestroy(e);
+  };
+#define SOLVE_CUDA(call)                 \
+  do {                                   \
+    if ((call) != cudaSuccess) {         \
+      cleanup();                         \
+      return set_error(TBGPU_E_CUDA);    \
+    }                                    \
+  } while (0)
+#define SOLVE_RC(expr)        \
+  do {                        \
+    int rc_ = (expr);         \
+    if (rc_) {                \
+      cleanup();              \
+      return rc_;             \
+    }                         \
+  } while (0)
+  for (int i = 0; i < S1; i++) SOLVE_CUDA(cudaMalloc(&ring[i], vbytes));
+  SOLVE_CUDA(cudaMalloc(&W, vbytes));
+  SOLVE_CUDA(cudaMalloc(&d_alpha, sizeof(double) * (A.imax + 1)));
+  SOLVE_CUDA(cudaMalloc(&d_bet, sizeof(double) * (A.imax + 2)));
+  SOLVE_CUDA(cudaMalloc(&d_tmp, sizeof(double) * 4));
+  SOLVE_CUDA(cudaMallocHost(&h_alpha, sizeof(double) * (A.imax + 2) * 3));
+  SOLVE_CUDA(cudaMallocHost(&h_bet, sizeof(double) * (A.imax + 2) * 3));
+  Timers tm;
+  cudaEventCreate(&tm.t0);
+  cudaEventCreate(&tm.t1);
+  cudaEventCreate(&tm.t2);
+  cudaEventCreate(&tm.t3);
+
+  // start vector: r = r0 / ||r0||; bet[0] = ||r||
+  auto start = [&](double *bet) -> int {
+    k_norm<<<rg, kRedThreads, 0, s>>>(n2, reinterpret_cast<const double2 *>(r0_dev),
+                                      c.d_partial, c.d_counter, d_tmp, 0);
+    k_divide<<<rg, kRedThreads, 0, s>>>(n2, reinterpret_cast<const double2 *>(r0_dev), d_tmp,
+                                        ring[0]);
+    k_norm<<<rg, kRedThreads, 0, s>>>(n2, ring[0], c.d_partial, c.d_counter, bet, 0);
+    launches += 3;
+    return cudaGetLastError() == cudaSuccess ? TBGPU_OK : set_error(TBGPU_E_CUDA);
+  };
+  // one Lanczos iteration with ring size S
+  auto step = [&](int it, int S, double *bet) -> int {
+    double2 *rc_ = ring[it % S], *rp_ = ring[(it + S - 1) % S], *ro = ring[(it + 1) % S];
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (c.profiling) {
+      cudaEventCreate(&e0);
+      cudaEventCreate(&e1);
+      cudaEventRecord(e0, s);
+    }
+    int r_ = launch_spmv(c, reinterpret_cast<const double *>(rc_), reinterpret_cast<double *>(W),
+                         0.0, bet, it, d_alpha, it, s);
+    if (r_) return r_;
+    if (c.profiling) {
+      cudaEventRecord(e1, s);
+      spmv_ev.push_back(e0);
+      spmv_ev.push_back(e1);
+    }
+    k_update<<<rg, kRedThreads, 0, s>>>(n2, W, rc_, it > 0 ? rp_ : nullptr, ro, d_alpha, bet, it,
+                                        c.d_partial, c.d_counter);
+    launches += 2;
+    return cudaGetLastError() == cudaSuccess ? TBGPU_OK : set_error(TBGPU_E_CUDA);
+  };
+
+  // ---- first pass: eigenvalues --------------------------------------------
+  cudaEventRecord(tm.t0, s);
+  SOLVE_RC(start(d_bet));
+  std::vector<double> c1, c2;
+  std::vector<int> i1, i2;
+  Rng rng{0x9E3779B97F4A7C15ULL};  // starts of the eigenvector inverse iterations
+  const double res = 100.0 * A.tol;
+  // check points exactly as lanczos_tridiagonal's skip counter places them
+  auto next_check = [&](int after, int skip_at_after) {
+    int skip = skip_at_after;
+    for (int it = after + 1; it < A.imax; it++) {
+      skip++;
+      if (A.conv_start < it && A.conv_skip <= skip) return it;
+    }
+    return A.imax;  // none before the iteration limit
+  };
+  // all check points below the iteration limit
+  std::vector<int> checks;
+  for (int at = next_check(0, 0); at < A.imax; at = next_check(at, 0)) checks.push_back(at);
+  // The GPU runs up to kAhead check batches ahead of the host's test; each
+  // check in flight copies alpha/beta into its own pinned slot.
+  constexpr int kAhead = 2;
+  const size_t slot = size_t(A.imax) + 2;
+  int launched = 0;  // iterations enqueued
+  int final_it = -1;
+  struct Pending {
+    int at, slot;
+    cudaEvent_t ev;
+  };
+  std::vector<Pending> pend;
+  auto enqueue_until = [&](int upto) -> int {  // launch iterations [launched, upto)
+    const int lim = std::min(upto, A.imax - 1);
+    for (; launched < lim; launched++) {
+      int r_ = step(launched, S1, d_bet);
+      if (r_) return r_;
+    }
+    return TBGPU_OK;
+  };
+  size_t qi = 0;  // next check to enqueue
+  auto fill = [&]() -> int {
+    while (qi < checks.size() && pend.size() < size_t(kAhead)) {
+      const int at = checks[qi];
+      int r_ = enqueue_until(at);
+      if (r_) return r_;
+      const int sl = int(qi % (kAhead + 1));
+      cudaEvent_t ev;
+      if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess)
+        return set_error(TBGPU_E_CUDA);
+      cudaMemcpyAsync(h_alpha + sl * slot, d_alpha, sizeof(double) * at, cudaMemcpyDeviceToHost, s);
+      cudaMemcpyAsync(h_bet + sl * slot, d_bet, sizeof(double) * (at + 1), cudaMemcpyDeviceToHost, s);
+      if (cudaEventRecord(ev, s) != cudaSuccess) return set_error(TBGPU_E_CUDA);
+      pend.push_back({at, sl, ev});
+      qi++;
+    }
+    return TBGPU_OK;
+  };
+  std::vector<double> Ta, Tb;
+  const double *hb_final = h_bet;  // beta copy used by the second pass
+  SOLVE_RC(fill());
+  while (!pend.empty()) {
+    Pending p = pend.front();
+    pend.erase(pend.begin());
+    SOLVE_CUDA(cudaEventSynchronize(p.ev));
+    cudaEventDestroy(p.ev);
+    const double *ha = h_alpha + p.slot * slot, *hb = h_bet + p.slot * slot;
+    Ta.assign(ha, ha + p.at);
+    // off-diagonal: beta_n couples n and n+1, beta_n = bet[n+1]
+    Tb.assign(hb + 1, hb + 1 + p.at);
+    for (double v : Ta)
+      if (!std::isfinite(v)) {
+        cleanup();
+        return set_error(TBGPU_E_NUMERIC);
+      }
+    if (A.req1 > 0 && int(c1.size()) <= A.req1)
+      check_window(p.at, Ta.data(), Tb.data(), A.emin1, A.emax1, A.tol, res, c1, i1,
+                   0x51ED27ULL * p.at + 1);
+    if (A.req2 > 0 && int(c2.size()) <= A.req2)
+      check_window(p.at, Ta.data(), Tb.data(), A.emin2, A.emax2, A.tol, res, c2, i2,
+                   0x51ED27ULL * p.at + 2);
+    const bool more = (p.at + 1 < A.imax) &&
+                      (int(c1.size()) < A.req1 || int(c2.size()) < A.req2);
+    if (!more) {
+      final_it = p.at;
+      hb_final = hb;
+      break;
+    }
+    SOLVE_RC(fill());
+  }
+  for (auto &p : pend) cudaEventDestroy(p.ev);
+  pend.clear();
+  if (final_it < 0) {  // no check declared convergence: run to the iteration limit
+    SOLVE_RC(enqueue_until(A.imax));
+    final_it = launched;
+  }
+  SOLVE_CUDA(cudaEventRecord(tm.t1, s));
+  SOLVE_CUDA(cudaStreamSynchronize(s));
+  if (final_it == launched) {  // stopped by the iteration limit: T up to there
+    SOLVE_CUDA(cudaMemcpy(h_alpha, d_alpha, sizeof(double) * final_it, cudaMemcpyDeviceToHost));
+    SOLVE_CUDA(cudaMemcpy(h_bet, d_bet, sizeof(double) * (final_it + 1), cudaMemcpyDeviceToHost));
+    Ta.assign(h_alpha, h_alpha + final_it);
+    Tb.assign(h_bet + 1, h_bet + 1 + final_it);
+    hb_final = h_bet;
+  }
+  c.alpha = Ta;
+  c.beta = Tb;
+  std::vector<std::pair<double, int>> found;
+  for (size_t k = 0; k < c1.size(); k++) found.push_back({c1[k], i1[k]});
+  for (size_t k = 0; k < c2.size(); k++) found.push_back({c2[k], i2[k]});
+  std::stable_sort(found.begin(), found.end(),
+                   [](const std::pair<double, int> &x, const std::pair<double, int> &y) {
+                     return x.first < y.first;
+                   });
+  const int ne = int(found.size());
+  for (int k = 0; k < ne; k++) {
+    values[k] = found[k].first;
+    if (conv_iters) conv_iters[k] = found[k].second;
+  }
+  if (iterations) *iterations = final_it;
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, tm.t0, tm.t1);
+  c.stats.solve_ms = ms;
+  c.stats.vectors_ms = 0.0;
+  c.stats.lanczos_iterations = launched;
+
+  // ---- second pass: eigenvectors -------------------------------------------
+  const int nvec = std::min(ne, std::max(maxvec, 0));
+  if (V_dev && nvec > 0) {
+    // Ritz coefficients on the truncated tridiagonal of each eigenvalue
+    int maxit = 0;
+    for (int k = 0; k < nvec; k++) maxit = std::max(maxit, found[k].second);
+    std::vector<double> coef(size_t(maxit) * nvec, 0.0), x;
+    for (int k = 0; k < nvec; k++) {
+      const int req = found[k].second;
+      if (!inverse_iteration(req, Ta.data(), Tb.data(), found[k].first, rng, x)) {
+        cleanup();
+        return set_error(TBGPU_E_NUMERIC);
+      }
+      // q_it = r_{it-1} / bet[it]; fold the 1/bet into the coefficient
+      for (int it = 0; it < req; it++) coef[size_t(it) * nvec + k] = x[it] * (1.0 / hb_final[it]);
+    }
+    // bet of the first pass up to maxit is needed on the host
+    if (maxit > final_it) maxit = final_it;
+    double *d_coef = nullptr;
+    SOLVE_CUDA(cudaMalloc(&d_coef, sizeof(double) * coef.size()));
+    SOLVE_CUDA(cudaMemcpyAsync(d_coef, coef.data(), sizeof(double) * coef.size(),
+                               cudaMemcpyHostToDevice, s));
+    // chunk size limited by free memory
+    size_t fre = 0, tot = 0;
+    cudaMemGetInfo(&fre, &tot);
+    int K = kMaxChunk;
+    while (K > 2 && size_t(K + 1 - S1) * vbytes + (256ull << 20) > fre) K /= 2;
+    const int S2 = K + 1;
+    for (int i = S1; i < S2; i++) SOLVE_CUDA(cudaMalloc(&ring[i], vbytes));
+    SOLVE_CUDA(cudaMemsetAsync(V_dev, 0, vbytes * nvec, s));
+    cudaEventRecord(tm.t2, s);
+    SOLVE_RC(start(d_bet));
+    int it0 = 0;
+    for (int it = 0; it < maxit; it++) {
+      SOLVE_RC(step(it, S2, d_bet));
+      if ((it + 1 - it0) == K || it == maxit - 1) {
+        ChunkPtrs P{};
+        const int nk = it + 1 - it0;
+        for (int k = 0; k < nk; k++) P.r[k] = ring[(it0 + k) % S2];
+        for (int g = 0; g < nvec; g += kVecGroup) {
+          const int nv = std::min(kVecGroup, nvec - g);
+          k_accum<<<rg, 256, 0, s>>>(n2, nk, nv, P, d_coef + size_t(it0) * nvec + g, nvec,
+                                     reinterpret_cast<double2 *>(V_dev) + size_t(g) * n2);
+          launches++;
+        }
+        it0 = it + 1;
+      }
+    }
+    cudaEventRecord(tm.t3, s);
+    SOLVE_CUDA(cudaStreamSynchronize(s));
+    cudaFree(d_coef);
+    cudaEventElapsedTime(&ms, tm.t2, tm.t3);
+    c.stats.vectors_ms = ms;
+  }
+  if (c.profiling) {
+    SOLVE_CUDA(cudaStreamSynchronize(s));
+    double tot = 0.0;
+    for (size_t k = 0; k + 1 < spmv_ev.size(); k += 2) {
+      float t = 0.f;
+      cudaEventElapsedTime(&t, spmv_ev[k], spmv_ev[k + 1]);
+      tot += t;
+    }
+    c.stats.spmv_ms = tot;
+    c.stats.spmv_launches = long(spmv_ev.size() / 2);
+  }
+  c.stats.kernel_launches = launches;
+  cudaEventDestroy(tm.t0);
+  cudaEventDestroy(tm.t1);
+  cudaEventDestroy(tm.t2);
+  cudaEventDestroy(tm.t3);
+  cleanup();
+#undef SOLVE_CUDA
+#undef SOLVE_RC
+  return ne;
+}
+
+}  // namespace tbgpu

@@ -1,0 +1,182 @@
+// y = (H - shift) x over the stored Hamiltonian, optionally with the Lanczos
+// alpha = Re<x, y> fused into the epilogue.
+//
+// Restates Hmult_spds_col_stored / Hv_stored_20_Hzb
+// (nemo3d/src/base/Hmult_stored.c:73-172, 176-607) and the alpha dot of
+// single_lanczos_iteration (eigen/src/lanczos.c:679-707).
+//
+// Layout: NORB lanes per atom (one lane per orbital, all spins), 32/NORB atoms
+// per warp.  The warp stages its atoms' own and neighbour vector segments in
+// shared memory; each lane then streams its row of every bond block (cation:
+// row of the stored block, anion: column of the neighbour cation's block,
+// i.e. the Hermitian transpose, each bond being stored once).
+#include "tbgpu_internal.cuh"
+#include "reduce.cuh"
+#include "zincblende.cuh"
+
+namespace tbgpu {
+
+__device__ __forceinline__ double2 cmul_r(double v, double2 a) { return make_double2(v * a.x, v * a.y); }
+__device__ __forceinline__ void cfma_r(double2 &acc, double v, double2 a) {
+  acc.x = fma(v, a.x, acc.x);
+  acc.y = fma(v, a.y, acc.y);
+}
+// acc += (i*lambda) * a
+__device__ __forceinline__ void cfma_i(double2 &acc, double lam, double2 a) {
+  acc.x -= lam * a.y;
+  acc.y += lam * a.x;
+}
+
+template <int NORB, int NSPIN, int WPB, bool DOT>
+__global__ void __launch_bounds__(WPB * 32)
+    k_spmv(long natoms, const int4 *__restrict__ nbr, const unsigned char *__restrict__ site_m,
+           const double *__restrict__ onsite, const double *__restrict__ blocks,
+           const double2 *__restrict__ x, double2 *__restrict__ y, double shift,
+           const double *__restrict__ xnorm, int xnorm_idx, double *partial,
+           unsigned int *counter, double *alpha_out, int alpha_idx) {
+  constexpr int NB = NORB * NSPIN;
+  constexpr int APW = 32 / NORB;
+  constexpr int ONS = onsite_len(NB);
+  __shared__ double2 xs[WPB][APW][5][NB];  // slots 0..3 neighbours, 4 own
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int ai = lane / NORB, o = lane - ai * NORB;
+  const long a = (long(blockIdx.x) * WPB + w) * APW + ai;
+  const bool act = ai < APW && a < natoms;
+  const double scale = xnorm ? 1.0 / xnorm[xnorm_idx] : 1.0;
+  int nb[4] = {-1, -1, -1, -1};
+  int m = 0;
+  if (act) {
+    const int4 v = nbr[a];
+    nb[0] = v.x; nb[1] = v.y; nb[2] = v.z; nb[3] = v.w;
+    m = site_m[a];
+#pragma unroll
+    for (int s = 0; s < NSPIN; s++) {
+      const int e = s * NORB + o;
+      xs[w][ai][4][e] = cmul_r(scale, x[a * NB + e]);
+#pragma unroll
+      for (int n = 0; n < 4; n++)
+        xs[w][ai][n][e] = nb[n] >= 0 ? cmul_r(scale, x[long(nb[n]) * NB + e]) : make_double2(0, 0);
+    }
+  }
+  __syncwarp();
+  double dot = 0.0;
+  if (act) {
+    const double *rec = onsite + a * ONS;
+    double2 acc[NSPIN];
+#pragma unroll
+    for (int s = 0; s < NSPIN; s++) acc[s] = cmul_r(rec[s * NORB + o], xs[w][ai][4][s * NORB + o]);
+    // dangling-bond sp3 couplings among s, px, py, pz (surface atoms only)
+    if (o >= 1 && o <= 4 && rec[NB + 1] != 0.0) {
+      const double sx = rec[NB + 2], sy = rec[NB + 3], sz = rec[NB + 4];
+      const double xy = rec[NB + 5], xz = rec[NB + 6], yz = rec[NB + 7];
+      double c1, c2, c3;
+      int k1, k2, k3;
+      if (o == 1) { c1 = sx; k1 = 2; c2 = sy; k2 = 3; c3 = sz; k3 = 4; }
+      else if (o == 2) { c1 = sx; k1 = 1; c2 = xy; k2 = 3; c3 = xz; k3 = 4; }
+      else if (o == 3) { c1 = sy; k1 = 1; c2 = xy; k2 = 2; c3 = yz; k3 = 4; }
+      else { c1 = sz; k1 = 1; c2 = xz; k2 = 2; c3 = yz; k3 = 3; }
+#pragma unroll
+      for (int s = 0; s < NSPIN; s++) {
+        cfma_r(acc[s], c1, xs[w][ai][4][s * NORB + k1]);
+        cfma_r(acc[s], c2, xs[w][ai][4][s * NORB + k2]);
+        cfma_r(acc[s], c3, xs[w][ai][4][s * NORB + k3]);
+      }
+    }
+    // on-site spin-orbit (mb_ham_spds_so.h), p orbitals 2,3,4 of both spins
+    if (NSPIN == 2 && o >= 2 && o <= 4) {
+      const double L = rec[NB];
+      const double2 *U = xs[w][ai][4], *D = xs[w][ai][4] + NORB;
+      if (o == 2) {
+        cfma_i(acc[0], -L, U[3]); cfma_r(acc[0], L, D[4]);
+        cfma_i(acc[1], L, D[3]);  cfma_r(acc[1], -L, U[4]);
+      } else if (o == 3) {
+        cfma_i(acc[0], L, U[2]);  cfma_i(acc[0], -L, D[4]);
+        cfma_i(acc[1], -L, D[2]); cfma_i(acc[1], -L, U[4]);
+      } else {
+        cfma_r(acc[0], -L, D[2]); cfma_i(acc[0], L, D[3]);
+        cfma_r(acc[1], L, U[2]);  cfma_i(acc[1], L, U[3]);
+      }
+    }
+    // bonds
+    const bool cat = m < 4;
+#pragma unroll
+    for (int n = 0; n < 4; n++) {
+      if (nb[n] < 0) continue;
+      const double2 *xn = xs[w][ai][n];
+      if (cat) {
+        const double *M = blocks + (a * 4 + n) * (NORB * NORB) + o * NORB;
+        double r[NORB];
+        if constexpr (NORB % 2 == 0) {
+          // rows start on 16-byte boundaries when NORB is even (block = NORB^2
+          // doubles, row = NORB doubles): 128-bit loads
+#pragma unroll
+          for (int k = 0; k < NORB; k += 2) {
+            const double2 t = __ldg(reinterpret_cast<const double2 *>(M + k));
+            r[k] = t.x;
+            r[k + 1] = t.y;
+          }
+        } else {
+#pragma unroll
+          for (int k = 0; k < NORB; k++) r[k] = __ldg(M + k);
+        }
+#pragma unroll
+        for (int k = 0; k < NORB; k++)
+#pragma unroll
+          for (int s = 0; s < NSPIN; s++) cfma_r(acc[s], r[k], xn[s * NORB + k]);
+      } else {
+        const double *M = blocks + (long(nb[n]) * 4 + c_rev_slot[m][n]) * (NORB * NORB) + o;
+#pragma unroll
+        for (int k = 0; k < NORB; k++) {
+          const double v = __ldg(M + k * NORB);
+#pragma unroll
+          for (int s = 0; s < NSPIN; s++) cfma_r(acc[s], v, xn[s * NORB + k]);
+        }
+      }
+    }
+#pragma unroll
+    for (int s = 0; s < NSPIN; s++) {
+      const double2 xo = xs[w][ai][4][s * NORB + o];
+      double2 out = make_double2(acc[s].x - shift * xo.x, acc[s].y - shift * xo.y);
+      y[a * NB + s * NORB + o] = out;
+      dot += xo.x * out.x + xo.y * out.y;
+    }
+  }
+  if (DOT) grid_reduce<WPB * 32>(dot, partial, counter, alpha_out, alpha_idx, false);
+}
+
+constexpr int kWPB = 8;
+
+template <int NORB, int NSPIN>
+static int launch_t(Ctx &c, const double *x, double *y, double shift,
+                    const double *xnorm, int xidx, double *alpha_out, int aidx,
+                    cudaStream_t s) {
+  constexpr int APW = 32 / NORB;
+  const long per_block = long(kWPB) * APW;
+  const unsigned grid = unsigned((c.natoms + per_block - 1) / per_block);
+  const double2 *X = reinterpret_cast<const double2 *>(x);
+  double2 *Y = reinterpret_cast<double2 *>(y);
+  if (alpha_out) {
+    int rc = ensure_partials(c, int(grid));
+    if (rc) return rc;
+    k_spmv<NORB, NSPIN, kWPB, true><<<grid, kWPB * 32, 0, s>>>(
+        c.natoms, c.d_nbr, c.d_site_m, c.d_onsite, c.d_blocks, X, Y, shift, xnorm, xidx,
+        c.d_partial, c.d_counter, alpha_out, aidx);
+  } else {
+    k_spmv<NORB, NSPIN, kWPB, false><<<grid, kWPB * 32, 0, s>>>(
+        c.natoms, c.d_nbr, c.d_site_m, c.d_onsite, c.d_blocks, X, Y, shift, xnorm, xidx,
+        nullptr, nullptr, nullptr, 0);
+  }
+  TB_CUDA(cudaGetLastError());
+  return TBGPU_OK;
+}
+
+int launch_spmv(Ctx &c, const double *x, double *y, double shift, const double *xnorm,
+                int xidx, double *alpha_out, int aidx, cudaStream_t s) {
+  if (c.norb == 10 && c.nspin == 2) return launch_t<10, 2>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
+  if (c.norb == 10 && c.nspin == 1) return launch_t<10, 1>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
+  if (c.norb == 5 && c.nspin == 2) return launch_t<5, 2>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
+  if (c.norb == 5 && c.nspin == 1) return launch_t<5, 1>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
+  return set_error(TBGPU_E_UNSUPPORTED);
+}
+
+}  // namespace tbgpu

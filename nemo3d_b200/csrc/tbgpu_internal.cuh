@@ -1,0 +1,107 @@
+// Internal definitions shared by the libtbgpu.so translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "../../include/tbgpu.h"
+
+namespace tbgpu {
+
+// The reference's sqrt(3) (nemo3d/src/ham/mb_ham_spds_micro.c:42).  Kept so
+// that Hamiltonian entries agree with the reference to 1e-12.
+constexpr double kSqr3 = 1.73205080757;
+
+constexpr int kNPV = 35;
+constexpr int kNPAR = TBGPU_NPAR;
+
+// parameter-vector indices (nemo3d/src/ham/mb_ham_spds_micro.h:100-264)
+enum : int {
+  pE_sa = 0, pE_pa = 1, pE_sc = 2, pE_pc = 3, pE_sta = 4, pE_stc = 5,
+  pE_da = 6, pE_dc = 7, pE_La = 8, pE_Lc = 9, pA0 = 31
+};
+enum : int {
+  eta_ssts = 0, eta_ststs, eta_sss, eta_sps, eta_pps, eta_ppp, eta_sds,
+  eta_stps, eta_pds, eta_pdp, eta_const, eta_dds, eta_ddp, eta_ddd, eta_stds,
+  eta_cat_shift, eta_an_shift
+};
+
+// per-atom on-site record (doubles): [0,nb) diagonal, [nb] spin-orbit
+// lambda, [nb+1] passivated flag, [nb+2, nb+8) dangling-bond sp3 couplings
+// (s-x, s-y, s-z, x-y, x-z, y-z); padded to a multiple of 8 doubles.
+__host__ __device__ constexpr int onsite_len(int nb) { return ((nb + 8 + 7) / 8) * 8; }
+
+struct Timer {
+  cudaEvent_t a = nullptr, b = nullptr;
+};
+
+struct Ctx {
+  // model
+  int band_model = 0, norb = 0, nspin = 0, nb = 0, ons = 0;
+  int include_strain = 1, passivate = 1;
+  double dangling_shift = 0.0;
+  int nspecies = 0;
+  // geometry
+  int nx = 0, ny = 0, nz = 0;
+  int periodic[3] = {0, 0, 0};
+  double lattice[3] = {0, 0, 0};
+  long nsites = 0;
+  long natoms = 0;
+  bool built = false;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  // device arrays
+  unsigned char *d_type = nullptr;  // [nsites]
+  double *d_dsp = nullptr;          // [nsites*3] or null
+  double *d_par = nullptr;          // [ns*ns*NPAR]
+  unsigned char *d_par_ok = nullptr;
+  int *d_site_index = nullptr;      // [nsites] atom index or -1
+  int *d_atom_site = nullptr;       // [natoms]
+  int4 *d_nbr = nullptr;            // [natoms]
+  unsigned char *d_site_m = nullptr;// [natoms] in-cell site 0..7
+  unsigned char *d_surface = nullptr;
+  double *d_onsite = nullptr;       // [natoms*ons]
+  double *d_blocks = nullptr;       // [natoms*4*norb*norb], cation atoms
+  // reduction scratch (per-block partials + completion counter)
+  double *d_partial = nullptr;
+  unsigned int *d_counter = nullptr;
+  int partial_cap = 0;
+  int *d_status = nullptr;          // device error word
+  // Lanczos state
+  std::vector<double> alpha, beta;  // host copy of the last tridiagonal
+  // stats
+  tbgpu_stats stats{};
+  bool profiling = false;
+  // scratch for the host-pointer matvec
+  double *d_x = nullptr, *d_y = nullptr;
+};
+
+// error helpers
+int set_error(int code);
+#define TB_CUDA(call)                                              \
+  do {                                                             \
+    cudaError_t e_ = (call);                                       \
+    if (e_ != cudaSuccess) return ::tbgpu::set_error(TBGPU_E_CUDA); \
+  } while (0)
+
+// topology.cu
+int build_topology(Ctx &c);
+// build.cu
+int assemble(Ctx &c);
+// spmv.cu
+int launch_spmv(Ctx &c, const double *x, double *y, double shift,
+                const double *xscale_dev, int scale_index, double *alpha_out,
+                int alpha_index, cudaStream_t s);
+// lanczos.cu
+int ensure_partials(Ctx &c, int nblocks);
+struct SolveArgs {
+  int conv_start, conv_skip, imax, req1, req2;
+  double emin1, emax1, emin2, emax2, tol;
+};
+int solve(Ctx &c, const SolveArgs &A, const double *r0_dev, double *values, int *conv_iters,
+          int *iterations, double *V_dev, int maxvec);
+
+}  // namespace tbgpu

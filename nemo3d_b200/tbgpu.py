@@ -1,0 +1,296 @@
+"""Python front end of libtbgpu.so, mirroring the reference's entry points.
+
+The reference drives its eigensolver from C: ``setup_hamiltonian`` builds the
+structure, the ``matmul`` function pointer (``matvect_mult``) applies H and
+``eigensolve_lanczos`` runs the solver (nemo3d/src/base/eigsys3d_par.c:217-405,
+eigen/src/lanczos.c:1823-2089).  ``Hamiltonian`` wraps one libtbgpu context
+with the same three operations and the same argument meaning; failures raise
+``TbgpuError`` carrying the library's status code.  There is no CPU path: if
+the CUDA library or a GPU is missing, construction fails.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import materials as _mat
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libtbgpu.so")
+
+BAND_MODEL_IDS = {"sp3s*": 1, "sp3s*_so": 2, "sp3d5s*": 3, "sp3d5s*_so": 4}
+NPAR = 68
+
+
+class TbgpuError(RuntimeError):
+    def __init__(self, code: int, where: str):
+        self.code = code
+        msg = _lib().tbgpu_error_string(code).decode() if _LIB else str(code)
+        super().__init__(f"{where}: {msg} (code {code})")
+
+
+class _Geom(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+                ("periodic", C.c_int * 3), ("lattice", C.c_double * 3),
+                ("type", C.c_void_p), ("dsp", C.c_void_p)]
+
+
+class _Model(C.Structure):
+    _fields_ = [("band_model", C.c_int), ("include_strain", C.c_int),
+                ("passivate", C.c_int), ("dangling_shift", C.c_double),
+                ("nspecies", C.c_int), ("par", C.c_void_p), ("par_ok", C.c_void_p)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("build_ms", C.c_double), ("solve_ms", C.c_double),
+                ("vectors_ms", C.c_double), ("spmv_ms", C.c_double),
+                ("spmv_launches", C.c_long), ("lanczos_iterations", C.c_long),
+                ("kernel_launches", C.c_long)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_LIB = None
+
+
+def _lib():
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: run nemo3d_b200.build.build() "
+                               "(the CUDA library is required; there is no CPU path)")
+        L = C.CDLL(LIB_PATH)
+        vp, ip, dp = C.c_void_p, C.c_int, C.c_double
+        L.tbgpu_error_string.restype = C.c_char_p
+        L.tbgpu_error_string.argtypes = [ip]
+        L.tbgpu_prepare_params.argtypes = [ip, ip, vp, vp, dp, dp, vp]
+        L.tbgpu_ctx_create.argtypes = [C.POINTER(_Geom), C.POINTER(_Model), C.POINTER(vp)]
+        L.tbgpu_ctx_create_dev.argtypes = [C.POINTER(_Geom), C.POINTER(_Model), C.POINTER(vp)]
+        L.tbgpu_ctx_destroy.argtypes = [vp]
+        L.tbgpu_set_stream.argtypes = [vp, vp]
+        L.tbgpu_build_hamiltonian.argtypes = [vp]
+        L.tbgpu_num_atoms.restype = C.c_long
+        L.tbgpu_num_atoms.argtypes = [vp]
+        L.tbgpu_dimension.restype = C.c_long
+        L.tbgpu_dimension.argtypes = [vp]
+        L.tbgpu_matvect_mult.restype = None
+        L.tbgpu_matvect_mult.argtypes = [C.POINTER(vp), vp, vp]
+        L.tbgpu_hx_dev.argtypes = [vp, dp, vp, vp]
+        L.tbgpu_eigensolve_lanczos.argtypes = [vp, ip, ip, ip, ip, ip, dp, dp, dp, dp, dp,
+                                               vp, vp, vp, vp, vp, ip]
+        L.tbgpu_eigensolve_lanczos_dev.argtypes = [vp, ip, ip, ip, ip, ip, dp, dp, dp, dp,
+                                                   dp, vp, vp, vp, vp, vp, ip]
+        L.tbgpu_get_tridiagonal.argtypes = [vp, vp, vp, ip]
+        L.tbgpu_export_pattern.argtypes = [vp, vp, vp, vp]
+        L.tbgpu_export_hamiltonian.argtypes = [vp, vp, vp]
+        L.tbgpu_set_profiling.argtypes = [vp, ip]
+        L.tbgpu_get_stats.argtypes = [vp, C.POINTER(Stats)]
+        _LIB = L
+    return _LIB
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def prepare_params(mat: dict, include_strain: bool = True) -> np.ndarray:
+    """param_init for one material set (nemo3d/src/base/mat3d.c:133-307)."""
+    out = np.zeros(NPAR)
+    pv = np.zeros(35)
+    pv[:len(mat["pv"])] = mat["pv"]
+    st = np.asarray(mat["strain"], np.float64)
+    rc = _lib().tbgpu_prepare_params(int(mat["family"] == "sp3s*"), int(include_strain),
+                                     _p(pv), _p(st), float(mat["ev_offset"]),
+                                     float(mat["a0"]), _p(out))
+    if rc:
+        raise TbgpuError(rc, "prepare_params")
+    return out
+
+
+def param_table(mats, include_strain=True, nspecies=8):
+    par = np.zeros((nspecies, nspecies, NPAR))
+    ok = np.zeros((nspecies, nspecies), np.uint8)
+    for m in mats:
+        c, a = _mat.SPECIES[m["cation"]], _mat.SPECIES[m["anion"]]
+        par[c, a] = prepare_params(m, include_strain)
+        ok[c, a] = 1
+    return par, ok
+
+
+class Hamiltonian:
+    """A structure's tight-binding Hamiltonian on the GPU (one libtbgpu context).
+
+    ``structure``: a ``workloads.Structure``; ``model``: one of
+    ``materials.BAND_MODELS``; ``materials``: parameter sets (default: every
+    shipped set of the model's family).
+    """
+
+    def __init__(self, structure, model="sp3d5s*_so", materials=None, include_strain=True,
+                 passivate=True, dangling_shift=30.0, device_inputs=None, build=True):
+        L = _lib()
+        self.structure = structure
+        self.model = model
+        self.norb, self.nspin = _mat.BAND_MODELS[model]
+        self.nb = self.norb * self.nspin
+        mats = materials if materials is not None else _mat.materials_for(model)
+        if isinstance(mats, dict):
+            mats = [mats]
+        self._par, self._ok = param_table(mats, include_strain)
+        g = _Geom()
+        g.nx, g.ny, g.nz = structure.nx, structure.ny, structure.nz
+        g.periodic[:] = [int(bool(v)) for v in structure.periodic]
+        g.lattice[:] = list(structure.lattice)
+        m = _Model()
+        m.band_model = BAND_MODEL_IDS[model]
+        m.include_strain, m.passivate = int(include_strain), int(passivate)
+        m.dangling_shift = float(dangling_shift)
+        m.nspecies = self._par.shape[0]
+        m.par, m.par_ok = _p(self._par), _p(self._ok)
+        ctx = C.c_void_p()
+        if device_inputs is not None:  # (type_dev_ptr, dsp_dev_ptr or 0)
+            g.type, g.dsp = device_inputs[0], (device_inputs[1] or None)
+            rc = L.tbgpu_ctx_create_dev(C.byref(g), C.byref(m), C.byref(ctx))
+        else:
+            self._types = np.ascontiguousarray(structure.types, np.uint8)
+            self._dsp = (None if structure.dsp is None
+                         else np.ascontiguousarray(structure.dsp, np.float64))
+            g.type, g.dsp = _p(self._types), _p(self._dsp)
+            rc = L.tbgpu_ctx_create(C.byref(g), C.byref(m), C.byref(ctx))
+        if rc:
+            raise TbgpuError(rc, "tbgpu_ctx_create")
+        self._ctx = ctx
+        self._built = False
+        if build:
+            self.build()
+
+    # -- lifecycle --------------------------------------------------------
+    def close(self):
+        if getattr(self, "_ctx", None):
+            _lib().tbgpu_ctx_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr: int):
+        rc = _lib().tbgpu_set_stream(self._ctx, C.c_void_p(stream_ptr))
+        if rc:
+            raise TbgpuError(rc, "tbgpu_set_stream")
+
+    def build(self):
+        rc = _lib().tbgpu_build_hamiltonian(self._ctx)
+        if rc:
+            raise TbgpuError(rc, "tbgpu_build_hamiltonian")
+        self._built = True
+        self.natoms = int(_lib().tbgpu_num_atoms(self._ctx))
+        self.n = int(_lib().tbgpu_dimension(self._ctx))
+
+    # -- H x ----------------------------------------------------------------
+    def matvect_mult(self, x: np.ndarray, shift: float = 0.0) -> np.ndarray:
+        """y = (H - shift) x through the reference's matmul signature."""
+        x = np.ascontiguousarray(x, np.float64)
+        if x.size != 2 * self.n:
+            raise ValueError("x must hold 2*dimension doubles (interleaved complex)")
+        y = np.empty_like(x)
+        sh = C.c_double(shift)
+        args = (C.c_void_p * 3)(self._ctx.value, C.cast(C.pointer(sh), C.c_void_p).value, None)
+        L = _lib()
+        L.tbgpu_matvect_mult(args, _p(y), _p(x))
+        rc = L.tbgpu_last_error()
+        if rc:
+            raise TbgpuError(rc, "tbgpu_matvect_mult")
+        return y
+
+    def hx_dev(self, x_ptr: int, y_ptr: int, shift: float = 0.0):
+        rc = _lib().tbgpu_hx_dev(self._ctx, float(shift), C.c_void_p(x_ptr), C.c_void_p(y_ptr))
+        if rc:
+            raise TbgpuError(rc, "tbgpu_hx_dev")
+
+    # -- eigensolver ----------------------------------------------------------
+    def eigensolve_lanczos(self, r_0, ConvCheckStartIter=200, ConvCheckSkipRate=50,
+                           imax=2400, requested1=1, requested2=1, emin1=-0.6, emax1=0.2,
+                           emin2=1.4, emax2=2.0, tolerance=1e-7, vectors=0):
+        """Lanczos with the reference's parameters (eigensolve_lanczos).
+
+        r_0: host start vector (2*dimension doubles).  Returns a dict with
+        ``values`` (ascending), ``conv_iterations``, ``iterations`` and, when
+        ``vectors`` > 0, ``vectors`` (complex, [k, dimension])."""
+        r0 = np.ascontiguousarray(r_0, np.float64)
+        if r0.size != 2 * self.n:
+            raise ValueError("r_0 must hold 2*dimension doubles")
+        vals = np.zeros(imax)
+        cit = np.zeros(imax, np.int32)
+        its = np.zeros(1, np.int32)
+        V = np.zeros((vectors, 2 * self.n)) if vectors else None
+        ne = _lib().tbgpu_eigensolve_lanczos(
+            self._ctx, ConvCheckStartIter, ConvCheckSkipRate, imax, requested1, requested2,
+            emin1, emax1, emin2, emax2, tolerance, _p(r0), _p(vals), _p(cit), _p(its),
+            _p(V), int(vectors))
+        if ne < 0:
+            raise TbgpuError(ne, "tbgpu_eigensolve_lanczos")
+        out = dict(values=vals[:ne].copy(), conv_iterations=cit[:ne].copy(),
+                   iterations=int(its[0]))
+        if vectors:
+            k = min(ne, vectors)
+            v = V[:k].reshape(k, self.n, 2)
+            out["vectors"] = v[..., 0] + 1j * v[..., 1]
+        return out
+
+    def eigensolve_lanczos_dev(self, r0_ptr: int, vectors_ptr: int = 0, max_vectors: int = 0,
+                               ConvCheckStartIter=200, ConvCheckSkipRate=50, imax=2400,
+                               requested1=1, requested2=1, emin1=-0.6, emax1=0.2, emin2=1.4,
+                               emax2=2.0, tolerance=1e-7):
+        vals = np.zeros(imax)
+        cit = np.zeros(imax, np.int32)
+        its = np.zeros(1, np.int32)
+        ne = _lib().tbgpu_eigensolve_lanczos_dev(
+            self._ctx, ConvCheckStartIter, ConvCheckSkipRate, imax, requested1, requested2,
+            emin1, emax1, emin2, emax2, tolerance, C.c_void_p(r0_ptr), _p(vals), _p(cit),
+            _p(its), C.c_void_p(vectors_ptr or None), int(max_vectors))
+        if ne < 0:
+            raise TbgpuError(ne, "tbgpu_eigensolve_lanczos_dev")
+        return dict(values=vals[:ne].copy(), conv_iterations=cit[:ne].copy(),
+                    iterations=int(its[0]))
+
+    def tridiagonal(self, cap=100000):
+        a = np.zeros(cap)
+        b = np.zeros(cap)
+        n = _lib().tbgpu_get_tridiagonal(self._ctx, _p(a), _p(b), cap)
+        if n < 0:
+            raise TbgpuError(n, "tbgpu_get_tridiagonal")
+        return a[:n].copy(), b[:n].copy()
+
+    # -- exports ----------------------------------------------------------------
+    def export_pattern(self):
+        site = np.zeros(self.natoms, np.int32)
+        nbr = np.zeros(self.natoms * 4, np.int32)
+        surf = np.zeros(self.natoms, np.uint8)
+        rc = _lib().tbgpu_export_pattern(self._ctx, _p(site), _p(nbr), _p(surf))
+        if rc:
+            raise TbgpuError(rc, "tbgpu_export_pattern")
+        return site, nbr, surf
+
+    def export_hamiltonian(self):
+        ons = np.zeros(self.natoms * self.nb * self.nb * 2)
+        blk = np.zeros(self.natoms * 4 * self.norb * self.norb)
+        rc = _lib().tbgpu_export_hamiltonian(self._ctx, _p(ons), _p(blk))
+        if rc:
+            raise TbgpuError(rc, "tbgpu_export_hamiltonian")
+        return ons, blk
+
+    def set_profiling(self, on=True):
+        _lib().tbgpu_set_profiling(self._ctx, int(bool(on)))
+
+    def stats(self) -> dict:
+        s = Stats()
+        rc = _lib().tbgpu_get_stats(self._ctx, C.byref(s))
+        if rc:
+            raise TbgpuError(rc, "tbgpu_get_stats")
+        return s.as_dict()
