@@ -44,6 +44,7 @@ extern "C" {
 #define TBGPU_E_STATE (-5)        /* call out of order (e.g. H not built)     */
 #define TBGPU_E_UNSUPPORTED (-6)  /* option not supported by this build       */
 #define TBGPU_E_NUMERIC (-7)      /* breakdown (beta = 0, zero pivot, NaN)    */
+#define TBGPU_E_TIMEOUT (-8)      /* a bounded device-side wait ran out       */
 
 /* band models: orbitals per spin x spins (mb_ham_spds_micro2.h:43-48) */
 #define TBGPU_SP3S 1          /* 5 x 1: spin-up block of Bands_10_sp3ss_spin   */
@@ -167,6 +168,12 @@ int tbgpu_export_pattern(const tbgpu_ctx *ctx, int *atom_site, int *nbr,
  * blocks[c][a] = <anion orbital a | H | cation orbital c>. */
 int tbgpu_export_hamiltonian(const tbgpu_ctx *ctx, double *onsite,
                              double *blocks);
+
+/* H*x kernel: 0 = default (warp-staged cp.async kernel, 14 warps x 1 stage
+ * per SM, for the 10-orbital models; lane-gather kernel otherwise),
+ * 1 = lane-gather kernel for every model, 2 = warp-staged kernel with
+ * 7 warps x 2 stages. */
+int tbgpu_set_spmv_variant(tbgpu_ctx *ctx, int variant);
 
 /* Timing of the last solve / build (ms, CUDA events on the context stream). */
 typedef struct {

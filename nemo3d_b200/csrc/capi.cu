@@ -172,6 +172,7 @@ int tbgpu_hx_dev(tbgpu_ctx *ctx, double shift, const double *x_dev, double *y_de
 }
 
 void tbgpu_matvect_mult(const int **argList, tbgpu_dcomplex *y, const tbgpu_dcomplex *x) {
+  set_error(TBGPU_OK);  // void entry point: status is read back via tbgpu_last_error
   if (!argList || !argList[0] || !x || !y) {
     set_error(TBGPU_E_ARG);
     return;
@@ -313,6 +314,12 @@ int tbgpu_export_hamiltonian(const tbgpu_ctx *ctx, double *onsite, double *block
   return TBGPU_OK;
 }
 
+int tbgpu_set_spmv_variant(tbgpu_ctx *ctx, int variant) {
+  if (!ctx || variant < 0 || variant > 2) return set_error(TBGPU_E_ARG);
+  C(ctx)->spmv_variant = variant;
+  return TBGPU_OK;
+}
+
 int tbgpu_set_profiling(tbgpu_ctx *ctx, int on) {
   if (!ctx) return set_error(TBGPU_E_ARG);
   C(ctx)->profiling = on != 0;
@@ -337,6 +344,7 @@ const char *tbgpu_error_string(int code) {
     case TBGPU_E_STATE: return "call out of order";
     case TBGPU_E_UNSUPPORTED: return "unsupported option";
     case TBGPU_E_NUMERIC: return "numerical breakdown";
+    case TBGPU_E_TIMEOUT: return "a bounded device-side wait ran out";
     default: return "unknown error";
   }
 }

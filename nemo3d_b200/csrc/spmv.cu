@@ -172,6 +172,8 @@ static int launch_t(Ctx &c, const double *x, double *y, double shift,
 
 int launch_spmv(Ctx &c, const double *x, double *y, double shift, const double *xnorm,
                 int xidx, double *alpha_out, int aidx, cudaStream_t s) {
+  if (c.norb == 10 && c.spmv_variant != 1)
+    return launch_spmv_async(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
   if (c.norb == 10 && c.nspin == 2) return launch_t<10, 2>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
   if (c.norb == 10 && c.nspin == 1) return launch_t<10, 1>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
   if (c.norb == 5 && c.nspin == 2) return launch_t<5, 2>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);

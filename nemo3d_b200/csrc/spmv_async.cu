@@ -1,0 +1,333 @@
+// H*x for the 10-orbital (sp3d5s*) models with asynchronous 16-byte gathers.
+//
+// Same product as k_spmv (spmv.cu; restates Hv_stored_20_Hzb,
+// nemo3d/src/base/Hmult_stored.c:176-607, with the Lanczos alpha dot of
+// eigen/src/lanczos.c:679-707 fused).  Each warp owns a private
+// shared-memory stage (one or two) holding, for three atoms, the four bond
+// blocks (a cation's own 3200-byte run, or the four 800-byte blocks stored
+// by an anion's cation neighbours), the own and four neighbour vector
+// segments and the on-site record (5056 bytes per atom).  The warp fills a
+// stage with coalesced 16-byte cp.async copies (one instruction moves 512
+// bytes, nothing is held in registers) and computes it, one lane per orbital
+// row, from shared memory; with one stage per warp, the other warps of the
+// SM cover its wait, with two it also overlaps its own next copies.  Groups of three atoms
+// are dealt to warps in order, so all SMs sweep the atom order together and
+// the blocks an anion reads transposed (stored once, by the cation) are
+// still in L2 when they are needed the second time.
+//
+// (A variant that gathered the same bytes with one 1-D TMA bulk copy per
+// 300-800-byte segment took 2.4 ms per launch on the 1.02M-atom dot: that
+// many small requests are limited by the TMA request rate, not by HBM.)
+#include <cstdint>
+
+#include "tbgpu_internal.cuh"
+#include "reduce.cuh"
+#include "zincblende.cuh"
+
+namespace tbgpu {
+
+namespace {
+
+constexpr int kNorb = 10;
+constexpr int kAPW = 3;      // atoms per warp
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void cp16(void *dst, const void *src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+__device__ __forceinline__ void cfma_r(double2 &acc, double v, double2 a) {
+  acc.x = fma(v, a.x, acc.x);
+  acc.y = fma(v, a.y, acc.y);
+}
+__device__ __forceinline__ void cfma_i(double2 &acc, double lam, double2 a) {
+  acc.x -= lam * a.y;
+  acc.y += lam * a.x;
+}
+
+template <int NSPIN, int WARPS, int STAGES>
+struct Layout {
+  static constexpr int NB = kNorb * NSPIN;
+  static constexpr int ONS = onsite_len(NB);
+  static constexpr int BLK = kNorb * kNorb;      // doubles per bond block
+  static constexpr int BLK_CH = BLK * 8 / 16;    // 16-byte chunks per block (50)
+  static constexpr int X_CH = NB * 16 / 16;      // chunks per vector segment
+  static constexpr int ONS_CH = ONS * 8 / 16;    // chunks per on-site record
+  // per-atom stride, padded by 48 bytes so the three atoms of a warp start
+  // on different shared-memory banks
+  static constexpr int ATOM = 4 * BLK * 8 + 5 * NB * 16 + ONS * 8 + 48;
+  static constexpr int STAGE = kAPW * ATOM;
+  static constexpr int WARP = STAGES * STAGE;
+  static constexpr int SMEM = WARPS * WARP;
+  static __device__ __forceinline__ int blk(int i) { return i * ATOM; }
+  static __device__ __forceinline__ int xs(int i) { return i * ATOM + 4 * BLK * 8; }
+  static __device__ __forceinline__ int ons(int i) { return i * ATOM + 4 * BLK * 8 + 5 * NB * 16; }
+};
+
+struct Meta {
+  int nb[kAPW][4];
+  int m[kAPW];  // -1: no atom
+};
+
+__device__ __forceinline__ Meta load_meta(long g, long natoms, const int4 *__restrict__ nbr,
+                                          const unsigned char *__restrict__ site_m) {
+  Meta M;
+#pragma unroll
+  for (int i = 0; i < kAPW; i++) {
+    const long a = g * kAPW + i;
+    if (a < natoms) {
+      const int4 v = __ldg(nbr + a);
+      M.nb[i][0] = v.x; M.nb[i][1] = v.y; M.nb[i][2] = v.z; M.nb[i][3] = v.w;
+      M.m[i] = __ldg(site_m + a);
+    } else {
+      M.nb[i][0] = M.nb[i][1] = M.nb[i][2] = M.nb[i][3] = -1;
+      M.m[i] = -1;
+    }
+  }
+  return M;
+}
+
+// Issue the copies of group g into one stage (all lanes; no wait).
+template <class L>
+__device__ __forceinline__ void issue(unsigned char *st, long g, const Meta &M, int lane,
+                                      const double *__restrict__ onsite,
+                                      const double *__restrict__ blocks,
+                                      const double2 *__restrict__ x) {
+  constexpr int NB = L::NB;
+#pragma unroll
+  for (int i = 0; i < kAPW; i++) {
+    const int m = M.m[i];
+    if (m < 0) continue;
+    const long a = g * kAPW + i;
+    const bool cat = m < 4;
+    unsigned char *bk = st + L::blk(i);
+    if (cat) {  // the cation's four blocks are one contiguous run
+      const unsigned char *src = reinterpret_cast<const unsigned char *>(blocks + a * 4 * L::BLK);
+#pragma unroll
+      for (int c = lane; c < 4 * L::BLK_CH; c += 32) cp16(bk + c * 16, src + c * 16);
+    } else {
+#pragma unroll
+      for (int n = 0; n < 4; n++) {
+        const int b = M.nb[i][n];
+        if (b < 0) continue;
+        const unsigned char *src = reinterpret_cast<const unsigned char *>(
+            blocks + (long(b) * 4 + c_rev_slot[m][n]) * L::BLK);
+#pragma unroll
+        for (int c = lane; c < L::BLK_CH; c += 32) cp16(bk + n * L::BLK * 8 + c * 16, src + c * 16);
+      }
+    }
+    unsigned char *xs = st + L::xs(i);
+    // own segment in slot 4, neighbours in slots 0..3; one lane per chunk
+    if (lane < L::X_CH) {
+      cp16(xs + 4 * NB * 16 + lane * 16, reinterpret_cast<const unsigned char *>(x + a * NB) + lane * 16);
+#pragma unroll
+      for (int n = 0; n < 4; n++) {
+        const int b = M.nb[i][n];
+        if (b >= 0)
+          cp16(xs + n * NB * 16 + lane * 16,
+               reinterpret_cast<const unsigned char *>(x + long(b) * NB) + lane * 16);
+      }
+    }
+    if (lane < L::ONS_CH)
+      cp16(st + L::ons(i) + lane * 16,
+           reinterpret_cast<const unsigned char *>(onsite + a * L::ONS) + lane * 16);
+  }
+}
+
+template <int NSPIN, bool DOT, int WARPS, int STAGES>
+__global__ void __launch_bounds__(WARPS * 32, 1)
+    k_spmv_async(long natoms, long ngroups, const int4 *__restrict__ nbr,
+                 const unsigned char *__restrict__ site_m, const double *__restrict__ onsite,
+                 const double *__restrict__ blocks, const double2 *__restrict__ x,
+                 double2 *__restrict__ y, double shift, const double *__restrict__ xnorm,
+                 int xnorm_idx, double *partial, unsigned int *counter, double *alpha_out,
+                 int alpha_idx) {
+  using L = Layout<NSPIN, WARPS, STAGES>;
+  constexpr int NB = L::NB;
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  unsigned char *wbase = smem + warp * L::WARP;
+  const int ai = lane / kNorb, o = lane - ai * kNorb;
+  const double scale = xnorm ? 1.0 / xnorm[xnorm_idx] : 1.0;
+  double dot = 0.0;
+  const long nw = long(gridDim.x) * WARPS;
+  long g = long(blockIdx.x) * WARPS + warp;
+  // prologue: copies of the first group in flight, metadata of the next
+  Meta cur = load_meta(g, natoms, nbr, site_m);
+  if (STAGES > 1 && g < ngroups) issue<L>(wbase, g, cur, lane, onsite, blocks, x);
+  cp_commit();
+  Meta nxt = load_meta(g + nw, natoms, nbr, site_m);
+  int k = 0;
+  for (; g < ngroups; g += nw, ++k) {
+    const long gn = g + nw;
+    unsigned char *st = wbase + (k % STAGES) * L::STAGE;
+    if (STAGES > 1) {  // next group's copies overlap this group's compute
+      if (gn < ngroups) issue<L>(wbase + ((k + 1) % STAGES) * L::STAGE, gn, nxt, lane, onsite,
+                                 blocks, x);
+      cp_commit();
+    } else {           // single stage: other warps overlap this one's wait
+      issue<L>(st, g, cur, lane, onsite, blocks, x);
+      cp_commit();
+    }
+    const Meta nn = load_meta(gn + nw, natoms, nbr, site_m);  // two groups ahead
+    if (STAGES > 1) cp_wait<1>(); else cp_wait<0>();  // this lane's copies of g landed
+    __syncwarp();   // ... and every lane's
+    // this lane's atom, selected without indexing the metadata at run time
+    const int m = ai == 0 ? cur.m[0] : ai == 1 ? cur.m[1] : ai == 2 ? cur.m[2] : -1;
+    int nbv[4];
+#pragma unroll
+    for (int n = 0; n < 4; n++)
+      nbv[n] = ai == 0 ? cur.nb[0][n] : ai == 1 ? cur.nb[1][n] : cur.nb[2][n];
+    if (ai < kAPW && m >= 0) {
+      const bool cat = m < 4;
+      const long a = g * kAPW + ai;
+      const double2 *xs = reinterpret_cast<const double2 *>(st + L::xs(ai));
+      const double2 *X0 = xs + 4 * NB;
+      const double *rec = reinterpret_cast<const double *>(st + L::ons(ai));
+      const double *bk = reinterpret_cast<const double *>(st + L::blk(ai));
+      double2 acc[NSPIN];
+#pragma unroll
+      for (int sp = 0; sp < NSPIN; sp++) {
+        const double2 v = X0[sp * kNorb + o];
+        acc[sp] = make_double2(rec[sp * kNorb + o] * v.x, rec[sp * kNorb + o] * v.y);
+      }
+      if (o >= 1 && o <= 4 && rec[NB + 1] != 0.0) {  // dangling-bond sp3 couplings
+        const double sx = rec[NB + 2], sy = rec[NB + 3], sz = rec[NB + 4];
+        const double cxy = rec[NB + 5], cxz = rec[NB + 6], cyz = rec[NB + 7];
+        double c1, c2, c3;
+        int k1, k2, k3;
+        if (o == 1) { c1 = sx; k1 = 2; c2 = sy; k2 = 3; c3 = sz; k3 = 4; }
+        else if (o == 2) { c1 = sx; k1 = 1; c2 = cxy; k2 = 3; c3 = cxz; k3 = 4; }
+        else if (o == 3) { c1 = sy; k1 = 1; c2 = cxy; k2 = 2; c3 = cyz; k3 = 4; }
+        else { c1 = sz; k1 = 1; c2 = cxz; k2 = 2; c3 = cyz; k3 = 3; }
+#pragma unroll
+        for (int sp = 0; sp < NSPIN; sp++) {
+          cfma_r(acc[sp], c1, X0[sp * kNorb + k1]);
+          cfma_r(acc[sp], c2, X0[sp * kNorb + k2]);
+          cfma_r(acc[sp], c3, X0[sp * kNorb + k3]);
+        }
+      }
+      if (NSPIN == 2 && o >= 2 && o <= 4) {  // on-site spin-orbit (mb_ham_spds_so.h)
+        const double Lm = rec[NB];
+        const double2 *U = X0, *D = X0 + kNorb;
+        if (o == 2) {
+          cfma_i(acc[0], -Lm, U[3]); cfma_r(acc[0], Lm, D[4]);
+          cfma_i(acc[NSPIN - 1], Lm, D[3]); cfma_r(acc[NSPIN - 1], -Lm, U[4]);
+        } else if (o == 3) {
+          cfma_i(acc[0], Lm, U[2]); cfma_i(acc[0], -Lm, D[4]);
+          cfma_i(acc[NSPIN - 1], -Lm, D[2]); cfma_i(acc[NSPIN - 1], -Lm, U[4]);
+        } else {
+          cfma_r(acc[0], -Lm, D[2]); cfma_i(acc[0], Lm, D[3]);
+          cfma_r(acc[NSPIN - 1], Lm, U[2]); cfma_i(acc[NSPIN - 1], Lm, U[3]);
+        }
+      }
+      // bonds: one accumulator per neighbour so the four chains are independent
+      double2 part[4][NSPIN];
+#pragma unroll
+      for (int n = 0; n < 4; n++) {
+#pragma unroll
+        for (int sp = 0; sp < NSPIN; sp++) part[n][sp] = make_double2(0.0, 0.0);
+        if (nbv[n] < 0) continue;
+        const double2 *xn = xs + n * NB;
+        const double *Mb = bk + n * L::BLK;
+        double r[kNorb];
+        if (cat) {
+#pragma unroll
+          for (int kk = 0; kk < kNorb; kk += 2) {
+            const double2 t2 = *reinterpret_cast<const double2 *>(Mb + o * kNorb + kk);
+            r[kk] = t2.x;
+            r[kk + 1] = t2.y;
+          }
+        } else {
+#pragma unroll
+          for (int kk = 0; kk < kNorb; kk++) r[kk] = Mb[kk * kNorb + o];
+        }
+#pragma unroll
+        for (int kk = 0; kk < kNorb; kk++)
+#pragma unroll
+          for (int sp = 0; sp < NSPIN; sp++) cfma_r(part[n][sp], r[kk], xn[sp * kNorb + kk]);
+      }
+#pragma unroll
+      for (int sp = 0; sp < NSPIN; sp++) {
+        const double2 bsum = make_double2((part[0][sp].x + part[1][sp].x) + (part[2][sp].x + part[3][sp].x),
+                                          (part[0][sp].y + part[1][sp].y) + (part[2][sp].y + part[3][sp].y));
+        acc[sp].x += bsum.x;
+        acc[sp].y += bsum.y;
+      }
+#pragma unroll
+      for (int sp = 0; sp < NSPIN; sp++) {
+        const double2 xv = X0[sp * kNorb + o];
+        const double2 xo = make_double2(scale * xv.x, scale * xv.y);
+        const double2 out = make_double2(scale * acc[sp].x - shift * xo.x,
+                                         scale * acc[sp].y - shift * xo.y);
+        y[a * NB + sp * kNorb + o] = out;
+        dot += xo.x * out.x + xo.y * out.y;
+      }
+    }
+    __syncwarp();  // stage k is free before the next iteration overwrites it
+    cur = nxt;
+    nxt = nn;
+  }
+  cp_wait<0>();
+  if (DOT) grid_reduce<WARPS * 32>(dot, partial, counter, alpha_out, alpha_idx, false);
+}
+
+template <int NSPIN, bool DOT, int WARPS, int STAGES>
+int launch_async_t(Ctx &c, const double *x, double *y, double shift, const double *xnorm,
+                   int xidx, double *alpha_out, int aidx, cudaStream_t s) {
+  using L = Layout<NSPIN, WARPS, STAGES>;
+  static int sms = 0;
+  if (!sms) {
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device);
+    if (cudaFuncSetAttribute(k_spmv_async<NSPIN, DOT, WARPS, STAGES>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM) != cudaSuccess)
+      return set_error(TBGPU_E_CUDA);
+  }
+  const long ngroups = (c.natoms + kAPW - 1) / kAPW;
+  const unsigned grid = unsigned(sms);
+  if (DOT) {
+    int rc = ensure_partials(c, int(grid));
+    if (rc) return rc;
+  }
+  k_spmv_async<NSPIN, DOT, WARPS, STAGES><<<grid, WARPS * 32, L::SMEM, s>>>(
+      c.natoms, ngroups, c.d_nbr, c.d_site_m, c.d_onsite, c.d_blocks,
+      reinterpret_cast<const double2 *>(x), reinterpret_cast<double2 *>(y), shift, xnorm, xidx,
+      DOT ? c.d_partial : nullptr, DOT ? c.d_counter : nullptr, alpha_out, aidx);
+  TB_CUDA(cudaGetLastError());
+  return TBGPU_OK;
+}
+
+}  // namespace
+
+template <int WARPS, int STAGES>
+int launch_cfg(Ctx &c, const double *x, double *y, double shift, const double *xnorm, int xidx,
+               double *alpha_out, int aidx, cudaStream_t s) {
+  if (c.nspin == 2)
+    return alpha_out
+               ? launch_async_t<2, true, WARPS, STAGES>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s)
+               : launch_async_t<2, false, WARPS, STAGES>(c, x, y, shift, xnorm, xidx, nullptr, 0, s);
+  return alpha_out
+             ? launch_async_t<1, true, WARPS, STAGES>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s)
+             : launch_async_t<1, false, WARPS, STAGES>(c, x, y, shift, xnorm, xidx, nullptr, 0, s);
+}
+
+int launch_spmv_async(Ctx &c, const double *x, double *y, double shift, const double *xnorm,
+                      int xidx, double *alpha_out, int aidx, cudaStream_t s) {
+  if (c.norb != kNorb) return set_error(TBGPU_E_UNSUPPORTED);
+  // variant 0: 14 warps x 1 stage per SM (other warps cover a warp's wait;
+  // 0.82 ms per launch on the 1.02M-atom dot); variant 2: 7 warps x 2
+  // stages (each warp overlaps its own next copies; 0.91 ms)
+  if (c.spmv_variant == 2)
+    return launch_cfg<7, 2>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
+  return launch_cfg<14, 1>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
+}
+
+}  // namespace tbgpu

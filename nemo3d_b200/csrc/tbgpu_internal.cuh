@@ -75,6 +75,7 @@ struct Ctx {
   // stats
   tbgpu_stats stats{};
   bool profiling = false;
+  int spmv_variant = 0;
   // scratch for the host-pointer matvec
   double *d_x = nullptr, *d_y = nullptr;
 };
@@ -95,6 +96,10 @@ int assemble(Ctx &c);
 int launch_spmv(Ctx &c, const double *x, double *y, double shift,
                 const double *xscale_dev, int scale_index, double *alpha_out,
                 int alpha_index, cudaStream_t s);
+// spmv_async.cu
+int launch_spmv_async(Ctx &c, const double *x, double *y, double shift,
+                      const double *xscale_dev, int scale_index, double *alpha_out,
+                      int alpha_index, cudaStream_t s);
 // lanczos.cu
 int ensure_partials(Ctx &c, int nblocks);
 struct SolveArgs {

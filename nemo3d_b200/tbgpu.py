@@ -88,6 +88,7 @@ def _lib():
         L.tbgpu_export_pattern.argtypes = [vp, vp, vp, vp]
         L.tbgpu_export_hamiltonian.argtypes = [vp, vp, vp]
         L.tbgpu_set_profiling.argtypes = [vp, ip]
+        L.tbgpu_set_spmv_variant.argtypes = [vp, ip]
         L.tbgpu_get_stats.argtypes = [vp, C.POINTER(Stats)]
         _LIB = L
     return _LIB
@@ -284,6 +285,12 @@ class Hamiltonian:
         if rc:
             raise TbgpuError(rc, "tbgpu_export_hamiltonian")
         return ons, blk
+
+    def set_spmv_variant(self, variant: int):
+        """0: warp-staged cp.async kernel (default, 10 orbitals); 1: lane-gather; 2: 2-stage."""
+        rc = _lib().tbgpu_set_spmv_variant(self._ctx, int(variant))
+        if rc:
+            raise TbgpuError(rc, "tbgpu_set_spmv_variant")
 
     def set_profiling(self, on=True):
         _lib().tbgpu_set_profiling(self._ctx, int(bool(on)))
