@@ -321,7 +321,7 @@ def main():
     ap.add_argument("--profile-case", action="store_true",
                     help="small-case run of the solver kernels for ncu captures")
     ap.add_argument("--profile-iterations", type=int, default=6)
-    ap.add_argument("--ref-iterations", type=int, default=19000,
+    ap.add_argument("--ref-iterations", type=int, default=19002,
                     help="iterations of a full solve (both passes) the CPU sample is scaled to")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))

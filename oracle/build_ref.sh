@@ -1,0 +1,34 @@
+#!/bin/sh
+# build_ref.sh -- TEST INFRASTRUCTURE ONLY.
+#
+# Compiles the reference's Slater-Koster routines
+# (nemo3d/src/ham/mb_ham_spds_micro.c) from the NEMO-3D source tree, where
+# they lie, together with oracle/ref_sk_driver.cc into oracle/_ref/ref_sk.
+# The tests use it to check the oracle's restatement of the bond blocks, the
+# strain diagonal correction, the on-site/spin-orbit block and the sp3s*
+# parameter conversion.  Outputs go to oracle/_ref/ only.
+#
+# Usage: oracle/build_ref.sh [path to the NEMO_3D directory of the reference]
+set -e
+HERE=$(cd "$(dirname "$0")" && pwd)
+R=${1:-${NEMO3D_SRC:-/root/reference/NEMO_3D}}
+OUT="$HERE/_ref"
+if [ ! -f "$R/nemo3d/src/ham/mb_ham_spds_micro.c" ]; then
+  # machines without the reference tree use the prebuilt binary, if any
+  echo "build_ref.sh: reference sources not found under $R; skipped" >&2
+  exit 0
+fi
+mkdir -p "$OUT"
+INC="-I$R/nemo3d/src/base -I$R/nemo3d/src/ham -I$R/nemo3d/src/math -I$R/nemo3d/src/io \
+ -I$R/nemo3d/src/util -I$R/nemo3d/src/top -I$R/eigen/include -I$R/nml/include \
+ -I$R/XMLtoC/apps/ioNemo3D/src -I$R/XMLtoC/src -I$R/xerces-c-src2_1_0/include \
+ -I$R/xerces-c-src2_1_0/src -I$R/xerces-c-src2_1_0/src/xercesc"
+# the reference's own macro set (mb_ham_spds_micro.h:74-80) plus the serial build
+DEFS="-DFAKE_MPI -DLINUX"
+FLAGS="-O2 -ffp-contract=off -fpermissive -w -ffunction-sections -fdata-sections"
+g++ -x c++ $FLAGS $DEFS $INC -c "$R/nemo3d/src/ham/mb_ham_spds_micro.c" -o "$OUT/mb_ham_spds_micro.o"
+g++ $FLAGS $DEFS $INC -c "$HERE/ref_sk_driver.cc" -o "$OUT/ref_sk_driver.o"
+# routines the driver never reaches (geometry, dense eigensolvers) are
+# dropped by --gc-sections together with their unresolved references
+g++ -Wl,--gc-sections -o "$OUT/ref_sk" "$OUT/ref_sk_driver.o" "$OUT/mb_ham_spds_micro.o" -lm
+echo "$OUT/ref_sk"

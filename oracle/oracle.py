@@ -79,6 +79,9 @@ def lib():
                                              C.c_void_p, C.POINTER(_Opts), C.c_void_p,
                                              C.c_void_p, C.c_void_p, C.c_void_p,
                                              C.c_void_p, C.c_void_p]
+        L.orc_onsite_block.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
+        L.orc_bond.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                               C.c_int, C.c_double, C.c_void_p, C.c_void_p]
     return _lib
 
 

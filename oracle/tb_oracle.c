@@ -384,6 +384,35 @@ static void so_elem(int b1, int b2, int s1, int s2, double d, double *re,
   }
 }
 
+/* On-site block of one atom from its (bond-averaged) parameter vector p:
+ * on-site energies on the diagonal and, for nspin = 2, the spin-orbit
+ * couplings.  Restates h3d_diag (mb_ham_spds_micro.c:1453-1505) with the
+ * spin-orbit table of mb_ham_spds_so.h.  h: [nb][nb] complex, overwritten. */
+void orc_onsite_block(int norb, int nspin, int cation, const double *p, double *h) {
+  const int nb = norb * nspin;
+  int i, j;
+  memset(h, 0, sizeof(double) * nb * nb * 2);
+  for (i = 0; i < nb; i++) {
+    int oi = i % norb, si = nspin == 2 ? (i < norb ? 1 : 0) : -1;
+    h[(i * nb + i) * 2] = p[onsite_index(orb_type[oi], cation)];
+    if (nspin == 2)
+      for (j = 0; j < nb; j++) {
+        int oj = j % norb, sj = j < norb ? 1 : 0;
+        double re, im;
+        so_elem(oi, oj, si, sj, cation ? p[pE_Lc] : p[pE_La], &re, &im);
+        h[(i * nb + j) * 2] += re;
+        h[(i * nb + j) * 2 + 1] += im;
+      }
+  }
+}
+
+/* One bond seen from "this" atom (public form of bond_block, for tests). */
+void orc_bond(int norb, int this_cation, const double *nnv, const double *nnv0,
+              const double *par, int use_strain, double a0, double *blk,
+              double *ediag) {
+  bond_block(norb, this_cation, nnv, nnv0, par, use_strain, a0, blk, ediag);
+}
+
 /* bond vectors anion->cation of atom (site) "this" to its neighbour n
  * (geo_struct::getRelativePosVec, geo_struct.c:2224-2297, with the sign flip
  * for a cation in H_DiagStrainCorr_OffDiag_Wrapper, h_cvectr_mult.c:1077-1100) */
@@ -443,19 +472,7 @@ int orc_build(const orc_geom *g, const orc_model *md, long natoms,
     if (cnt == 0) continue;
     shiftsum /= cnt;
     for (i = 0; i < ORC_NPV; i++) p[i] /= cnt;
-    /* h3d_diag: on-site energies and spin-orbit */
-    for (i = 0; i < nb; i++) {
-      int oi = i % norb, si = nspin == 2 ? (i < norb ? 1 : 0) : -1;
-      h[(i * nb + i) * 2] = p[onsite_index(orb_type[oi], cat)];
-      if (nspin == 2)
-        for (j = 0; j < nb; j++) {
-          int oj = j % norb, sj = j < norb ? 1 : 0;
-          double re, im;
-          so_elem(oi, oj, si, sj, cat ? p[pE_Lc] : p[pE_La], &re, &im);
-          h[(i * nb + j) * 2] += re;
-          h[(i * nb + j) * 2 + 1] += im;
-        }
-    }
+    orc_onsite_block(norb, nspin, cat, p, h); /* h3d_diag */
     /* dangling-bond passivation of surface atoms */
     if (md->passivate && surface[a]) {
       static const double bond[4][3] = {{0.25, 0.25, 0.25},

@@ -59,6 +59,16 @@ int orc_build(const orc_geom *g, const orc_model *m, long natoms,
               const int *atom_slot, const int *nbr, const signed char *wrap,
               const unsigned char *surface, double *onsite, double *blocks);
 
+/* Building blocks of orc_build, exposed for checks against the reference's
+ * own routines.  orc_onsite_block: h3d_diag for one atom (h [nb][nb]
+ * complex).  orc_bond: one bond seen from "this" atom, nnv and nnv0 pointing
+ * anion -> cation; blk[c][a] = <anion a|H|cation c>; the strain correction of
+ * this atom's on-site energies is added to ediag[norb]. */
+void orc_onsite_block(int norb, int nspin, int cation, const double *p, double *h);
+void orc_bond(int norb, int this_cation, const double *nnv, const double *nnv0,
+              const double *par, int use_strain, double a0, double *blk,
+              double *ediag);
+
 /* y = (H - shift) x with per-bond Bloch phases k (NULL = Gamma / closed).
  * x,y: [natoms][nb] complex interleaved. */
 void orc_hx(int norb, int nspin, long natoms, const int *atom_slot,

@@ -1,0 +1,139 @@
+"""The oracle's Slater-Koster restatement against the reference's own routines.
+
+``oracle/_ref/ref_sk`` links the reference's ``mb_ham_spds_micro.c`` compiled
+from its own source (``oracle/build_ref.sh``).  These checks pin the parts of
+the Hamiltonian that the golden eigenvalue files cannot: Harrison strain
+scaling of the two-centre integrals, the strain diagonal correction, the
+anion/cation orientation of the bond block, the spin-orbit on-site block and
+the sp3s* -> sp3d5s* parameter conversion (mb_ham_spds_micro.c:597-1505,
+2848-3026).  Skipped where neither the binary nor the reference tree exists.
+"""
+
+import os
+import struct
+import subprocess
+
+import numpy as np
+import pytest
+
+from nemo3d_b200 import materials as M
+import oracle as O
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "ref_sk")
+
+# (material, nbasis passed to the reference, spin model, oracle norb, nspin)
+MODELS = {
+    "sp3d5s*_so": ("GaAs_spds", 20, 1, 10, 2),
+    "sp3d5s*": ("GaAs_spds", 10, -1, 10, 1),
+    "sp3s*_so": ("GaAs_sps", 10, 1, 5, 2),
+}
+# the four bond directions anion -> cation of a zincblende anion, in units of a
+TETRA = np.array([[1, 1, 1], [-1, -1, 1], [1, -1, -1], [-1, 1, -1]], float) * 0.25
+
+
+@pytest.fixture(scope="module")
+def ref_sk():
+    if not os.path.exists(REF_BIN):
+        subprocess.check_call(["sh", os.path.join(ROOT, "oracle", "build_ref.sh")])
+    if not os.path.exists(REF_BIN):
+        pytest.skip("reference sources not present; oracle/_ref/ref_sk not built")
+    return REF_BIN
+
+
+def _run(binary, payload: bytes) -> bytes:
+    p = subprocess.run([binary], input=payload, capture_output=True, timeout=120)
+    assert p.returncode == 0, p.stderr.decode()
+    return p.stdout
+
+
+def _cmat(buf, nb):
+    a = np.frombuffer(buf, dtype=np.float64).reshape(nb, nb, 2)
+    return a[..., 0] + 1j * a[..., 1]
+
+
+def _bonds(rng, a0, count):
+    out = []
+    for i in range(count):
+        nnv0 = TETRA[i % 4] * a0
+        nnv = nnv0 * (1 + rng.normal(0, 0.02)) + rng.normal(0, 0.01 * a0, 3)
+        out.append((nnv, nnv0))
+    return out
+
+
+@pytest.mark.parametrize("model", list(MODELS))
+@pytest.mark.parametrize("with_strain", [1, 0])
+def test_bond_blocks_and_strain_correction(ref_sk, model, with_strain):
+    mat_name, nbasis, spin_model, norb, nspin = MODELS[model]
+    rng = np.random.default_rng(7)
+    for mname in (mat_name, mat_name.replace("GaAs", "InAs")):
+        par = O.prepare_params(M.MATERIALS[mname], include_strain=True)
+        a0 = par[31]
+        payload = b""
+        cases = []
+        for this_cation in (0, 1):
+            for nnv, nnv0 in _bonds(rng, a0, 8):
+                payload += struct.pack("<5i", 1, nbasis, spin_model, this_cation, with_strain)
+                payload += np.concatenate([nnv, nnv0, [a0], par[:35], par[35:]]).tobytes()
+                cases.append((this_cation, nnv, nnv0))
+        out = _run(ref_sk, payload)
+        step = 2 * nbasis * nbasis * 16
+        assert len(out) == step * len(cases)
+        for i, (this_cation, nnv, nnv0) in enumerate(cases):
+            ho = _cmat(out[i * step:i * step + step // 2], nbasis)
+            hd = _cmat(out[i * step + step // 2:(i + 1) * step], nbasis)
+            blk = np.zeros(norb * norb)
+            ediag = np.zeros(norb)
+            O.lib().orc_bond(norb, this_cation, O._p(np.ascontiguousarray(nnv)),
+                             O._p(np.ascontiguousarray(nnv0)), O._p(par), with_strain,
+                             float(a0), O._p(blk), O._p(ediag))
+            blk = blk.reshape(norb, norb)            # [cation c][anion a]
+            want = blk if not this_cation else blk.T  # rows: the neighbour's orbitals
+            scale = np.abs(blk).max()
+            assert np.abs(ho.imag).max() == 0.0
+            assert np.abs(ho.real[:norb, :norb] - want).max() <= 1e-12 * scale, (mname, i)
+            if nspin == 2:  # spin-down copy, no spin-flip hopping
+                assert np.abs(ho.real[norb:, norb:] - want).max() <= 1e-12 * scale
+                assert np.abs(ho[:norb, norb:]).max() == 0.0
+                assert np.abs(ho[norb:, :norb]).max() == 0.0
+            for half in range(nspin):  # the correction is the same for both spins
+                corr = np.diag(hd.real)[half * norb:(half + 1) * norb]
+                assert np.abs(corr - ediag).max() <= 1e-12 * max(1.0, np.abs(ediag).max()), \
+                    (mname, i, half)
+            if not with_strain:
+                assert np.abs(ediag).max() == 0.0
+
+
+@pytest.mark.parametrize("model", list(MODELS))
+def test_onsite_block(ref_sk, model):
+    mat_name, nbasis, spin_model, norb, nspin = MODELS[model]
+    rng = np.random.default_rng(3)
+    base = O.prepare_params(M.MATERIALS[mat_name], include_strain=True)[:35]
+    payload = b""
+    cases = []
+    for cation in (0, 1):
+        for _ in range(3):
+            p = base + rng.normal(0, 0.05, 35)  # stands in for a bond average
+            payload += struct.pack("<4i", 2, nbasis, spin_model, cation) + p.tobytes()
+            cases.append((cation, p))
+    out = _run(ref_sk, payload)
+    step = nbasis * nbasis * 16
+    for i, (cation, p) in enumerate(cases):
+        h_ref = _cmat(out[i * step:(i + 1) * step], nbasis)
+        h = np.zeros(nbasis * nbasis * 2)
+        O.lib().orc_onsite_block(norb, nspin, cation, O._p(p), O._p(h))
+        h = h.reshape(nbasis, nbasis, 2)
+        assert np.array_equal(h[..., 0] + 1j * h[..., 1], h_ref), (model, cation)
+
+
+def test_sp3s_parameter_conversion(ref_sk):
+    for name in ("GaAs_sps", "InAs_sps"):
+        mat = M.MATERIALS[name]
+        pv = np.asarray(mat["pv"], float)[:15]
+        out = _run(ref_sk, struct.pack("<i", 3) + pv.tobytes() + struct.pack("<d", mat["a0"]))
+        ref = np.frombuffer(out, np.float64)
+        ours = np.zeros(O.NPAR)
+        O.lib().orc_prepare_params(1, 0, O._p(np.ascontiguousarray(pv)),
+                                   O._p(np.zeros(O.NSTR)), 0.0, float(mat["a0"]), O._p(ours))
+        assert np.array_equal(ours[:35], ref), name
