@@ -169,6 +169,22 @@ int tbgpu_export_pattern(const tbgpu_ctx *ctx, int *atom_site, int *nbr,
 int tbgpu_export_hamiltonian(const tbgpu_ctx *ctx, double *onsite,
                              double *blocks);
 
+/* y = (H - shift) x and *dot_dev = Re<x, y> on device buffers (x, y of
+ * tbgpu_dimension(ctx) complex entries, dot_dev one double), allocating
+ * nothing.  No counterpart in the reference: it serves callers that cannot
+ * let the library allocate -- device memory handed entirely to their own pool
+ * allocator, or iteration loops that cannot take the device-wide
+ * synchronisation of cudaMalloc/cudaFree.  The reduction scratch is a fixed
+ * array inside the library (2048 block partials + a counter, 16,640 bytes
+ * per device, held until exit); launches needing more than 2048 blocks are
+ * refused with TBGPU_E_ARG (10-orbital models: never; 5-orbital models: above
+ * 98,304 atoms).  Every call shares that array: calls that overlap on the GPU
+ * race and must be serialised by the caller.  The first call on a device
+ * looks up the array's address with that device current; make that first
+ * call before any stream capture.  The context's device must be current. */
+int tbgpu_hx_dot_noalloc(tbgpu_ctx *ctx, double shift, const double *x_dev,
+                         double *y_dev, double *dot_dev);
+
 /* H*x kernel: 0 = default (warp-staged cp.async kernel, 14 warps x 1 stage
  * per SM, for the 10-orbital models; lane-gather kernel otherwise),
  * 1 = lane-gather kernel for every model, 2 = warp-staged kernel with

@@ -181,4 +181,32 @@ int launch_spmv(Ctx &c, const double *x, double *y, double shift, const double *
   return set_error(TBGPU_E_UNSUPPORTED);
 }
 
+// Lane-gather launch with the alpha dot reduced through caller-provided
+// scratch (partial[cap] doubles, zeroed counter).  Allocates nothing; fails
+// with TBGPU_E_ARG when the launch needs more than cap blocks.
+template <int NORB, int NSPIN>
+static int launch_scratch_t(Ctx &c, const double *x, double *y, double shift, double *partial,
+                            unsigned int *counter, int cap, double *dot_out, cudaStream_t s) {
+  constexpr int APW = 32 / NORB;
+  const long per_block = long(kWPB) * APW;
+  const long grid = (c.natoms + per_block - 1) / per_block;
+  if (grid > cap) return set_error(TBGPU_E_ARG);
+  k_spmv<NORB, NSPIN, kWPB, true><<<unsigned(grid), kWPB * 32, 0, s>>>(
+      c.natoms, c.d_nbr, c.d_site_m, c.d_onsite, c.d_blocks, reinterpret_cast<const double2 *>(x),
+      reinterpret_cast<double2 *>(y), shift, nullptr, 0, partial, counter, dot_out, 0);
+  TB_CUDA(cudaGetLastError());
+  return TBGPU_OK;
+}
+
+int launch_spmv_scratch(Ctx &c, const double *x, double *y, double shift, double *partial,
+                        unsigned int *counter, int cap, double *dot_out, cudaStream_t s) {
+  if (c.norb == 10)
+    return launch_spmv_async_scratch(c, x, y, shift, partial, counter, cap, dot_out, s);
+  if (c.norb == 5 && c.nspin == 2)
+    return launch_scratch_t<5, 2>(c, x, y, shift, partial, counter, cap, dot_out, s);
+  if (c.norb == 5 && c.nspin == 1)
+    return launch_scratch_t<5, 1>(c, x, y, shift, partial, counter, cap, dot_out, s);
+  return set_error(TBGPU_E_UNSUPPORTED);
+}
+
 }  // namespace tbgpu

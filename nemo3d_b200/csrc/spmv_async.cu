@@ -330,4 +330,36 @@ int launch_spmv_async(Ctx &c, const double *x, double *y, double shift, const do
   return launch_cfg<14, 1>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
 }
 
+// Launch of the default 10-orbital configuration (14 warps x 1 stage) with
+// the alpha dot reduced through caller-provided scratch: partial[cap]
+// doubles and a zeroed counter.  Allocates nothing.
+int launch_spmv_async_scratch(Ctx &c, const double *x, double *y, double shift,
+                              double *partial, unsigned int *counter, int cap, double *dot_out,
+                              cudaStream_t s) {
+  if (c.norb != kNorb) return set_error(TBGPU_E_UNSUPPORTED);
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device);
+  if (sms > cap) return set_error(TBGPU_E_ARG);
+  const long ngroups = (c.natoms + kAPW - 1) / kAPW;
+  const double2 *X = reinterpret_cast<const double2 *>(x);
+  double2 *Y = reinterpret_cast<double2 *>(y);
+  if (c.nspin == 2) {
+    using L = Layout<2, 14, 1>;
+    TB_CUDA(cudaFuncSetAttribute(k_spmv_async<2, true, 14, 1>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM));
+    k_spmv_async<2, true, 14, 1><<<sms, 14 * 32, L::SMEM, s>>>(
+        c.natoms, ngroups, c.d_nbr, c.d_site_m, c.d_onsite, c.d_blocks, X, Y, shift, nullptr, 0,
+        partial, counter, dot_out, 0);
+  } else {
+    using L = Layout<1, 14, 1>;
+    TB_CUDA(cudaFuncSetAttribute(k_spmv_async<1, true, 14, 1>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM));
+    k_spmv_async<1, true, 14, 1><<<sms, 14 * 32, L::SMEM, s>>>(
+        c.natoms, ngroups, c.d_nbr, c.d_site_m, c.d_onsite, c.d_blocks, X, Y, shift, nullptr, 0,
+        partial, counter, dot_out, 0);
+  }
+  TB_CUDA(cudaGetLastError());
+  return TBGPU_OK;
+}
+
 }  // namespace tbgpu

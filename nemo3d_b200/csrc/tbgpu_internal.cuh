@@ -100,6 +100,12 @@ int launch_spmv(Ctx &c, const double *x, double *y, double shift,
 int launch_spmv_async(Ctx &c, const double *x, double *y, double shift,
                       const double *xscale_dev, int scale_index, double *alpha_out,
                       int alpha_index, cudaStream_t s);
+// caller-provided reduction scratch (noalloc.cu)
+int launch_spmv_scratch(Ctx &c, const double *x, double *y, double shift, double *partial,
+                        unsigned int *counter, int cap, double *dot_out, cudaStream_t s);
+int launch_spmv_async_scratch(Ctx &c, const double *x, double *y, double shift,
+                              double *partial, unsigned int *counter, int cap, double *dot_out,
+                              cudaStream_t s);
 // lanczos.cu
 int ensure_partials(Ctx &c, int nblocks);
 struct SolveArgs {
