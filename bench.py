@@ -39,8 +39,9 @@ from nemo3d_b200 import materials, workloads  # noqa: E402
 # store (blocks once per bond, on-site diagonal + spin-orbit, int32 column
 # per bond, x read once, y written once): 1864 + 640 bytes.
 BYTES_PER_ATOM = 2504
-# DRAM bytes per atom of one k_spmv launch measured with ncu
-# (profiles/spmv_cfg2_ncu.md); None until measured.
+# DRAM bytes per atom of one H*x launch on this workload measured with ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum); None until measured at
+# full size.
 NCU_TRAFFIC_PER_ATOM = None
 
 # band-edge windows of this dot (eV): 4 highest hole and 4 lowest electron
