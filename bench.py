@@ -299,8 +299,11 @@ def run_profile_case(args):
     import torch
     from nemo3d_b200 import tbgpu
     torch.cuda.set_device(0)
-    st = workloads.dome_in_box(cells=(40, 40, 30), base_nm=14.0, height_nm=4.0,
-                               sigma_frac=0.005, seed=1)
+    if args.profile_full:  # the bench's own 1.02M-atom dot (for 1-pass captures)
+        st = make_structure()
+    else:
+        st = workloads.dome_in_box(cells=(40, 40, 30), base_nm=14.0, height_nm=4.0,
+                                   sigma_frac=0.005, seed=1)
     H = tbgpu.Hamiltonian(st, "sp3d5s*_so", MATS)
     r0 = workloads.random_start(H.n, seed=0)
     res = H.eigensolve_lanczos(r0, imax=args.profile_iterations + 1, requested1=1,
@@ -322,6 +325,8 @@ def main():
     ap.add_argument("--profile-case", action="store_true",
                     help="small-case run of the solver kernels for ncu captures")
     ap.add_argument("--profile-iterations", type=int, default=6)
+    ap.add_argument("--profile-full", action="store_true",
+                    help="with --profile-case: use the full-size workload")
     ap.add_argument("--ref-iterations", type=int, default=19002,
                     help="iterations of a full solve (both passes) the CPU sample is scaled to")
     args = ap.parse_args()

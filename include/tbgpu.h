@@ -116,6 +116,15 @@ long tbgpu_dimension(const tbgpu_ctx *ctx); /* complex length n_atoms * nb */
 void tbgpu_matvect_mult(const int **argList, tbgpu_dcomplex *y,
                         const tbgpu_dcomplex *x);
 
+/* Bloch vector for periodic structures (geo_struct::phasePeriodic,
+ * nemo3d/src/base/geo_struct.h:811-826, used by Hmult_stored.c:386-437): a
+ * bond that crosses the periodic boundary by images w (-1/0/+1 per axis)
+ * carries exp(i*ph), ph = -pi*(w.k - 2*int(0.5*w.k)), k in the reference's
+ * units.  k = NULL or (0,0,0) is the Gamma point.  Call after
+ * tbgpu_build_hamiltonian; applies to every later H*x and solve.  Away from
+ * Gamma, H*x runs the lane-gather kernel. */
+int tbgpu_set_bloch_k(tbgpu_ctx *ctx, const double *k);
+
 /* y = (H - shift) x on device vectors (asynchronous on the context stream). */
 int tbgpu_hx_dev(tbgpu_ctx *ctx, double shift, const double *x_dev,
                  double *y_dev);
@@ -177,7 +186,8 @@ int tbgpu_export_hamiltonian(const tbgpu_ctx *ctx, double *onsite,
  * synchronisation of cudaMalloc/cudaFree.  The reduction scratch is a fixed
  * array inside the library (2048 block partials + a counter, 16,640 bytes
  * per device, held until exit); launches needing more than 2048 blocks are
- * refused with TBGPU_E_ARG (10-orbital models: never; 5-orbital models: above
+ * refused with TBGPU_E_ARG (10-orbital models: never at the Gamma point,
+ * above 49,152 atoms with a Bloch vector set; 5-orbital models: above
  * 98,304 atoms).  Every call shares that array: calls that overlap on the GPU
  * race and must be serialised by the caller.  The first call on a device
  * looks up the array's address with that device current; make that first

@@ -30,7 +30,7 @@ static void free_ctx(Ctx *c) {
   if (!c) return;
   void *ptrs[] = {c->d_type, c->d_dsp, c->d_par, c->d_par_ok, c->d_site_index, c->d_atom_site,
                   c->d_nbr, c->d_site_m, c->d_surface, c->d_onsite, c->d_blocks, c->d_partial,
-                  c->d_counter, c->d_status, c->d_x, c->d_y};
+                  c->d_counter, c->d_status, c->d_x, c->d_y, c->d_phase, c->d_groups};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -317,6 +317,21 @@ int tbgpu_export_hamiltonian(const tbgpu_ctx *ctx, double *onsite, double *block
 int tbgpu_set_spmv_variant(tbgpu_ctx *ctx, int variant) {
   if (!ctx || variant < 0 || variant > 2) return set_error(TBGPU_E_ARG);
   C(ctx)->spmv_variant = variant;
+  return TBGPU_OK;
+}
+
+int tbgpu_set_bloch_k(tbgpu_ctx *ctx, const double *k) {
+  if (!ctx) return set_error(TBGPU_E_ARG);
+  Ctx &c = *C(ctx);
+  if (!c.built) return set_error(TBGPU_E_STATE);
+  for (int d = 0; d < 3; d++) c.kvec[d] = k ? k[d] : 0.0;
+  const bool periodic = c.periodic[0] || c.periodic[1] || c.periodic[2];
+  const bool nonzero = c.kvec[0] != 0.0 || c.kvec[1] != 0.0 || c.kvec[2] != 0.0;
+  c.bloch = false;
+  if (!periodic || !nonzero) return TBGPU_OK;  // Gamma point: no phases
+  int rc = build_phases(c);
+  if (rc) return rc;
+  c.bloch = true;
   return TBGPU_OK;
 }
 

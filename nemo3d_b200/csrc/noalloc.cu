@@ -13,9 +13,10 @@
 // The scratch: kMaxBlocks (2048) block partials plus a completion counter,
 // 16,640 bytes held on every device that loads the library, until the
 // process exits.  A launch that would need more than 2048 blocks is refused
-// with TBGPU_E_ARG: the 10-orbital models always launch one block per SM;
-// the 5-orbital models launch one block per 48 atoms, so at most 98,304
-// atoms.
+// with TBGPU_E_ARG: the 10-orbital models launch one block per SM at the
+// Gamma point (one block per 24 atoms, at most 49,152 atoms, with a Bloch
+// vector set); the 5-orbital models launch one block per 48 atoms, so at
+// most 98,304 atoms.
 //
 // The array is shared by every call and keeps the last call's contents; the
 // counter is cleared before each launch.  Calls that overlap on the GPU (from

@@ -27,13 +27,16 @@ __device__ __forceinline__ void cfma_i(double2 &acc, double lam, double2 a) {
   acc.y += lam * a.x;
 }
 
-template <int NORB, int NSPIN, int WPB, bool DOT>
+// PHASE: bonds carry the Bloch phase phase[a*4+n] of H[a][nbr] (periodic
+// structures away from the Gamma point).
+template <int NORB, int NSPIN, int WPB, bool DOT, bool PHASE = false>
 __global__ void __launch_bounds__(WPB * 32)
     k_spmv(long natoms, const int4 *__restrict__ nbr, const unsigned char *__restrict__ site_m,
            const double *__restrict__ onsite, const double *__restrict__ blocks,
            const double2 *__restrict__ x, double2 *__restrict__ y, double shift,
            const double *__restrict__ xnorm, int xnorm_idx, double *partial,
-           unsigned int *counter, double *alpha_out, int alpha_idx) {
+           unsigned int *counter, double *alpha_out, int alpha_idx,
+           const double2 *__restrict__ phase = nullptr) {
   constexpr int NB = NORB * NSPIN;
   constexpr int APW = 32 / NORB;
   constexpr int ONS = onsite_len(NB);
@@ -103,6 +106,14 @@ __global__ void __launch_bounds__(WPB * 32)
     for (int n = 0; n < 4; n++) {
       if (nb[n] < 0) continue;
       const double2 *xn = xs[w][ai][n];
+      // with phases, the bond's product is formed apart and then rotated
+      double2 part[NSPIN];
+      double2 *tgt = acc;
+      if (PHASE) {
+#pragma unroll
+        for (int s = 0; s < NSPIN; s++) part[s] = make_double2(0.0, 0.0);
+        tgt = part;
+      }
       if (cat) {
         const double *M = blocks + (a * 4 + n) * (NORB * NORB) + o * NORB;
         double r[NORB];
@@ -122,14 +133,22 @@ __global__ void __launch_bounds__(WPB * 32)
 #pragma unroll
         for (int k = 0; k < NORB; k++)
 #pragma unroll
-          for (int s = 0; s < NSPIN; s++) cfma_r(acc[s], r[k], xn[s * NORB + k]);
+          for (int s = 0; s < NSPIN; s++) cfma_r(tgt[s], r[k], xn[s * NORB + k]);
       } else {
         const double *M = blocks + (long(nb[n]) * 4 + c_rev_slot[m][n]) * (NORB * NORB) + o;
 #pragma unroll
         for (int k = 0; k < NORB; k++) {
           const double v = __ldg(M + k * NORB);
 #pragma unroll
-          for (int s = 0; s < NSPIN; s++) cfma_r(acc[s], v, xn[s * NORB + k]);
+          for (int s = 0; s < NSPIN; s++) cfma_r(tgt[s], v, xn[s * NORB + k]);
+        }
+      }
+      if (PHASE) {
+        const double2 ph = __ldg(phase + a * 4 + n);
+#pragma unroll
+        for (int s = 0; s < NSPIN; s++) {
+          acc[s].x += ph.x * part[s].x - ph.y * part[s].y;
+          acc[s].y += ph.x * part[s].y + ph.y * part[s].x;
         }
       }
     }
@@ -158,13 +177,23 @@ static int launch_t(Ctx &c, const double *x, double *y, double shift,
   if (alpha_out) {
     int rc = ensure_partials(c, int(grid));
     if (rc) return rc;
-    k_spmv<NORB, NSPIN, kWPB, true><<<grid, kWPB * 32, 0, s>>>(
-        c.natoms, c.d_nbr, c.d_site_m, c.d_onsite, c.d_blocks, X, Y, shift, xnorm, xidx,
-        c.d_partial, c.d_counter, alpha_out, aidx);
+    if (c.bloch)
+      k_spmv<NORB, NSPIN, kWPB, true, true><<<grid, kWPB * 32, 0, s>>>(
+          c.natoms, c.d_nbr, c.d_site_m, c.d_onsite, c.d_blocks, X, Y, shift, xnorm, xidx,
+          c.d_partial, c.d_counter, alpha_out, aidx, c.d_phase);
+    else
+      k_spmv<NORB, NSPIN, kWPB, true><<<grid, kWPB * 32, 0, s>>>(
+          c.natoms, c.d_nbr, c.d_site_m, c.d_onsite, c.d_blocks, X, Y, shift, xnorm, xidx,
+          c.d_partial, c.d_counter, alpha_out, aidx);
   } else {
-    k_spmv<NORB, NSPIN, kWPB, false><<<grid, kWPB * 32, 0, s>>>(
-        c.natoms, c.d_nbr, c.d_site_m, c.d_onsite, c.d_blocks, X, Y, shift, xnorm, xidx,
-        nullptr, nullptr, nullptr, 0);
+    if (c.bloch)
+      k_spmv<NORB, NSPIN, kWPB, false, true><<<grid, kWPB * 32, 0, s>>>(
+          c.natoms, c.d_nbr, c.d_site_m, c.d_onsite, c.d_blocks, X, Y, shift, xnorm, xidx,
+          nullptr, nullptr, nullptr, 0, c.d_phase);
+    else
+      k_spmv<NORB, NSPIN, kWPB, false><<<grid, kWPB * 32, 0, s>>>(
+          c.natoms, c.d_nbr, c.d_site_m, c.d_onsite, c.d_blocks, X, Y, shift, xnorm, xidx,
+          nullptr, nullptr, nullptr, 0);
   }
   TB_CUDA(cudaGetLastError());
   return TBGPU_OK;
@@ -172,7 +201,9 @@ static int launch_t(Ctx &c, const double *x, double *y, double shift,
 
 int launch_spmv(Ctx &c, const double *x, double *y, double shift, const double *xnorm,
                 int xidx, double *alpha_out, int aidx, cudaStream_t s) {
-  if (c.norb == 10 && c.spmv_variant != 1)
+  // the warp-staged kernel has no phase support: periodic structures away
+  // from Gamma take the lane-gather kernel
+  if (c.norb == 10 && c.spmv_variant != 1 && !c.bloch)
     return launch_spmv_async(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
   if (c.norb == 10 && c.nspin == 2) return launch_t<10, 2>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
   if (c.norb == 10 && c.nspin == 1) return launch_t<10, 1>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
@@ -191,17 +222,28 @@ static int launch_scratch_t(Ctx &c, const double *x, double *y, double shift, do
   const long per_block = long(kWPB) * APW;
   const long grid = (c.natoms + per_block - 1) / per_block;
   if (grid > cap) return set_error(TBGPU_E_ARG);
-  k_spmv<NORB, NSPIN, kWPB, true><<<unsigned(grid), kWPB * 32, 0, s>>>(
-      c.natoms, c.d_nbr, c.d_site_m, c.d_onsite, c.d_blocks, reinterpret_cast<const double2 *>(x),
-      reinterpret_cast<double2 *>(y), shift, nullptr, 0, partial, counter, dot_out, 0);
+  if (c.bloch)
+    k_spmv<NORB, NSPIN, kWPB, true, true><<<unsigned(grid), kWPB * 32, 0, s>>>(
+        c.natoms, c.d_nbr, c.d_site_m, c.d_onsite, c.d_blocks,
+        reinterpret_cast<const double2 *>(x), reinterpret_cast<double2 *>(y), shift, nullptr, 0,
+        partial, counter, dot_out, 0, c.d_phase);
+  else
+    k_spmv<NORB, NSPIN, kWPB, true><<<unsigned(grid), kWPB * 32, 0, s>>>(
+        c.natoms, c.d_nbr, c.d_site_m, c.d_onsite, c.d_blocks,
+        reinterpret_cast<const double2 *>(x), reinterpret_cast<double2 *>(y), shift, nullptr, 0,
+        partial, counter, dot_out, 0);
   TB_CUDA(cudaGetLastError());
   return TBGPU_OK;
 }
 
 int launch_spmv_scratch(Ctx &c, const double *x, double *y, double shift, double *partial,
                         unsigned int *counter, int cap, double *dot_out, cudaStream_t s) {
-  if (c.norb == 10)
+  if (c.norb == 10 && !c.bloch)
     return launch_spmv_async_scratch(c, x, y, shift, partial, counter, cap, dot_out, s);
+  if (c.norb == 10 && c.nspin == 2)
+    return launch_scratch_t<10, 2>(c, x, y, shift, partial, counter, cap, dot_out, s);
+  if (c.norb == 10 && c.nspin == 1)
+    return launch_scratch_t<10, 1>(c, x, y, shift, partial, counter, cap, dot_out, s);
   if (c.norb == 5 && c.nspin == 2)
     return launch_scratch_t<5, 2>(c, x, y, shift, partial, counter, cap, dot_out, s);
   if (c.norb == 5 && c.nspin == 1)

@@ -10,10 +10,12 @@
 // stage with coalesced 16-byte cp.async copies (one instruction moves 512
 // bytes, nothing is held in registers) and computes it, one lane per orbital
 // row, from shared memory; with one stage per warp, the other warps of the
-// SM cover its wait, with two it also overlaps its own next copies.  Groups of three atoms
-// are dealt to warps in order, so all SMs sweep the atom order together and
-// the blocks an anion reads transposed (stored once, by the cation) are
-// still in L2 when they are needed the second time.
+// SM cover its wait, with two it also overlaps its own next copies.  Groups
+// (up to three consecutive atoms of one k-pencil of cells) are dealt to
+// warps in the work order of the context (pencils visited j-block by
+// j-block, see build_work_order), so all SMs sweep the structure together and
+// a neighbour's x segment, or a block an anion reads transposed (stored once,
+// by the cation), is still in L2 when it is needed the second time.
 //
 // (A variant that gathered the same bytes with one 1-D TMA bulk copy per
 // 300-800-byte segment took 2.4 ms per launch on the 1.02M-atom dot: that
@@ -75,15 +77,21 @@ struct Layout {
 struct Meta {
   int nb[kAPW][4];
   int m[kAPW];  // -1: no atom
+  int a0;       // first atom of the group
 };
 
-__device__ __forceinline__ Meta load_meta(long g, long natoms, const int4 *__restrict__ nbr,
+// Group g of the work order: up to three consecutive atoms of one pencil.
+__device__ __forceinline__ Meta load_meta(long g, long ngroups, const int2 *__restrict__ groups,
+                                          const int4 *__restrict__ nbr,
                                           const unsigned char *__restrict__ site_m) {
   Meta M;
+  int2 e = make_int2(0, 0);
+  if (g < ngroups) e = __ldg(groups + g);
+  M.a0 = e.x;
 #pragma unroll
   for (int i = 0; i < kAPW; i++) {
-    const long a = g * kAPW + i;
-    if (a < natoms) {
+    const long a = long(e.x) + i;
+    if (i < e.y) {
       const int4 v = __ldg(nbr + a);
       M.nb[i][0] = v.x; M.nb[i][1] = v.y; M.nb[i][2] = v.z; M.nb[i][3] = v.w;
       M.m[i] = __ldg(site_m + a);
@@ -106,7 +114,7 @@ __device__ __forceinline__ void issue(unsigned char *st, long g, const Meta &M, 
   for (int i = 0; i < kAPW; i++) {
     const int m = M.m[i];
     if (m < 0) continue;
-    const long a = g * kAPW + i;
+    const long a = long(M.a0) + i;
     const bool cat = m < 4;
     unsigned char *bk = st + L::blk(i);
     if (cat) {  // the cation's four blocks are one contiguous run
@@ -144,7 +152,7 @@ __device__ __forceinline__ void issue(unsigned char *st, long g, const Meta &M, 
 
 template <int NSPIN, bool DOT, int WARPS, int STAGES>
 __global__ void __launch_bounds__(WARPS * 32, 1)
-    k_spmv_async(long natoms, long ngroups, const int4 *__restrict__ nbr,
+    k_spmv_async(long ngroups, const int2 *__restrict__ groups, const int4 *__restrict__ nbr,
                  const unsigned char *__restrict__ site_m, const double *__restrict__ onsite,
                  const double *__restrict__ blocks, const double2 *__restrict__ x,
                  double2 *__restrict__ y, double shift, const double *__restrict__ xnorm,
@@ -161,10 +169,10 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
   const long nw = long(gridDim.x) * WARPS;
   long g = long(blockIdx.x) * WARPS + warp;
   // prologue: copies of the first group in flight, metadata of the next
-  Meta cur = load_meta(g, natoms, nbr, site_m);
+  Meta cur = load_meta(g, ngroups, groups, nbr, site_m);
   if (STAGES > 1 && g < ngroups) issue<L>(wbase, g, cur, lane, onsite, blocks, x);
   cp_commit();
-  Meta nxt = load_meta(g + nw, natoms, nbr, site_m);
+  Meta nxt = load_meta(g + nw, ngroups, groups, nbr, site_m);
   int k = 0;
   for (; g < ngroups; g += nw, ++k) {
     const long gn = g + nw;
@@ -177,7 +185,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
       issue<L>(st, g, cur, lane, onsite, blocks, x);
       cp_commit();
     }
-    const Meta nn = load_meta(gn + nw, natoms, nbr, site_m);  // two groups ahead
+    const Meta nn = load_meta(gn + nw, ngroups, groups, nbr, site_m);  // two groups ahead
     if (STAGES > 1) cp_wait<1>(); else cp_wait<0>();  // this lane's copies of g landed
     __syncwarp();   // ... and every lane's
     // this lane's atom, selected without indexing the metadata at run time
@@ -188,7 +196,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
       nbv[n] = ai == 0 ? cur.nb[0][n] : ai == 1 ? cur.nb[1][n] : cur.nb[2][n];
     if (ai < kAPW && m >= 0) {
       const bool cat = m < 4;
-      const long a = g * kAPW + ai;
+      const long a = long(cur.a0) + ai;
       const double2 *xs = reinterpret_cast<const double2 *>(st + L::xs(ai));
       const double2 *X0 = xs + 4 * NB;
       const double *rec = reinterpret_cast<const double *>(st + L::ons(ai));
@@ -291,14 +299,13 @@ int launch_async_t(Ctx &c, const double *x, double *y, double shift, const doubl
                              cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM) != cudaSuccess)
       return set_error(TBGPU_E_CUDA);
   }
-  const long ngroups = (c.natoms + kAPW - 1) / kAPW;
   const unsigned grid = unsigned(sms);
   if (DOT) {
     int rc = ensure_partials(c, int(grid));
     if (rc) return rc;
   }
   k_spmv_async<NSPIN, DOT, WARPS, STAGES><<<grid, WARPS * 32, L::SMEM, s>>>(
-      c.natoms, ngroups, c.d_nbr, c.d_site_m, c.d_onsite, c.d_blocks,
+      c.ngroups, c.d_groups, c.d_nbr, c.d_site_m, c.d_onsite, c.d_blocks,
       reinterpret_cast<const double2 *>(x), reinterpret_cast<double2 *>(y), shift, xnorm, xidx,
       DOT ? c.d_partial : nullptr, DOT ? c.d_counter : nullptr, alpha_out, aidx);
   TB_CUDA(cudaGetLastError());
@@ -340,7 +347,6 @@ int launch_spmv_async_scratch(Ctx &c, const double *x, double *y, double shift,
   int sms = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device);
   if (sms > cap) return set_error(TBGPU_E_ARG);
-  const long ngroups = (c.natoms + kAPW - 1) / kAPW;
   const double2 *X = reinterpret_cast<const double2 *>(x);
   double2 *Y = reinterpret_cast<double2 *>(y);
   if (c.nspin == 2) {
@@ -348,14 +354,14 @@ int launch_spmv_async_scratch(Ctx &c, const double *x, double *y, double shift,
     TB_CUDA(cudaFuncSetAttribute(k_spmv_async<2, true, 14, 1>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM));
     k_spmv_async<2, true, 14, 1><<<sms, 14 * 32, L::SMEM, s>>>(
-        c.natoms, ngroups, c.d_nbr, c.d_site_m, c.d_onsite, c.d_blocks, X, Y, shift, nullptr, 0,
+        c.ngroups, c.d_groups, c.d_nbr, c.d_site_m, c.d_onsite, c.d_blocks, X, Y, shift, nullptr, 0,
         partial, counter, dot_out, 0);
   } else {
     using L = Layout<1, 14, 1>;
     TB_CUDA(cudaFuncSetAttribute(k_spmv_async<1, true, 14, 1>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM));
     k_spmv_async<1, true, 14, 1><<<sms, 14 * 32, L::SMEM, s>>>(
-        c.natoms, ngroups, c.d_nbr, c.d_site_m, c.d_onsite, c.d_blocks, X, Y, shift, nullptr, 0,
+        c.ngroups, c.d_groups, c.d_nbr, c.d_site_m, c.d_onsite, c.d_blocks, X, Y, shift, nullptr, 0,
         partial, counter, dot_out, 0);
   }
   TB_CUDA(cudaGetLastError());

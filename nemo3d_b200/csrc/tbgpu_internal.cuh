@@ -65,6 +65,10 @@ struct Ctx {
   unsigned char *d_surface = nullptr;
   double *d_onsite = nullptr;       // [natoms*ons]
   double *d_blocks = nullptr;       // [natoms*4*norb*norb], cation atoms
+  // H*x work order: groups of up to 3 consecutive atoms of one k-pencil of
+  // cells, pencils visited in j-blocks (first atom, atom count)
+  int2 *d_groups = nullptr;
+  long ngroups = 0;
   // reduction scratch (per-block partials + completion counter)
   double *d_partial = nullptr;
   unsigned int *d_counter = nullptr;
@@ -76,6 +80,10 @@ struct Ctx {
   tbgpu_stats stats{};
   bool profiling = false;
   int spmv_variant = 0;
+  // Bloch phases of bonds that cross a periodic boundary (off: Gamma point)
+  bool bloch = false;
+  double kvec[3] = {0, 0, 0};
+  double2 *d_phase = nullptr;       // [natoms*4] phase of H[a][nbr], or null
   // scratch for the host-pointer matvec
   double *d_x = nullptr, *d_y = nullptr;
 };
@@ -90,6 +98,7 @@ int set_error(int code);
 
 // topology.cu
 int build_topology(Ctx &c);
+int build_phases(Ctx &c);  // fills d_phase for c.kvec
 // build.cu
 int assemble(Ctx &c);
 // spmv.cu

@@ -8,6 +8,9 @@
 //   FindSurfaceAtoms (bit 0, isOnSurface) nemo3d/src/base/geo_struct.c:1374-1463
 // Atoms are numbered in site order (cell-major, k fastest, then in-cell site),
 // which is the reference's vector layout.
+#include <algorithm>
+#include <vector>
+
 #include <cub/device/device_scan.cuh>
 
 #include "tbgpu_internal.cuh"
@@ -20,8 +23,10 @@ struct Grid {
 };
 
 // neighbour site of site s along slot n; -1 outside a closed boundary.
-// *wrapped is set when a periodic image is crossed.
-__device__ __forceinline__ long nbr_site(const Grid g, long s, int n, bool *wrapped) {
+// *wrapped is set when a periodic image is crossed; w (optional) receives the
+// image crossed along each axis (-1, 0, +1).
+__device__ __forceinline__ long nbr_site(const Grid g, long s, int n, bool *wrapped,
+                                         int *w = nullptr) {
   const int m = int(s & 7);
   long cell = s >> 3;
   int k = int(cell % g.nz);
@@ -33,9 +38,11 @@ __device__ __forceinline__ long nbr_site(const Grid g, long s, int n, bool *wrap
   *wrapped = false;
 #pragma unroll
   for (int d = 0; d < 3; d++) {
+    if (w) w[d] = 0;
     if (c[d] < 0 || c[d] >= dim[d]) {
       if (!per[d]) return -1;
       *wrapped = true;
+      if (w) w[d] = c[d] < 0 ? -1 : 1;
       c[d] = (c[d] + dim[d]) % dim[d];
     }
   }
@@ -82,6 +89,83 @@ __global__ void k_finalize(Grid g, long nsites, const int *flag, const int *inde
   surface[a] = (unsigned char)(cnt != 4);
 }
 
+// Phase of H[a][b] for every bond: the conjugate of the Bloch factor of the
+// periodic image crossed from a to b, exp(i*ph) with ph = -pi*(w.k -
+// 2*int(0.5*w.k)) (geo_struct::phasePeriodic, nemo3d/src/base/geo_struct.h:
+// 811-826, applied in Hmult_stored.c:386-437); 1 inside the domain.
+__global__ void k_phase(Grid g, long natoms, const int *atom_site, const int4 *nbr,
+                        double k0, double k1, double k2, double2 *phase) {
+  long a = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (a >= natoms) return;
+  const long s = atom_site[a];
+  const int4 v = nbr[a];
+  const int b[4] = {v.x, v.y, v.z, v.w};
+  for (int n = 0; n < 4; n++) {
+    double2 p = make_double2(1.0, 0.0);
+    bool wrapped;
+    int w[3];
+    nbr_site(g, s, n, &wrapped, w);
+    if (b[n] >= 0 && wrapped) {
+      double ph = w[0] * k0 + w[1] * k1 + w[2] * k2;
+      ph = -M_PI * (ph - 2 * (int)(0.5 * ph));
+      double sn, cs;
+      sincos(ph, &sn, &cs);
+      p = make_double2(cs, -sn);
+    }
+    phase[a * 4 + n] = p;
+  }
+}
+
+int build_phases(Ctx &c) {
+  if (!c.d_phase) TB_CUDA(cudaMalloc(&c.d_phase, sizeof(double2) * 4 * c.natoms));
+  Grid g{c.nx, c.ny, c.nz, c.periodic[0], c.periodic[1], c.periodic[2]};
+  const int threads = 256;
+  const unsigned blocks = unsigned((c.natoms + threads - 1) / threads);
+  k_phase<<<blocks, threads, 0, c.stream>>>(g, c.natoms, c.d_atom_site, c.d_nbr, c.kvec[0],
+                                            c.kvec[1], c.kvec[2], c.d_phase);
+  TB_CUDA(cudaGetLastError());
+  return TBGPU_OK;
+}
+
+// Work order of the warp-staged H*x kernel.  Atoms are numbered in site
+// order, so the atoms of a k-pencil of cells (i, j, 0..nz-1) are one
+// contiguous run.  Visiting pencils j-block by j-block (kPencilBlock pencils
+// wide, i slower than j inside a block) keeps the atoms that share a bond,
+// and with it the x segments and bond blocks read twice, within a few
+// thousand atoms of each other in processing order, so the second read hits
+// L2; in plain atom order the i-direction neighbours are a whole y-z plane
+// apart.
+#ifndef TBGPU_PENCIL_BLOCK
+#define TBGPU_PENCIL_BLOCK 8
+#endif
+constexpr int kPencilBlock = TBGPU_PENCIL_BLOCK;
+constexpr int kGroupAtoms = 3;
+
+static int build_work_order(Ctx &c, const int *index) {
+  const long npen = long(c.nx) * c.ny;
+  const size_t pitch = size_t(c.nz) * 8 * sizeof(int);
+  std::vector<int> start(npen + 1);
+  TB_CUDA(cudaMemcpy2DAsync(start.data(), sizeof(int), index, pitch, sizeof(int), npen,
+                            cudaMemcpyDeviceToHost, c.stream));
+  TB_CUDA(cudaStreamSynchronize(c.stream));
+  start[npen] = int(c.natoms);
+  std::vector<int2> groups;
+  groups.reserve(c.natoms / kGroupAtoms + npen + 1);
+  for (int jb = 0; jb < c.ny; jb += kPencilBlock)
+    for (int i = 0; i < c.nx; i++)
+      for (int j = jb; j < jb + kPencilBlock && j < c.ny; j++) {
+        const long p = long(i) * c.ny + j;
+        for (int a = start[p]; a < start[p + 1]; a += kGroupAtoms)
+          groups.push_back(make_int2(a, std::min(kGroupAtoms, start[p + 1] - a)));
+      }
+  c.ngroups = long(groups.size());
+  TB_CUDA(cudaMalloc(&c.d_groups, sizeof(int2) * groups.size()));
+  TB_CUDA(cudaMemcpyAsync(c.d_groups, groups.data(), sizeof(int2) * groups.size(),
+                          cudaMemcpyHostToDevice, c.stream));
+  TB_CUDA(cudaStreamSynchronize(c.stream));
+  return TBGPU_OK;
+}
+
 int build_topology(Ctx &c) {
   Grid g{c.nx, c.ny, c.nz, c.periodic[0], c.periodic[1], c.periodic[2]};
   const long ns = c.nsites;
@@ -117,6 +201,7 @@ int build_topology(Ctx &c) {
                                                  c.d_atom_site, c.d_nbr, c.d_site_m,
                                                  c.d_surface);
     TB_CUDA(cudaGetLastError());
+    rc = build_work_order(c, index);
   }
   cudaFreeAsync(tmp, c.stream);
   cudaFreeAsync(flag, c.stream);

@@ -68,6 +68,7 @@ def _lib():
         L.tbgpu_error_string.restype = C.c_char_p
         L.tbgpu_error_string.argtypes = [ip]
         L.tbgpu_prepare_params.argtypes = [ip, ip, vp, vp, dp, dp, vp]
+        L.tbgpu_set_bloch_k.argtypes = [vp, C.POINTER(C.c_double)]
         L.tbgpu_ctx_create.argtypes = [C.POINTER(_Geom), C.POINTER(_Model), C.POINTER(vp)]
         L.tbgpu_ctx_create_dev.argtypes = [C.POINTER(_Geom), C.POINTER(_Model), C.POINTER(vp)]
         L.tbgpu_ctx_destroy.argtypes = [vp]
@@ -285,6 +286,14 @@ class Hamiltonian:
         if rc:
             raise TbgpuError(rc, "tbgpu_export_hamiltonian")
         return ons, blk
+
+    def set_bloch_k(self, k):
+        """Bloch vector (reference units) for periodic structures; None or
+        zeros is the Gamma point (tbgpu_set_bloch_k)."""
+        kv = None if k is None else (C.c_double * 3)(*[float(v) for v in k])
+        rc = _lib().tbgpu_set_bloch_k(self._ctx, kv)
+        if rc:
+            raise TbgpuError(rc, "tbgpu_set_bloch_k")
 
     def set_spmv_variant(self, variant: int):
         """0: warp-staged cp.async kernel (default, 10 orbitals); 1: lane-gather; 2: 2-stage."""
