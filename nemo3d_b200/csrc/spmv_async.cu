@@ -40,6 +40,13 @@ __device__ __forceinline__ void cp16(void *dst, const void *src) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src)
                : "memory");
 }
+// 16-byte copy that reads `bytes` (16 or 0) from global memory and fills the
+// rest of the chunk with zeros: a missing neighbour costs no branch
+__device__ __forceinline__ void cp16z(void *dst, const void *src, int bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_addr(dst)), "l"(src),
+               "r"(bytes)
+               : "memory");
+}
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_wait() {
@@ -122,14 +129,16 @@ __device__ __forceinline__ void issue(unsigned char *st, long g, const Meta &M, 
 #pragma unroll
       for (int c = lane; c < 4 * L::BLK_CH; c += 32) cp16(bk + c * 16, src + c * 16);
     } else {
+      // a missing neighbour (surface) is zero-filled, not skipped
 #pragma unroll
       for (int n = 0; n < 4; n++) {
         const int b = M.nb[i][n];
-        if (b < 0) continue;
+        const int bytes = b >= 0 ? 16 : 0;
         const unsigned char *src = reinterpret_cast<const unsigned char *>(
-            blocks + (long(b) * 4 + c_rev_slot[m][n]) * L::BLK);
+            blocks + (long(b >= 0 ? b : a) * 4 + c_rev_slot[m][n]) * L::BLK);
 #pragma unroll
-        for (int c = lane; c < L::BLK_CH; c += 32) cp16(bk + n * L::BLK * 8 + c * 16, src + c * 16);
+        for (int c = lane; c < L::BLK_CH; c += 32)
+          cp16z(bk + n * L::BLK * 8 + c * 16, src + c * 16, bytes);
       }
     }
     unsigned char *xs = st + L::xs(i);
@@ -139,9 +148,9 @@ __device__ __forceinline__ void issue(unsigned char *st, long g, const Meta &M, 
 #pragma unroll
       for (int n = 0; n < 4; n++) {
         const int b = M.nb[i][n];
-        if (b >= 0)
-          cp16(xs + n * NB * 16 + lane * 16,
-               reinterpret_cast<const unsigned char *>(x + long(b) * NB) + lane * 16);
+        cp16z(xs + n * NB * 16 + lane * 16,
+              reinterpret_cast<const unsigned char *>(x + long(b >= 0 ? b : a) * NB) + lane * 16,
+              b >= 0 ? 16 : 0);
       }
     }
     if (lane < L::ONS_CH)
@@ -237,32 +246,26 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
           cfma_r(acc[NSPIN - 1], Lm, U[2]); cfma_i(acc[NSPIN - 1], Lm, U[3]);
         }
       }
-      // bonds: one accumulator per neighbour so the four chains are independent
+      // bonds: one accumulator per neighbour, neighbours innermost so that
+      // consecutive FMAs feed independent chains; the lane's block element
+      // (o, k) is row o of a cation's own block or column o of the block an
+      // anion reads from its cation neighbour
       double2 part[4][NSPIN];
 #pragma unroll
-      for (int n = 0; n < 4; n++) {
+      for (int n = 0; n < 4; n++)
 #pragma unroll
         for (int sp = 0; sp < NSPIN; sp++) part[n][sp] = make_double2(0.0, 0.0);
-        if (nbv[n] < 0) continue;
-        const double2 *xn = xs + n * NB;
-        const double *Mb = bk + n * L::BLK;
-        double r[kNorb];
-        if (cat) {
+      const double *Mb = bk + (cat ? o * kNorb : o);
+      const int bstride = cat ? 1 : kNorb;
 #pragma unroll
-          for (int kk = 0; kk < kNorb; kk += 2) {
-            const double2 t2 = *reinterpret_cast<const double2 *>(Mb + o * kNorb + kk);
-            r[kk] = t2.x;
-            r[kk + 1] = t2.y;
-          }
-        } else {
+      for (int kk = 0; kk < kNorb; kk++)
 #pragma unroll
-          for (int kk = 0; kk < kNorb; kk++) r[kk] = Mb[kk * kNorb + o];
+        for (int n = 0; n < 4; n++) {
+          if (nbv[n] < 0) continue;
+          const double r = Mb[n * L::BLK + kk * bstride];
+#pragma unroll
+          for (int sp = 0; sp < NSPIN; sp++) cfma_r(part[n][sp], r, xs[n * NB + sp * kNorb + kk]);
         }
-#pragma unroll
-        for (int kk = 0; kk < kNorb; kk++)
-#pragma unroll
-          for (int sp = 0; sp < NSPIN; sp++) cfma_r(part[n][sp], r[kk], xn[sp * kNorb + kk]);
-      }
 #pragma unroll
       for (int sp = 0; sp < NSPIN; sp++) {
         const double2 bsum = make_double2((part[0][sp].x + part[1][sp].x) + (part[2][sp].x + part[3][sp].x),
