@@ -109,33 +109,49 @@ struct ChunkPtrs {
   const double2 *r[kMaxChunk];
 };
 
-// V[e] += sum_k coef[k][e] * R_k for one group of up to kVecGroup vectors
+// Coefficients of one chunk, passed by value: the kernel reads them from the
+// parameter bank as FMA operands (no shared-memory traffic per element).
+struct ChunkCoef {
+  double c[kMaxChunk][kVecGroup];
+};
+
+// V[e] += sum_k coef[k][e] * R_k for one group of NV vectors (memory bound:
+// the chunk's nk r-vectors and the NV eigenvectors are streamed once)
+template <int NV>
 __global__ void __launch_bounds__(256)
-    k_accum(long n2, int nk, int nv, ChunkPtrs R, const double *__restrict__ coef, int ldc,
-            double2 *__restrict__ V) {
-  __shared__ double cs[kMaxChunk * kVecGroup];
-  for (int t = threadIdx.x; t < nk * nv; t += blockDim.x)
-    cs[t] = coef[(t / nv) * ldc + (t % nv)];
-  __syncthreads();
+    k_accum(long n2, int nk, ChunkPtrs R, ChunkCoef C, double2 *__restrict__ V) {
   for (long j = blockIdx.x * (long)blockDim.x + threadIdx.x; j < n2;
        j += (long)gridDim.x * blockDim.x) {
-    double2 acc[kVecGroup];
+    double2 acc[NV];
 #pragma unroll
-    for (int e = 0; e < kVecGroup; e++)
-      if (e < nv) acc[e] = V[e * n2 + j];
-    for (int k = 0; k < nk; k++) {
-      const double2 r = R.r[k][j];
+    for (int e = 0; e < NV; e++) acc[e] = V[e * n2 + j];
 #pragma unroll
-      for (int e = 0; e < kVecGroup; e++)
-        if (e < nv) {
-          const double cf = cs[k * nv + e];
-          acc[e].x = fma(cf, r.x, acc[e].x);
-          acc[e].y = fma(cf, r.y, acc[e].y);
+    for (int k = 0; k < kMaxChunk; k++) {
+      if (k < nk) {
+        const double2 r = __ldg(R.r[k] + j);
+#pragma unroll
+        for (int e = 0; e < NV; e++) {
+          acc[e].x = fma(C.c[k][e], r.x, acc[e].x);
+          acc[e].y = fma(C.c[k][e], r.y, acc[e].y);
         }
+      }
     }
 #pragma unroll
-    for (int e = 0; e < kVecGroup; e++)
-      if (e < nv) V[e * n2 + j] = acc[e];
+    for (int e = 0; e < NV; e++) V[e * n2 + j] = acc[e];
+  }
+}
+
+static void launch_accum(int nv, unsigned grid, cudaStream_t s, long n2, int nk,
+                         const ChunkPtrs &R, const ChunkCoef &C, double2 *V) {
+  switch (nv) {
+#define TBGPU_ACCUM_CASE(N) \
+  case N: k_accum<N><<<grid, 256, 0, s>>>(n2, nk, R, C, V); break;
+    TBGPU_ACCUM_CASE(1) TBGPU_ACCUM_CASE(2) TBGPU_ACCUM_CASE(3) TBGPU_ACCUM_CASE(4)
+    TBGPU_ACCUM_CASE(5) TBGPU_ACCUM_CASE(6) TBGPU_ACCUM_CASE(7) TBGPU_ACCUM_CASE(8)
+    TBGPU_ACCUM_CASE(9) TBGPU_ACCUM_CASE(10) TBGPU_ACCUM_CASE(11) TBGPU_ACCUM_CASE(12)
+    TBGPU_ACCUM_CASE(13) TBGPU_ACCUM_CASE(14) TBGPU_ACCUM_CASE(15) TBGPU_ACCUM_CASE(16)
+#undef TBGPU_ACCUM_CASE
+    default: break;
   }
 }
 
@@ -519,10 +535,6 @@ int solve(Ctx &c, const SolveArgs &A, const double *r0_dev, double *values, int 
     }
     // bet of the first pass up to maxit is needed on the host
     if (maxit > final_it) maxit = final_it;
-    double *d_coef = nullptr;
-    SOLVE_CUDA(cudaMalloc(&d_coef, sizeof(double) * coef.size()));
-    SOLVE_CUDA(cudaMemcpyAsync(d_coef, coef.data(), sizeof(double) * coef.size(),
-                               cudaMemcpyHostToDevice, s));
     // chunk size limited by free memory
     size_t fre = 0, tot = 0;
     cudaMemGetInfo(&fre, &tot);
@@ -542,8 +554,10 @@ int solve(Ctx &c, const SolveArgs &A, const double *r0_dev, double *values, int 
         for (int k = 0; k < nk; k++) P.r[k] = ring[(it0 + k) % S2];
         for (int g = 0; g < nvec; g += kVecGroup) {
           const int nv = std::min(kVecGroup, nvec - g);
-          k_accum<<<rg, 256, 0, s>>>(n2, nk, nv, P, d_coef + size_t(it0) * nvec + g, nvec,
-                                     reinterpret_cast<double2 *>(V_dev) + size_t(g) * n2);
+          ChunkCoef C{};
+          for (int k = 0; k < nk; k++)
+            for (int e = 0; e < nv; e++) C.c[k][e] = coef[size_t(it0 + k) * nvec + g + e];
+          launch_accum(nv, rg, s, n2, nk, P, C, reinterpret_cast<double2 *>(V_dev) + size_t(g) * n2);
           launches++;
         }
         it0 = it + 1;
@@ -551,7 +565,6 @@ int solve(Ctx &c, const SolveArgs &A, const double *r0_dev, double *values, int 
     }
     cudaEventRecord(tm.t3, s);
     SOLVE_CUDA(cudaStreamSynchronize(s));
-    cudaFree(d_coef);
     cudaEventElapsedTime(&ms, tm.t2, tm.t3);
     c.stats.vectors_ms = ms;
   }
