@@ -160,6 +160,44 @@ int tbgpu_eigensolve_lanczos_dev(tbgpu_ctx *ctx, int ConvCheckStartIter,
                                  int *iterations, double *vectors_dev,
                                  int max_vectors);
 
+/* Eigenvalues in (vl, vu] of an n x n complex Hermitian band matrix with kd
+ * subdiagonals, lower band storage as LAPACK's UPLO='L' (column j holds rows
+ * j..j+kd at ab[(j*(kd+1) + i-j)*2 + {0,1}], interleaved complex): the
+ * solve the block Lanczos driver uses in place of zhbevx RANGE='V'
+ * (eigen/src/lanczos_blk.c:891-991).  Host only.  w receives up to cap
+ * values ascending; returns how many lie in the window. */
+int tbgpu_band_eigenvalues(int n, int kd, const double *ab, double vl, double vu,
+                           double abstol, double *w, int cap);
+
+/* Block Lanczos eigenvalues with the semantics of eigensolve_blk_lanczos
+ * (eigen/src/lanczos_blk.c:2145-2540, block_lanczos_blocktridiagonal
+ * 1412-1678): block size p (1..8), start block r0[p][dimension] (the
+ * reference draws it with rand(); here the caller supplies it), the band
+ * matrix solved in (emin1,emax1] and (emin2,emax2] every ConvCheckSkipRate
+ * steps after ConvCheckStartIter, convergence by Method 4 (values that
+ * repeat between checks to `tolerance`), stop when both windows have their
+ * requested counts, after max_no_success fruitless steps (<= 0: no limit)
+ * or at imax steps.  values[>= requested1 + requested2] receives the
+ * eigenvalues ascending; found_vb / found_cb the counts per window;
+ * *iterations the block steps.  Returns the number of eigenvalues or a
+ * negative error (TBGPU_E_NUMERIC when a block loses rank: deflation is not
+ * supported).  Eigenvectors are not computed. */
+int tbgpu_eigensolve_blk_lanczos(tbgpu_ctx *ctx, int ConvCheckStartIter,
+                                 int ConvCheckSkipRate, int imax, int requested1,
+                                 int requested2, double emin1, double emax1,
+                                 double emin2, double emax2, double tolerance,
+                                 int p, int max_no_success,
+                                 const tbgpu_dcomplex *r0, double *values,
+                                 int *found_vb, int *found_cb, int *iterations);
+int tbgpu_eigensolve_blk_lanczos_dev(tbgpu_ctx *ctx, int ConvCheckStartIter,
+                                     int ConvCheckSkipRate, int imax,
+                                     int requested1, int requested2,
+                                     double emin1, double emax1, double emin2,
+                                     double emax2, double tolerance, int p,
+                                     int max_no_success, const double *r0_dev,
+                                     double *values, int *found_vb,
+                                     int *found_cb, int *iterations);
+
 /* Tridiagonal matrix of the last solve: alpha[n], beta[n] (n <= cap). */
 int tbgpu_get_tridiagonal(const tbgpu_ctx *ctx, double *alpha, double *beta,
                           int cap);

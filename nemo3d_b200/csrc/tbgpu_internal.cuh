@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <complex>
 #include <cstdint>
 #include <vector>
 
@@ -95,6 +96,11 @@ int set_error(int code);
     cudaError_t e_ = (call);                                       \
     if (e_ != cudaSuccess) return ::tbgpu::set_error(TBGPU_E_CUDA); \
   } while (0)
+
+// band_eig.cu: eigenvalues in (vl, vu] of a Hermitian band matrix (lower
+// band storage, ldab = kd + 1), ascending
+int band_eigenvalues(int n, int kd, const std::complex<double> *ab, double vl, double vu,
+                     double abstol, std::vector<double> &w);
 
 // topology.cu
 int build_topology(Ctx &c);

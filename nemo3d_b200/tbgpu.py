@@ -69,6 +69,8 @@ def _lib():
         L.tbgpu_error_string.argtypes = [ip]
         L.tbgpu_prepare_params.argtypes = [ip, ip, vp, vp, dp, dp, vp]
         L.tbgpu_set_bloch_k.argtypes = [vp, C.POINTER(C.c_double)]
+        L.tbgpu_eigensolve_blk_lanczos.argtypes = [vp, ip, ip, ip, ip, ip, dp, dp, dp, dp, dp,
+                                                   ip, ip, vp, vp, vp, vp, vp]
         L.tbgpu_ctx_create.argtypes = [C.POINTER(_Geom), C.POINTER(_Model), C.POINTER(vp)]
         L.tbgpu_ctx_create_dev.argtypes = [C.POINTER(_Geom), C.POINTER(_Model), C.POINTER(vp)]
         L.tbgpu_ctx_destroy.argtypes = [vp]
@@ -286,6 +288,27 @@ class Hamiltonian:
         if rc:
             raise TbgpuError(rc, "tbgpu_export_hamiltonian")
         return ons, blk
+
+    def eigensolve_blk_lanczos(self, r0_block, ConvCheckStartIter=200, ConvCheckSkipRate=50,
+                               imax=2000, requested1=1, requested2=1, emin1=-0.6, emax1=0.2,
+                               emin2=1.4, emax2=2.0, tolerance=1e-7, max_no_success=0):
+        """Block Lanczos (eigensolve_blk_lanczos).  r0_block: host start block,
+        shape (p, 2*dimension) doubles.  Returns values (ascending),
+        found_vb, found_cb, iterations."""
+        r0 = np.ascontiguousarray(r0_block, np.float64)
+        p = r0.shape[0]
+        if r0.ndim != 2 or r0.shape[1] != 2 * self.n:
+            raise ValueError("r0_block must have shape (p, 2*dimension)")
+        vals = np.zeros(max(1, requested1 + requested2))
+        f1, f2, it = C.c_int(), C.c_int(), C.c_int()
+        rc = _lib().tbgpu_eigensolve_blk_lanczos(
+            self._ctx, ConvCheckStartIter, ConvCheckSkipRate, imax, requested1, requested2,
+            emin1, emax1, emin2, emax2, tolerance, p, max_no_success, _p(r0), _p(vals),
+            C.byref(f1), C.byref(f2), C.byref(it))
+        if rc < 0:
+            raise TbgpuError(rc, "tbgpu_eigensolve_blk_lanczos")
+        return {"values": vals[:rc].copy(), "found_vb": f1.value, "found_cb": f2.value,
+                "iterations": it.value}
 
     def set_bloch_k(self, k):
         """Bloch vector (reference units) for periodic structures; None or

@@ -209,3 +209,118 @@ def tridiag_eigs(d, e, vl, vu, abstol=1e-13):
     w = np.zeros(len(d))
     n = lib().orc_tridiag_eigs(len(d), _p(d), _p(e), vl, vu, abstol, _p(w))
     return w[:n].copy()
+
+
+def block_lanczos(hx, r0_block, imax=400, req=(1, 1), erange1=(-1, 0), erange2=(1, 2),
+                  tol=1e-7, conv_start=200, conv_skip=50, max_no_success=0):
+    """eigensolve_blk_lanczos restated with numpy (test infrastructure only).
+
+    Follows NEMO_3D/eigen/src/lanczos_blk.c: block_Lanczos_QR (273-357,
+    modified Gram-Schmidt), single_iteration (392-550, no deflation),
+    block_lanczos_blocktridiagonal (1412-1678: band storage, checks every
+    conv_skip steps after conv_start, n_nosuccess, stop rule) and
+    find_block_converged_eigvalues_Method4 (553-634).  The window
+    eigenvalues of the band matrix come from numpy's dense Hermitian solver
+    (the reference calls zhbevx).  In the valence window the reference takes
+    W[M-i], i = 0.., one past the last value found; this takes the highest
+    values W[M-1-i].  hx(x) maps a complex vector to H x.
+    """
+    Rb = np.array([r[0::2] + 1j * r[1::2] for r in np.asarray(r0_block, np.float64)])
+    p, n = Rb.shape
+
+    def qr(R):
+        Q = np.zeros_like(R)
+        B = np.zeros((p, p), complex)
+        g = np.sqrt(np.vdot(R[0], R[0]).real)
+        B[0, 0] = g
+        Q[0] = R[0] / g
+        for i in range(1, p):
+            r2 = R[i].copy()
+            for k in range(i):
+                b = np.vdot(Q[k], r2)
+                B[k, i] = b
+                r2 = r2 - b * Q[k]
+            g = np.sqrt(np.vdot(r2, r2).real)
+            B[i, i] = g
+            Q[i] = r2 / g
+        return Q, B
+
+    Q, _ = qr(Rb)
+    Qo = np.zeros_like(Q)
+    blocks_a, blocks_b = [], []
+    old1, old2, conv1, conv2 = [], [], [], []
+    nos = [0, 0]
+    mns = max_no_success if max_no_success > 0 else 1 << 30
+    skip, it = 0, 0
+
+    def method4(fresh, old, conv, requested, k):
+        tmp, olds = [], list(old)
+        for v in fresh:
+            for jj, o in enumerate(olds):
+                if abs(v - o) < tol:
+                    tmp.append(v)
+                    olds[jj] = 500.0
+                    break
+            if len(tmp) == requested:
+                break
+        for ci in range(len(conv)):
+            for tj in range(len(tmp)):
+                if abs(conv[ci] - tmp[tj]) < 100 * tol:
+                    conv[ci] = tmp[tj]
+                    tmp[tj] = 500.0
+                    break
+        for t in tmp:
+            if abs(t) < 490.0:
+                conv.append(t)
+                nos[k] = 0
+                if len(conv) == requested:
+                    break
+        old[:] = fresh
+
+    def window(T, lo, hi):
+        w = np.linalg.eigvalsh(T)
+        return w[(w > lo) & (w <= hi)]
+
+    B = None
+    while True:
+        if it != 0:
+            Q, B = qr(Rb)
+        Rb = np.array([hx(q) for q in Q])
+        if it != 0:
+            Rb = Rb - (B.conj() @ Qo)           # R_i -= sum_k conj(B[i,k]) Qold_k
+        A = np.array([[np.vdot(Q[i], Rb[j]) for j in range(p)] for i in range(p)])
+        A = np.tril(A) + np.tril(A, -1).conj().T
+        A[np.diag_indices(p)] = A.diagonal().real
+        Rb = Rb - A.T @ Q                        # R_i -= sum_k Q_k A[k, i]
+        Qo = Q
+        blocks_a.append(A)
+        if it != 0:
+            blocks_b.append(B)
+        skip += 1
+        if conv_start < it:
+            if len(conv1) < req[0]:
+                nos[0] += 1
+            if len(conv2) < req[1]:
+                nos[1] += 1
+        if conv_start < it and conv_skip <= skip:
+            skip = 0
+            m = len(blocks_a)
+            T = np.zeros((m * p, m * p), complex)
+            for k, Ak in enumerate(blocks_a):
+                T[k * p:(k + 1) * p, k * p:(k + 1) * p] = Ak
+            for k, Bk in enumerate(blocks_b):   # coupling of block k+1 to block k
+                T[(k + 1) * p:(k + 2) * p, k * p:(k + 1) * p] = np.triu(Bk)
+                T[k * p:(k + 1) * p, (k + 1) * p:(k + 2) * p] = np.triu(Bk).conj().T
+            if req[0] > 0 and len(conv1) < req[0]:
+                w = window(T, *erange1)
+                method4(list(w[::-1][:req[0] + 1]), old1, conv1, req[0], 0)
+            if req[1] > 0 and len(conv2) < req[1]:
+                w = window(T, *erange2)
+                method4(list(w[:req[1] + 1]), old2, conv2, req[1], 1)
+        done = (len(conv1) >= req[0] and len(conv2) >= req[1]) or it + 2 == imax
+        stalled = nos[0] >= mns or nos[1] >= mns
+        it += 1
+        if done or stalled or it + 1 >= imax:
+            break
+    return dict(evals=np.sort(np.array(conv1 + conv2)), found_vb=len(conv1),
+                found_cb=len(conv2), iterations=it)

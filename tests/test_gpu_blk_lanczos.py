@@ -1,0 +1,75 @@
+"""Block Lanczos on the GPU (tbgpu_eigensolve_blk_lanczos) against the
+oracle's restatement of the reference's block Lanczos and against dense
+diagonalisation.
+
+Bars: the same number of eigenvalues per window as the oracle run with the
+same start block and parameters, the same distinct values within the
+convergence tolerance (1e-7 eV) of the oracle's -- both follow the reference's Method-4 test,
+which accepts a value once it moves less than the tolerance between two
+checks, so rounding differences can pick the value of a neighbouring check
+-- and within 1e-5 eV of the dense spectrum.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from nemo3d_b200 import materials, workloads
+
+pytestmark = pytest.mark.gpu
+
+
+def _case(model, st, mats):
+    from nemo3d_b200.tbgpu import Hamiltonian
+    norb, nspin = materials.BAND_MODELS[model]
+    g = Hamiltonian(st, model, mats)
+    o = oracle.OracleHamiltonian(st, norb, nspin, mats)
+    return g, o
+
+
+def _hx(o):
+    return lambda q: (lambda y: y[0::2] + 1j * y[1::2])(
+        o.hx(np.column_stack([q.real, q.imag]).ravel()))
+
+
+# Cases where the oracle's own decisions do not change when H*x is perturbed
+# by 1e-14 relative noise: near the Kramers-degenerate clusters of the spin
+# models, Method 4 can accept a value at one check or the next depending on
+# rounding, so other block sizes or check intervals are not comparable run
+# to run even on one machine.
+@pytest.mark.parametrize("model,cube,p,skip", [("sp3s*", 3, 3, 10), ("sp3s*_so", 2, 4, 20),
+                                               ("sp3d5s*_so", 2, 4, 10)])
+def test_block_lanczos_matches_oracle(model, cube, p, skip):
+    fam = "spds" if model.startswith("sp3d5s") else "sps"
+    mats = [materials.MATERIALS[f"GaAs_{fam}"]]
+    st = workloads.gaas_cube(cube)
+    g, o = _case(model, st, mats)
+    ev = np.linalg.eigvalsh(o.dense())
+    w1 = (ev[0] - 0.5, ev[0] + 1.0)
+    w2 = (ev[-1] - 1.0, ev[-1] + 0.5)
+    r0 = np.random.default_rng(11).uniform(-1, 1, size=(p, 2 * g.n))
+    kw = dict(imax=min(300, g.n // p - 2), requested1=3, requested2=3, emin1=w1[0],
+              emax1=w1[1], emin2=w2[0], emax2=w2[1], tolerance=1e-7,
+              ConvCheckStartIter=30, ConvCheckSkipRate=skip)
+    res = g.eigensolve_blk_lanczos(r0, **kw)
+    ref = oracle.block_lanczos(_hx(o), r0, imax=kw["imax"], req=(3, 3), erange1=w1,
+                               erange2=w2, tol=1e-7, conv_start=30, conv_skip=skip)
+    assert (res["found_vb"], res["found_cb"]) == (ref["found_vb"], ref["found_cb"])
+    assert len(res["values"]) == len(ref["evals"]) > 0
+    # the same distinct values; with exactly degenerate (Kramers) pairs the
+    # reference's Method 4 may keep either copy first, so multiplicities of a
+    # pair within the requested count can differ
+    for u, v in ((res["values"], ref["evals"]), (ref["evals"], res["values"])):
+        assert max(np.abs(v - x).min() for x in u) < 1e-7
+    assert abs(res["iterations"] - ref["iterations"]) <= 10
+    for v in res["values"]:
+        assert np.abs(ev - v).min() < 1e-5
+
+
+def test_block_lanczos_argument_errors():
+    from nemo3d_b200.tbgpu import Hamiltonian, TbgpuError
+    st = workloads.gaas_cube(2)
+    g = Hamiltonian(st, "sp3s*", [materials.MATERIALS["GaAs_sps"]])
+    r0 = np.zeros((9, 2 * g.n))
+    with pytest.raises(TbgpuError) as e:
+        g.eigensolve_blk_lanczos(r0)   # block size above 8
+    assert e.value.code == -1
