@@ -129,6 +129,15 @@ int tbgpu_set_bloch_k(tbgpu_ctx *ctx, const double *k);
 int tbgpu_hx_dev(tbgpu_ctx *ctx, double shift, const double *x_dev,
                  double *y_dev);
 
+/* Y_v = (H - shift) X_v for a block of p <= 8 device vectors stored one
+ * after the other ([p][dimension] complex): the block product the block
+ * Lanczos driver needs (the reference's matmat_mult,
+ * nemo3d/src/base/h_cmat_mult.c:21).  For the 10-orbital models at the Gamma
+ * point one launch applies each staged bond block to all p vectors;
+ * otherwise it runs p H*x launches.  Asynchronous on the context stream. */
+int tbgpu_hx_block_dev(tbgpu_ctx *ctx, int p, double shift, const double *x_dev,
+                       double *y_dev);
+
 /* Lanczos eigensolver with the semantics of eigensolve_lanczos
  * (eigen/src/lanczos.c:1823-2089): plain Lanczos, convergence test every
  * ConvCheckSkipRate iterations after ConvCheckStartIter on the last two

@@ -6,7 +6,7 @@
 // One block step, p vectors at a time (Q: current block, Qold: previous
 // block, R: residual block, all [p][n] complex in HBM):
 //   [Q, B] = qr(R)            (not at the first step)
-//   R_i    = H Q_i            (p launches of the H*x kernel)
+//   R_i    = H Q_i            (one multi-vector H*x launch, spmm_async.cu)
 //   R     -= Qold B^H         (not at the first step)
 //   A      = Q^H R            (Hermitian p x p; lower triangle computed)
 //   R     -= Q A
@@ -306,11 +306,10 @@ static int blk_run(Ctx &c, const BlkArgs &A, const double *r0_dev, std::vector<d
   bool converged = false;
   while (!rc) {
     if (it != 0 && qr(B)) break;
-    for (int i = 0; i < P && !rc; i++)
-      if (launch_spmv(c, reinterpret_cast<const double *>(Q + size_t(i) * n2),
-                      reinterpret_cast<double *>(R + size_t(i) * n2), 0.0, nullptr, 0, nullptr,
-                      0, s))
-        rc = TBGPU_E_CUDA;
+    // R_i = H Q_i, the block at once
+    if (launch_spmm(c, P, reinterpret_cast<const double *>(Q), 2 * n2,
+                    reinterpret_cast<double *>(R), 2 * n2, 0.0, s))
+      rc = TBGPU_E_CUDA;
     if (rc) break;
     if (it != 0) {  // R -= Qold B^H
       Mat M(size_t(P) * P);

@@ -24,34 +24,15 @@
 
 #include "tbgpu_internal.cuh"
 #include "reduce.cuh"
+#include "stage.cuh"
 #include "zincblende.cuh"
 
 namespace tbgpu {
 
 namespace {
 
+using namespace stage;
 constexpr int kNorb = 10;
-constexpr int kAPW = 3;      // atoms per warp
-
-__device__ __forceinline__ uint32_t smem_addr(const void *p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ void cp16(void *dst, const void *src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src)
-               : "memory");
-}
-// 16-byte copy that reads `bytes` (16 or 0) from global memory and fills the
-// rest of the chunk with zeros: a missing neighbour costs no branch
-__device__ __forceinline__ void cp16z(void *dst, const void *src, int bytes) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_addr(dst)), "l"(src),
-               "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
 
 __device__ __forceinline__ void cfma_r(double2 &acc, double v, double2 a) {
   acc.x = fma(v, a.x, acc.x);
@@ -80,35 +61,6 @@ struct Layout {
   static __device__ __forceinline__ int xs(int i) { return i * ATOM + 4 * BLK * 8; }
   static __device__ __forceinline__ int ons(int i) { return i * ATOM + 4 * BLK * 8 + 5 * NB * 16; }
 };
-
-struct Meta {
-  int nb[kAPW][4];
-  int m[kAPW];  // -1: no atom
-  int a0;       // first atom of the group
-};
-
-// Group g of the work order: up to three consecutive atoms of one pencil.
-__device__ __forceinline__ Meta load_meta(long g, long ngroups, const int2 *__restrict__ groups,
-                                          const int4 *__restrict__ nbr,
-                                          const unsigned char *__restrict__ site_m) {
-  Meta M;
-  int2 e = make_int2(0, 0);
-  if (g < ngroups) e = __ldg(groups + g);
-  M.a0 = e.x;
-#pragma unroll
-  for (int i = 0; i < kAPW; i++) {
-    const long a = long(e.x) + i;
-    if (i < e.y) {
-      const int4 v = __ldg(nbr + a);
-      M.nb[i][0] = v.x; M.nb[i][1] = v.y; M.nb[i][2] = v.z; M.nb[i][3] = v.w;
-      M.m[i] = __ldg(site_m + a);
-    } else {
-      M.nb[i][0] = M.nb[i][1] = M.nb[i][2] = M.nb[i][3] = -1;
-      M.m[i] = -1;
-    }
-  }
-  return M;
-}
 
 // Issue the copies of group g into one stage (all lanes; no wait).
 template <class L>

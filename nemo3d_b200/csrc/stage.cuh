@@ -1,0 +1,66 @@
+// Shared-memory staging helpers of the warp-staged H*x kernels
+// (spmv_async.cu, spmm_async.cu): 16-byte cp.async copies, and the group
+// metadata of the context's work order (up to three consecutive atoms of
+// one k-pencil of cells per group).
+#pragma once
+
+#include <cstdint>
+
+#include "tbgpu_internal.cuh"
+
+namespace tbgpu {
+namespace stage {
+
+constexpr int kAPW = 3;  // atoms per warp (one lane per orbital, 10 orbitals)
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void cp16(void *dst, const void *src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src)
+               : "memory");
+}
+// 16-byte copy that reads `bytes` (16 or 0) from global memory and fills the
+// rest of the chunk with zeros: a missing neighbour costs no branch
+__device__ __forceinline__ void cp16z(void *dst, const void *src, int bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_addr(dst)), "l"(src),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+struct Meta {
+  int nb[kAPW][4];
+  int m[kAPW];  // -1: no atom
+  int a0;       // first atom of the group
+};
+
+// Group g of the work order: up to three consecutive atoms of one pencil.
+__device__ __forceinline__ Meta load_meta(long g, long ngroups, const int2 *__restrict__ groups,
+                                          const int4 *__restrict__ nbr,
+                                          const unsigned char *__restrict__ site_m) {
+  Meta M;
+  int2 e = make_int2(0, 0);
+  if (g < ngroups) e = __ldg(groups + g);
+  M.a0 = e.x;
+#pragma unroll
+  for (int i = 0; i < kAPW; i++) {
+    const long a = long(e.x) + i;
+    if (i < e.y) {
+      const int4 v = __ldg(nbr + a);
+      M.nb[i][0] = v.x; M.nb[i][1] = v.y; M.nb[i][2] = v.z; M.nb[i][3] = v.w;
+      M.m[i] = __ldg(site_m + a);
+    } else {
+      M.nb[i][0] = M.nb[i][1] = M.nb[i][2] = M.nb[i][3] = -1;
+      M.m[i] = -1;
+    }
+  }
+  return M;
+}
+
+}  // namespace stage
+}  // namespace tbgpu

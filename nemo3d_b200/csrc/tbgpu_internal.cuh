@@ -97,6 +97,10 @@ int set_error(int code);
     if (e_ != cudaSuccess) return ::tbgpu::set_error(TBGPU_E_CUDA); \
   } while (0)
 
+// spmm_async.cu: y + v*ystride = (H - shift)(x + v*xstride) for v < p <= 8
+int launch_spmm(Ctx &c, int p, const double *x, long xstride, double *y, long ystride,
+                double shift, cudaStream_t s);
+
 // band_eig.cu: eigenvalues in (vl, vu] of a Hermitian band matrix (lower
 // band storage, ldab = kd + 1), ascending
 int band_eigenvalues(int n, int kd, const std::complex<double> *ab, double vl, double vu,

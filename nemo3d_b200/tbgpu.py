@@ -69,6 +69,7 @@ def _lib():
         L.tbgpu_error_string.argtypes = [ip]
         L.tbgpu_prepare_params.argtypes = [ip, ip, vp, vp, dp, dp, vp]
         L.tbgpu_set_bloch_k.argtypes = [vp, C.POINTER(C.c_double)]
+        L.tbgpu_hx_block_dev.argtypes = [vp, ip, dp, vp, vp]
         L.tbgpu_eigensolve_blk_lanczos.argtypes = [vp, ip, ip, ip, ip, ip, dp, dp, dp, dp, dp,
                                                    ip, ip, vp, vp, vp, vp, vp]
         L.tbgpu_ctx_create.argtypes = [C.POINTER(_Geom), C.POINTER(_Model), C.POINTER(vp)]
@@ -216,6 +217,13 @@ class Hamiltonian:
         rc = _lib().tbgpu_hx_dev(self._ctx, float(shift), C.c_void_p(x_ptr), C.c_void_p(y_ptr))
         if rc:
             raise TbgpuError(rc, "tbgpu_hx_dev")
+
+    def hx_block_dev(self, p: int, x_ptr: int, y_ptr: int, shift: float = 0.0):
+        """Y_v = (H - shift) X_v for p device vectors stored back to back."""
+        rc = _lib().tbgpu_hx_block_dev(self._ctx, int(p), float(shift), C.c_void_p(x_ptr),
+                                       C.c_void_p(y_ptr))
+        if rc:
+            raise TbgpuError(rc, "tbgpu_hx_block_dev")
 
     # -- eigensolver ----------------------------------------------------------
     def eigensolve_lanczos(self, r_0, ConvCheckStartIter=200, ConvCheckSkipRate=50,

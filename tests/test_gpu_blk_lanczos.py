@@ -73,3 +73,27 @@ def test_block_lanczos_argument_errors():
     with pytest.raises(TbgpuError) as e:
         g.eigensolve_blk_lanczos(r0)   # block size above 8
     assert e.value.code == -1
+
+
+@pytest.mark.parametrize("model,p", [("sp3d5s*_so", 2), ("sp3d5s*_so", 3), ("sp3d5s*_so", 6),
+                                     ("sp3d5s*", 4), ("sp3d5s*_so", 8), ("sp3s*_so", 3)])
+def test_block_hx_matches_oracle(model, p):
+    """tbgpu_hx_block_dev vs the oracle's H*x per vector (45e-12 of max|H|)."""
+    import torch
+    from nemo3d_b200.tbgpu import Hamiltonian
+    fam = "spds" if model.startswith("sp3d5s") else "sps"
+    mats = [materials.MATERIALS[f"GaAs_{fam}"], materials.MATERIALS[f"InAs_{fam}"]]
+    st = workloads.dome_in_box(cells=(7, 6, 5), base_nm=2.4, height_nm=1.0, wl_z_nm=1.2,
+                               sigma_frac=0.02, seed=5)
+    norb, nspin = materials.BAND_MODELS[model]
+    g = Hamiltonian(st, model, mats)
+    o = oracle.OracleHamiltonian(st, norb, nspin, mats)
+    X = np.stack([workloads.random_start(g.n, seed=20 + v) for v in range(p)])
+    xd = torch.from_numpy(X).cuda()
+    yd = torch.empty_like(xd)
+    g.hx_block_dev(p, xd.data_ptr(), yd.data_ptr(), shift=0.3)
+    torch.cuda.synchronize()
+    Y = yd.cpu().numpy()
+    scale = max(np.abs(o.onsite).max(), np.abs(o.blocks).max())
+    for v in range(p):
+        assert np.abs(Y[v] - o.hx(X[v], shift=0.3)).max() <= 45e-12 * scale, v
