@@ -116,6 +116,14 @@ long tbgpu_dimension(const tbgpu_ctx *ctx); /* complex length n_atoms * nb */
 void tbgpu_matvect_mult(const int **argList, tbgpu_dcomplex *y,
                         const tbgpu_dcomplex *x);
 
+/* Precision of the stored Hamiltonian: 64 (default) or 32 bits, set before
+ * tbgpu_build_hamiltonian.  32 is the reference's HamMemorySave build
+ * (nemo3d/src/base/HamZincBlende.h:51-66, Hmult_stored.c:629, 910): the
+ * bond blocks and on-site records are rounded to float after assembly and
+ * widened again inside H*x, whose arithmetic and vectors stay double.  Half
+ * the Hamiltonian's bytes; entries carry float rounding (~6e-8 relative). */
+int tbgpu_set_ham_precision(tbgpu_ctx *ctx, int bits);
+
 /* Bloch vector for periodic structures (geo_struct::phasePeriodic,
  * nemo3d/src/base/geo_struct.h:811-826, used by Hmult_stored.c:386-437): a
  * bond that crosses the periodic boundary by images w (-1/0/+1 per axis)

@@ -308,15 +308,40 @@ static int assemble_t(Ctx &c) {
   return TBGPU_OK;
 }
 
+// round the assembled store to float (the reference's HamMemorySave build
+// keeps Hdd, Hdu, Hds and Hu as float: HamZincBlende.h:51-66)
+__global__ void k_to_float(long n, const double *__restrict__ in, float *__restrict__ out) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+       i += (long)gridDim.x * blockDim.x)
+    out[i] = float(in[i]);
+}
+
+static int to_float(Ctx &c, long n, const double *in, float **out) {
+  TB_CUDA(cudaMalloc(out, sizeof(float) * n));
+  k_to_float<<<1184, 256, 0, c.stream>>>(n, in, *out);
+  TB_CUDA(cudaGetLastError());
+  return TBGPU_OK;
+}
+
 int assemble(Ctx &c) {
   const long na = c.natoms;
   TB_CUDA(cudaMalloc(&c.d_blocks, sizeof(double) * na * 4 * c.norb * c.norb));
   TB_CUDA(cudaMalloc(&c.d_onsite, sizeof(double) * na * c.ons));
-  if (c.norb == 10 && c.nspin == 2) return assemble_t<10, 2>(c);
-  if (c.norb == 10 && c.nspin == 1) return assemble_t<10, 1>(c);
-  if (c.norb == 5 && c.nspin == 2) return assemble_t<5, 2>(c);
-  if (c.norb == 5 && c.nspin == 1) return assemble_t<5, 1>(c);
-  return set_error(TBGPU_E_UNSUPPORTED);
+  int rc = TBGPU_E_UNSUPPORTED;
+  if (c.norb == 10 && c.nspin == 2) rc = assemble_t<10, 2>(c);
+  else if (c.norb == 10 && c.nspin == 1) rc = assemble_t<10, 1>(c);
+  else if (c.norb == 5 && c.nspin == 2) rc = assemble_t<5, 2>(c);
+  else if (c.norb == 5 && c.nspin == 1) rc = assemble_t<5, 1>(c);
+  else return set_error(rc);
+  if (rc || !c.ham_fp32) return rc;
+  if ((rc = to_float(c, na * 4 * c.norb * c.norb, c.d_blocks, &c.d_blocks32))) return rc;
+  if ((rc = to_float(c, na * c.ons, c.d_onsite, &c.d_onsite32))) return rc;
+  TB_CUDA(cudaStreamSynchronize(c.stream));
+  cudaFree(c.d_blocks);
+  cudaFree(c.d_onsite);
+  c.d_blocks = nullptr;
+  c.d_onsite = nullptr;
+  return TBGPU_OK;
 }
 
 }  // namespace tbgpu

@@ -30,7 +30,8 @@ static void free_ctx(Ctx *c) {
   if (!c) return;
   void *ptrs[] = {c->d_type, c->d_dsp, c->d_par, c->d_par_ok, c->d_site_index, c->d_atom_site,
                   c->d_nbr, c->d_site_m, c->d_surface, c->d_onsite, c->d_blocks, c->d_partial,
-                  c->d_counter, c->d_status, c->d_x, c->d_y, c->d_phase, c->d_groups};
+                  c->d_counter, c->d_status, c->d_x, c->d_y, c->d_phase, c->d_groups,
+                  c->d_blocks32, c->d_onsite32};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -276,14 +277,21 @@ int tbgpu_export_hamiltonian(const tbgpu_ctx *ctx, double *onsite, double *block
   if (!c.built) return set_error(TBGPU_E_STATE);
   const size_t n = size_t(c.natoms);
   const int nb = c.nb, norb = c.norb;
-  if (blocks && cudaMemcpy(blocks, c.d_blocks, n * 4 * norb * norb * sizeof(double),
-                           cudaMemcpyDeviceToHost) != cudaSuccess)
+  // the single-precision store is exported widened to double
+  auto fetch = [&](double *dst, const double *src64, const float *src32, size_t count) -> bool {
+    if (!c.ham_fp32)
+      return cudaMemcpy(dst, src64, count * sizeof(double), cudaMemcpyDeviceToHost) == cudaSuccess;
+    std::vector<float> tmp(count);
+    if (cudaMemcpy(tmp.data(), src32, count * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)
+      return false;
+    for (size_t i = 0; i < count; i++) dst[i] = tmp[i];
+    return true;
+  };
+  if (blocks && !fetch(blocks, c.d_blocks, c.d_blocks32, n * 4 * norb * norb))
     return set_error(TBGPU_E_CUDA);
   if (!onsite) return TBGPU_OK;
   std::vector<double> rec(n * c.ons);
-  if (cudaMemcpy(rec.data(), c.d_onsite, rec.size() * sizeof(double), cudaMemcpyDeviceToHost) !=
-      cudaSuccess)
-    return set_error(TBGPU_E_CUDA);
+  if (!fetch(rec.data(), c.d_onsite, c.d_onsite32, rec.size())) return set_error(TBGPU_E_CUDA);
   std::memset(onsite, 0, sizeof(double) * n * nb * nb * 2);
   for (size_t a = 0; a < n; a++) {
     const double *r = rec.data() + a * c.ons;
@@ -317,6 +325,14 @@ int tbgpu_export_hamiltonian(const tbgpu_ctx *ctx, double *onsite, double *block
 int tbgpu_set_spmv_variant(tbgpu_ctx *ctx, int variant) {
   if (!ctx || variant < 0 || variant > 2) return set_error(TBGPU_E_ARG);
   C(ctx)->spmv_variant = variant;
+  return TBGPU_OK;
+}
+
+int tbgpu_set_ham_precision(tbgpu_ctx *ctx, int bits) {
+  if (!ctx || (bits != 32 && bits != 64)) return set_error(TBGPU_E_ARG);
+  Ctx &c = *C(ctx);
+  if (c.built) return set_error(TBGPU_E_STATE);
+  c.ham_fp32 = bits == 32;
   return TBGPU_OK;
 }
 

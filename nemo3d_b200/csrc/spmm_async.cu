@@ -250,12 +250,13 @@ int launch_ns(Ctx &c, int p, const double *x, long xs, double *y, long ys, doubl
 }  // namespace
 
 // y + v*ystride = (H - shift)(x + v*xstride), v < p (p <= 8; strides in
-// doubles).  Takes the block kernel for the 10-orbital models at the Gamma
-// point and p >= 2, one H*x launch per vector otherwise.
+// doubles).  Takes the block kernel for the 10-orbital models with the
+// double-precision store at the Gamma point and p >= 2, one H*x launch per
+// vector otherwise.
 int launch_spmm(Ctx &c, int p, const double *x, long xstride, double *y, long ystride,
                 double shift, cudaStream_t s) {
   if (p < 1 || p > 8) return set_error(TBGPU_E_ARG);
-  if (p >= 2 && c.norb == kNorb && !c.bloch && c.spmv_variant != 1)
+  if (p >= 2 && c.norb == kNorb && !c.bloch && !c.ham_fp32 && c.spmv_variant != 1)
     return c.nspin == 2 ? launch_ns<2>(c, p, x, xstride, y, ystride, shift, s)
                         : launch_ns<1>(c, p, x, xstride, y, ystride, shift, s);
   for (int v = 0; v < p; v++) {

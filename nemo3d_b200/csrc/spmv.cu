@@ -29,10 +29,12 @@ __device__ __forceinline__ void cfma_i(double2 &acc, double lam, double2 a) {
 
 // PHASE: bonds carry the Bloch phase phase[a*4+n] of H[a][nbr] (periodic
 // structures away from the Gamma point).
-template <int NORB, int NSPIN, int WPB, bool DOT, bool PHASE = false>
+// HT: element type of the stored Hamiltonian (double, or float for the
+// single-precision store; the arithmetic stays double).
+template <int NORB, int NSPIN, int WPB, bool DOT, bool PHASE = false, typename HT = double>
 __global__ void __launch_bounds__(WPB * 32)
     k_spmv(long natoms, const int4 *__restrict__ nbr, const unsigned char *__restrict__ site_m,
-           const double *__restrict__ onsite, const double *__restrict__ blocks,
+           const HT *__restrict__ onsite, const HT *__restrict__ blocks,
            const double2 *__restrict__ x, double2 *__restrict__ y, double shift,
            const double *__restrict__ xnorm, int xnorm_idx, double *partial,
            unsigned int *counter, double *alpha_out, int alpha_idx,
@@ -64,12 +66,12 @@ __global__ void __launch_bounds__(WPB * 32)
   __syncwarp();
   double dot = 0.0;
   if (act) {
-    const double *rec = onsite + a * ONS;
+    const HT *rec = onsite + a * ONS;
     double2 acc[NSPIN];
 #pragma unroll
-    for (int s = 0; s < NSPIN; s++) acc[s] = cmul_r(rec[s * NORB + o], xs[w][ai][4][s * NORB + o]);
+    for (int s = 0; s < NSPIN; s++) acc[s] = cmul_r(double(rec[s * NORB + o]), xs[w][ai][4][s * NORB + o]);
     // dangling-bond sp3 couplings among s, px, py, pz (surface atoms only)
-    if (o >= 1 && o <= 4 && rec[NB + 1] != 0.0) {
+    if (o >= 1 && o <= 4 && rec[NB + 1] != HT(0)) {
       const double sx = rec[NB + 2], sy = rec[NB + 3], sz = rec[NB + 4];
       const double xy = rec[NB + 5], xz = rec[NB + 6], yz = rec[NB + 7];
       double c1, c2, c3;
@@ -115,9 +117,9 @@ __global__ void __launch_bounds__(WPB * 32)
         tgt = part;
       }
       if (cat) {
-        const double *M = blocks + (a * 4 + n) * (NORB * NORB) + o * NORB;
+        const HT *M = blocks + (a * 4 + n) * (NORB * NORB) + o * NORB;
         double r[NORB];
-        if constexpr (NORB % 2 == 0) {
+        if constexpr (NORB % 2 == 0 && sizeof(HT) == 8) {
           // rows start on 16-byte boundaries when NORB is even (block = NORB^2
           // doubles, row = NORB doubles): 128-bit loads
 #pragma unroll
@@ -135,10 +137,10 @@ __global__ void __launch_bounds__(WPB * 32)
 #pragma unroll
           for (int s = 0; s < NSPIN; s++) cfma_r(tgt[s], r[k], xn[s * NORB + k]);
       } else {
-        const double *M = blocks + (long(nb[n]) * 4 + c_rev_slot[m][n]) * (NORB * NORB) + o;
+        const HT *M = blocks + (long(nb[n]) * 4 + c_rev_slot[m][n]) * (NORB * NORB) + o;
 #pragma unroll
         for (int k = 0; k < NORB; k++) {
-          const double v = __ldg(M + k * NORB);
+          const double v = double(__ldg(M + k * NORB));
 #pragma unroll
           for (int s = 0; s < NSPIN; s++) cfma_r(tgt[s], v, xn[s * NORB + k]);
         }
@@ -165,38 +167,48 @@ __global__ void __launch_bounds__(WPB * 32)
 
 constexpr int kWPB = 8;
 
-template <int NORB, int NSPIN>
-static int launch_t(Ctx &c, const double *x, double *y, double shift,
-                    const double *xnorm, int xidx, double *alpha_out, int aidx,
-                    cudaStream_t s) {
+template <int NORB, int NSPIN, typename HT>
+static int launch_ht(Ctx &c, const double *x, double *y, double shift,
+                     const double *xnorm, int xidx, double *alpha_out, int aidx,
+                     cudaStream_t s) {
   constexpr int APW = 32 / NORB;
   const long per_block = long(kWPB) * APW;
   const unsigned grid = unsigned((c.natoms + per_block - 1) / per_block);
   const double2 *X = reinterpret_cast<const double2 *>(x);
   double2 *Y = reinterpret_cast<double2 *>(y);
+  const HT *ons = ham_onsite<HT>(c), *blk = ham_blocks<HT>(c);
   if (alpha_out) {
     int rc = ensure_partials(c, int(grid));
     if (rc) return rc;
     if (c.bloch)
-      k_spmv<NORB, NSPIN, kWPB, true, true><<<grid, kWPB * 32, 0, s>>>(
-          c.natoms, c.d_nbr, c.d_site_m, c.d_onsite, c.d_blocks, X, Y, shift, xnorm, xidx,
-          c.d_partial, c.d_counter, alpha_out, aidx, c.d_phase);
+      k_spmv<NORB, NSPIN, kWPB, true, true, HT><<<grid, kWPB * 32, 0, s>>>(
+          c.natoms, c.d_nbr, c.d_site_m, ons, blk, X, Y, shift, xnorm, xidx, c.d_partial,
+          c.d_counter, alpha_out, aidx, c.d_phase);
     else
-      k_spmv<NORB, NSPIN, kWPB, true><<<grid, kWPB * 32, 0, s>>>(
-          c.natoms, c.d_nbr, c.d_site_m, c.d_onsite, c.d_blocks, X, Y, shift, xnorm, xidx,
-          c.d_partial, c.d_counter, alpha_out, aidx);
+      k_spmv<NORB, NSPIN, kWPB, true, false, HT><<<grid, kWPB * 32, 0, s>>>(
+          c.natoms, c.d_nbr, c.d_site_m, ons, blk, X, Y, shift, xnorm, xidx, c.d_partial,
+          c.d_counter, alpha_out, aidx);
   } else {
     if (c.bloch)
-      k_spmv<NORB, NSPIN, kWPB, false, true><<<grid, kWPB * 32, 0, s>>>(
-          c.natoms, c.d_nbr, c.d_site_m, c.d_onsite, c.d_blocks, X, Y, shift, xnorm, xidx,
-          nullptr, nullptr, nullptr, 0, c.d_phase);
+      k_spmv<NORB, NSPIN, kWPB, false, true, HT><<<grid, kWPB * 32, 0, s>>>(
+          c.natoms, c.d_nbr, c.d_site_m, ons, blk, X, Y, shift, xnorm, xidx, nullptr, nullptr,
+          nullptr, 0, c.d_phase);
     else
-      k_spmv<NORB, NSPIN, kWPB, false><<<grid, kWPB * 32, 0, s>>>(
-          c.natoms, c.d_nbr, c.d_site_m, c.d_onsite, c.d_blocks, X, Y, shift, xnorm, xidx,
-          nullptr, nullptr, nullptr, 0);
+      k_spmv<NORB, NSPIN, kWPB, false, false, HT><<<grid, kWPB * 32, 0, s>>>(
+          c.natoms, c.d_nbr, c.d_site_m, ons, blk, X, Y, shift, xnorm, xidx, nullptr, nullptr,
+          nullptr, 0);
   }
   TB_CUDA(cudaGetLastError());
   return TBGPU_OK;
+}
+
+template <int NORB, int NSPIN>
+static int launch_t(Ctx &c, const double *x, double *y, double shift,
+                    const double *xnorm, int xidx, double *alpha_out, int aidx,
+                    cudaStream_t s) {
+  return c.ham_fp32
+             ? launch_ht<NORB, NSPIN, float>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s)
+             : launch_ht<NORB, NSPIN, double>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
 }
 
 int launch_spmv(Ctx &c, const double *x, double *y, double shift, const double *xnorm,
@@ -212,28 +224,36 @@ int launch_spmv(Ctx &c, const double *x, double *y, double shift, const double *
   return set_error(TBGPU_E_UNSUPPORTED);
 }
 
+template <int NORB, int NSPIN, typename HT>
+static int launch_scratch_ht(Ctx &c, const double *x, double *y, double shift, double *partial,
+                             unsigned int *counter, int cap, double *dot_out, cudaStream_t s) {
+  constexpr int APW = 32 / NORB;
+  const long per_block = long(kWPB) * APW;
+  const long grid = (c.natoms + per_block - 1) / per_block;
+  if (grid > cap) return set_error(TBGPU_E_ARG);
+  const double2 *X = reinterpret_cast<const double2 *>(x);
+  double2 *Y = reinterpret_cast<double2 *>(y);
+  if (c.bloch)
+    k_spmv<NORB, NSPIN, kWPB, true, true, HT><<<unsigned(grid), kWPB * 32, 0, s>>>(
+        c.natoms, c.d_nbr, c.d_site_m, ham_onsite<HT>(c), ham_blocks<HT>(c), X, Y, shift,
+        nullptr, 0, partial, counter, dot_out, 0, c.d_phase);
+  else
+    k_spmv<NORB, NSPIN, kWPB, true, false, HT><<<unsigned(grid), kWPB * 32, 0, s>>>(
+        c.natoms, c.d_nbr, c.d_site_m, ham_onsite<HT>(c), ham_blocks<HT>(c), X, Y, shift,
+        nullptr, 0, partial, counter, dot_out, 0);
+  TB_CUDA(cudaGetLastError());
+  return TBGPU_OK;
+}
+
 // Lane-gather launch with the alpha dot reduced through caller-provided
 // scratch (partial[cap] doubles, zeroed counter).  Allocates nothing; fails
 // with TBGPU_E_ARG when the launch needs more than cap blocks.
 template <int NORB, int NSPIN>
 static int launch_scratch_t(Ctx &c, const double *x, double *y, double shift, double *partial,
                             unsigned int *counter, int cap, double *dot_out, cudaStream_t s) {
-  constexpr int APW = 32 / NORB;
-  const long per_block = long(kWPB) * APW;
-  const long grid = (c.natoms + per_block - 1) / per_block;
-  if (grid > cap) return set_error(TBGPU_E_ARG);
-  if (c.bloch)
-    k_spmv<NORB, NSPIN, kWPB, true, true><<<unsigned(grid), kWPB * 32, 0, s>>>(
-        c.natoms, c.d_nbr, c.d_site_m, c.d_onsite, c.d_blocks,
-        reinterpret_cast<const double2 *>(x), reinterpret_cast<double2 *>(y), shift, nullptr, 0,
-        partial, counter, dot_out, 0, c.d_phase);
-  else
-    k_spmv<NORB, NSPIN, kWPB, true><<<unsigned(grid), kWPB * 32, 0, s>>>(
-        c.natoms, c.d_nbr, c.d_site_m, c.d_onsite, c.d_blocks,
-        reinterpret_cast<const double2 *>(x), reinterpret_cast<double2 *>(y), shift, nullptr, 0,
-        partial, counter, dot_out, 0);
-  TB_CUDA(cudaGetLastError());
-  return TBGPU_OK;
+  return c.ham_fp32
+             ? launch_scratch_ht<NORB, NSPIN, float>(c, x, y, shift, partial, counter, cap, dot_out, s)
+             : launch_scratch_ht<NORB, NSPIN, double>(c, x, y, shift, partial, counter, cap, dot_out, s);
 }
 
 int launch_spmv_scratch(Ctx &c, const double *x, double *y, double shift, double *partial,

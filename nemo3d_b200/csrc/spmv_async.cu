@@ -43,30 +43,34 @@ __device__ __forceinline__ void cfma_i(double2 &acc, double lam, double2 a) {
   acc.y += lam * a.x;
 }
 
-template <int NSPIN, int WARPS, int STAGES>
+// HT: element type of the stored Hamiltonian (double, or float for the
+// single-precision store)
+template <int NSPIN, int WARPS, int STAGES, typename HT_ = double>
 struct Layout {
+  using HT = HT_;
+  static constexpr int HS = int(sizeof(HT));
   static constexpr int NB = kNorb * NSPIN;
   static constexpr int ONS = onsite_len(NB);
-  static constexpr int BLK = kNorb * kNorb;      // doubles per bond block
-  static constexpr int BLK_CH = BLK * 8 / 16;    // 16-byte chunks per block (50)
+  static constexpr int BLK = kNorb * kNorb;      // elements per bond block
+  static constexpr int BLK_CH = BLK * HS / 16;   // 16-byte chunks per block (50 or 25)
   static constexpr int X_CH = NB * 16 / 16;      // chunks per vector segment
-  static constexpr int ONS_CH = ONS * 8 / 16;    // chunks per on-site record
+  static constexpr int ONS_CH = ONS * HS / 16;   // chunks per on-site record
   // per-atom stride, padded by 48 bytes so the three atoms of a warp start
   // on different shared-memory banks
-  static constexpr int ATOM = 4 * BLK * 8 + 5 * NB * 16 + ONS * 8 + 48;
+  static constexpr int ATOM = 4 * BLK * HS + 5 * NB * 16 + ONS * HS + 48;
   static constexpr int STAGE = kAPW * ATOM;
   static constexpr int WARP = STAGES * STAGE;
   static constexpr int SMEM = WARPS * WARP;
   static __device__ __forceinline__ int blk(int i) { return i * ATOM; }
-  static __device__ __forceinline__ int xs(int i) { return i * ATOM + 4 * BLK * 8; }
-  static __device__ __forceinline__ int ons(int i) { return i * ATOM + 4 * BLK * 8 + 5 * NB * 16; }
+  static __device__ __forceinline__ int xs(int i) { return i * ATOM + 4 * BLK * HS; }
+  static __device__ __forceinline__ int ons(int i) { return i * ATOM + 4 * BLK * HS + 5 * NB * 16; }
 };
 
 // Issue the copies of group g into one stage (all lanes; no wait).
 template <class L>
 __device__ __forceinline__ void issue(unsigned char *st, long g, const Meta &M, int lane,
-                                      const double *__restrict__ onsite,
-                                      const double *__restrict__ blocks,
+                                      const typename L::HT *__restrict__ onsite,
+                                      const typename L::HT *__restrict__ blocks,
                                       const double2 *__restrict__ x) {
   constexpr int NB = L::NB;
 #pragma unroll
@@ -90,7 +94,7 @@ __device__ __forceinline__ void issue(unsigned char *st, long g, const Meta &M, 
             blocks + (long(b >= 0 ? b : a) * 4 + c_rev_slot[m][n]) * L::BLK);
 #pragma unroll
         for (int c = lane; c < L::BLK_CH; c += 32)
-          cp16z(bk + n * L::BLK * 8 + c * 16, src + c * 16, bytes);
+          cp16z(bk + n * L::BLK * L::HS + c * 16, src + c * 16, bytes);
       }
     }
     unsigned char *xs = st + L::xs(i);
@@ -111,15 +115,15 @@ __device__ __forceinline__ void issue(unsigned char *st, long g, const Meta &M, 
   }
 }
 
-template <int NSPIN, bool DOT, int WARPS, int STAGES>
+template <int NSPIN, bool DOT, int WARPS, int STAGES, typename HT = double>
 __global__ void __launch_bounds__(WARPS * 32, 1)
     k_spmv_async(long ngroups, const int2 *__restrict__ groups, const int4 *__restrict__ nbr,
-                 const unsigned char *__restrict__ site_m, const double *__restrict__ onsite,
-                 const double *__restrict__ blocks, const double2 *__restrict__ x,
+                 const unsigned char *__restrict__ site_m, const HT *__restrict__ onsite,
+                 const HT *__restrict__ blocks, const double2 *__restrict__ x,
                  double2 *__restrict__ y, double shift, const double *__restrict__ xnorm,
                  int xnorm_idx, double *partial, unsigned int *counter, double *alpha_out,
                  int alpha_idx) {
-  using L = Layout<NSPIN, WARPS, STAGES>;
+  using L = Layout<NSPIN, WARPS, STAGES, HT>;
   constexpr int NB = L::NB;
   extern __shared__ __align__(128) unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -160,15 +164,16 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
       const long a = long(cur.a0) + ai;
       const double2 *xs = reinterpret_cast<const double2 *>(st + L::xs(ai));
       const double2 *X0 = xs + 4 * NB;
-      const double *rec = reinterpret_cast<const double *>(st + L::ons(ai));
-      const double *bk = reinterpret_cast<const double *>(st + L::blk(ai));
+      const HT *rec = reinterpret_cast<const HT *>(st + L::ons(ai));
+      const HT *bk = reinterpret_cast<const HT *>(st + L::blk(ai));
       double2 acc[NSPIN];
 #pragma unroll
       for (int sp = 0; sp < NSPIN; sp++) {
         const double2 v = X0[sp * kNorb + o];
-        acc[sp] = make_double2(rec[sp * kNorb + o] * v.x, rec[sp * kNorb + o] * v.y);
+        const double dg = rec[sp * kNorb + o];
+        acc[sp] = make_double2(dg * v.x, dg * v.y);
       }
-      if (o >= 1 && o <= 4 && rec[NB + 1] != 0.0) {  // dangling-bond sp3 couplings
+      if (o >= 1 && o <= 4 && rec[NB + 1] != HT(0)) {  // dangling-bond sp3 couplings
         const double sx = rec[NB + 2], sy = rec[NB + 3], sz = rec[NB + 4];
         const double cxy = rec[NB + 5], cxz = rec[NB + 6], cyz = rec[NB + 7];
         double c1, c2, c3;
@@ -207,7 +212,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
       for (int n = 0; n < 4; n++)
 #pragma unroll
         for (int sp = 0; sp < NSPIN; sp++) part[n][sp] = make_double2(0.0, 0.0);
-      const double *Mb = bk + (cat ? o * kNorb : o);
+      const HT *Mb = bk + (cat ? o * kNorb : o);
       const int bstride = cat ? 1 : kNorb;
 #pragma unroll
       for (int kk = 0; kk < kNorb; kk++)
@@ -243,14 +248,14 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
   if (DOT) grid_reduce<WARPS * 32>(dot, partial, counter, alpha_out, alpha_idx, false);
 }
 
-template <int NSPIN, bool DOT, int WARPS, int STAGES>
+template <int NSPIN, bool DOT, int WARPS, int STAGES, typename HT>
 int launch_async_t(Ctx &c, const double *x, double *y, double shift, const double *xnorm,
                    int xidx, double *alpha_out, int aidx, cudaStream_t s) {
-  using L = Layout<NSPIN, WARPS, STAGES>;
+  using L = Layout<NSPIN, WARPS, STAGES, HT>;
   static int sms = 0;
   if (!sms) {
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device);
-    if (cudaFuncSetAttribute(k_spmv_async<NSPIN, DOT, WARPS, STAGES>,
+    if (cudaFuncSetAttribute(k_spmv_async<NSPIN, DOT, WARPS, STAGES, HT>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM) != cudaSuccess)
       return set_error(TBGPU_E_CUDA);
   }
@@ -259,8 +264,8 @@ int launch_async_t(Ctx &c, const double *x, double *y, double shift, const doubl
     int rc = ensure_partials(c, int(grid));
     if (rc) return rc;
   }
-  k_spmv_async<NSPIN, DOT, WARPS, STAGES><<<grid, WARPS * 32, L::SMEM, s>>>(
-      c.ngroups, c.d_groups, c.d_nbr, c.d_site_m, c.d_onsite, c.d_blocks,
+  k_spmv_async<NSPIN, DOT, WARPS, STAGES, HT><<<grid, WARPS * 32, L::SMEM, s>>>(
+      c.ngroups, c.d_groups, c.d_nbr, c.d_site_m, ham_onsite<HT>(c), ham_blocks<HT>(c),
       reinterpret_cast<const double2 *>(x), reinterpret_cast<double2 *>(y), shift, xnorm, xidx,
       DOT ? c.d_partial : nullptr, DOT ? c.d_counter : nullptr, alpha_out, aidx);
   TB_CUDA(cudaGetLastError());
@@ -269,16 +274,16 @@ int launch_async_t(Ctx &c, const double *x, double *y, double shift, const doubl
 
 }  // namespace
 
-template <int WARPS, int STAGES>
+template <int WARPS, int STAGES, typename HT>
 int launch_cfg(Ctx &c, const double *x, double *y, double shift, const double *xnorm, int xidx,
                double *alpha_out, int aidx, cudaStream_t s) {
   if (c.nspin == 2)
     return alpha_out
-               ? launch_async_t<2, true, WARPS, STAGES>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s)
-               : launch_async_t<2, false, WARPS, STAGES>(c, x, y, shift, xnorm, xidx, nullptr, 0, s);
+               ? launch_async_t<2, true, WARPS, STAGES, HT>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s)
+               : launch_async_t<2, false, WARPS, STAGES, HT>(c, x, y, shift, xnorm, xidx, nullptr, 0, s);
   return alpha_out
-             ? launch_async_t<1, true, WARPS, STAGES>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s)
-             : launch_async_t<1, false, WARPS, STAGES>(c, x, y, shift, xnorm, xidx, nullptr, 0, s);
+             ? launch_async_t<1, true, WARPS, STAGES, HT>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s)
+             : launch_async_t<1, false, WARPS, STAGES, HT>(c, x, y, shift, xnorm, xidx, nullptr, 0, s);
 }
 
 int launch_spmv_async(Ctx &c, const double *x, double *y, double shift, const double *xnorm,
@@ -287,14 +292,31 @@ int launch_spmv_async(Ctx &c, const double *x, double *y, double shift, const do
   // variant 0: 14 warps x 1 stage per SM (other warps cover a warp's wait;
   // 0.82 ms per launch on the 1.02M-atom dot); variant 2: 7 warps x 2
   // stages (each warp overlaps its own next copies; 0.91 ms)
+  // single-precision store: half the block bytes, 16 warps fit
+  if (c.ham_fp32)
+    return launch_cfg<16, 1, float>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
   if (c.spmv_variant == 2)
-    return launch_cfg<7, 2>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
-  return launch_cfg<14, 1>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
+    return launch_cfg<7, 2, double>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
+  return launch_cfg<14, 1, double>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
 }
 
-// Launch of the default 10-orbital configuration (14 warps x 1 stage) with
-// the alpha dot reduced through caller-provided scratch: partial[cap]
-// doubles and a zeroed counter.  Allocates nothing.
+template <int NSPIN, int WARPS, typename HT>
+static int launch_scratch_async_t(Ctx &c, int sms, const double2 *X, double2 *Y, double shift,
+                                  double *partial, unsigned int *counter, double *dot_out,
+                                  cudaStream_t s) {
+  using L = Layout<NSPIN, WARPS, 1, HT>;
+  TB_CUDA(cudaFuncSetAttribute(k_spmv_async<NSPIN, true, WARPS, 1, HT>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM));
+  k_spmv_async<NSPIN, true, WARPS, 1, HT><<<sms, WARPS * 32, L::SMEM, s>>>(
+      c.ngroups, c.d_groups, c.d_nbr, c.d_site_m, ham_onsite<HT>(c), ham_blocks<HT>(c), X, Y,
+      shift, nullptr, 0, partial, counter, dot_out, 0);
+  TB_CUDA(cudaGetLastError());
+  return TBGPU_OK;
+}
+
+// Launch of the default 10-orbital configuration (one CTA per SM) with the
+// alpha dot reduced through caller-provided scratch: partial[cap] doubles
+// and a zeroed counter.  Allocates nothing.
 int launch_spmv_async_scratch(Ctx &c, const double *x, double *y, double shift,
                               double *partial, unsigned int *counter, int cap, double *dot_out,
                               cudaStream_t s) {
@@ -304,23 +326,13 @@ int launch_spmv_async_scratch(Ctx &c, const double *x, double *y, double shift,
   if (sms > cap) return set_error(TBGPU_E_ARG);
   const double2 *X = reinterpret_cast<const double2 *>(x);
   double2 *Y = reinterpret_cast<double2 *>(y);
-  if (c.nspin == 2) {
-    using L = Layout<2, 14, 1>;
-    TB_CUDA(cudaFuncSetAttribute(k_spmv_async<2, true, 14, 1>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM));
-    k_spmv_async<2, true, 14, 1><<<sms, 14 * 32, L::SMEM, s>>>(
-        c.ngroups, c.d_groups, c.d_nbr, c.d_site_m, c.d_onsite, c.d_blocks, X, Y, shift, nullptr, 0,
-        partial, counter, dot_out, 0);
-  } else {
-    using L = Layout<1, 14, 1>;
-    TB_CUDA(cudaFuncSetAttribute(k_spmv_async<1, true, 14, 1>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM));
-    k_spmv_async<1, true, 14, 1><<<sms, 14 * 32, L::SMEM, s>>>(
-        c.ngroups, c.d_groups, c.d_nbr, c.d_site_m, c.d_onsite, c.d_blocks, X, Y, shift, nullptr, 0,
-        partial, counter, dot_out, 0);
-  }
-  TB_CUDA(cudaGetLastError());
-  return TBGPU_OK;
+  if (c.ham_fp32)
+    return c.nspin == 2
+               ? launch_scratch_async_t<2, 16, float>(c, sms, X, Y, shift, partial, counter, dot_out, s)
+               : launch_scratch_async_t<1, 16, float>(c, sms, X, Y, shift, partial, counter, dot_out, s);
+  return c.nspin == 2
+             ? launch_scratch_async_t<2, 14, double>(c, sms, X, Y, shift, partial, counter, dot_out, s)
+             : launch_scratch_async_t<1, 14, double>(c, sms, X, Y, shift, partial, counter, dot_out, s);
 }
 
 }  // namespace tbgpu

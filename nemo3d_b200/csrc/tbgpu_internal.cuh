@@ -66,6 +66,11 @@ struct Ctx {
   unsigned char *d_surface = nullptr;
   double *d_onsite = nullptr;       // [natoms*ons]
   double *d_blocks = nullptr;       // [natoms*4*norb*norb], cation atoms
+  // single-precision store (the reference's HamMemorySave build): the same
+  // arrays in float, and d_onsite / d_blocks released after assembly
+  bool ham_fp32 = false;
+  float *d_onsite32 = nullptr;
+  float *d_blocks32 = nullptr;
   // H*x work order: groups of up to 3 consecutive atoms of one k-pencil of
   // cells, pencils visited in j-blocks (first atom, atom count)
   int2 *d_groups = nullptr;
@@ -88,6 +93,14 @@ struct Ctx {
   // scratch for the host-pointer matvec
   double *d_x = nullptr, *d_y = nullptr;
 };
+
+// the stored Hamiltonian in its element type
+template <typename HT> inline const HT *ham_blocks(const Ctx &c);
+template <> inline const double *ham_blocks<double>(const Ctx &c) { return c.d_blocks; }
+template <> inline const float *ham_blocks<float>(const Ctx &c) { return c.d_blocks32; }
+template <typename HT> inline const HT *ham_onsite(const Ctx &c);
+template <> inline const double *ham_onsite<double>(const Ctx &c) { return c.d_onsite; }
+template <> inline const float *ham_onsite<float>(const Ctx &c) { return c.d_onsite32; }
 
 // error helpers
 int set_error(int code);

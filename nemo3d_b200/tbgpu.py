@@ -69,6 +69,7 @@ def _lib():
         L.tbgpu_error_string.argtypes = [ip]
         L.tbgpu_prepare_params.argtypes = [ip, ip, vp, vp, dp, dp, vp]
         L.tbgpu_set_bloch_k.argtypes = [vp, C.POINTER(C.c_double)]
+        L.tbgpu_set_ham_precision.argtypes = [vp, ip]
         L.tbgpu_hx_block_dev.argtypes = [vp, ip, dp, vp, vp]
         L.tbgpu_eigensolve_blk_lanczos.argtypes = [vp, ip, ip, ip, ip, ip, dp, dp, dp, dp, dp,
                                                    ip, ip, vp, vp, vp, vp, vp]
@@ -135,7 +136,8 @@ class Hamiltonian:
     """
 
     def __init__(self, structure, model="sp3d5s*_so", materials=None, include_strain=True,
-                 passivate=True, dangling_shift=30.0, device_inputs=None, build=True):
+                 passivate=True, dangling_shift=30.0, device_inputs=None, build=True,
+                 ham_bits=64):
         L = _lib()
         self.structure = structure
         self.model = model
@@ -169,6 +171,11 @@ class Hamiltonian:
             raise TbgpuError(rc, "tbgpu_ctx_create")
         self._ctx = ctx
         self._built = False
+        if ham_bits != 64:
+            rc = L.tbgpu_set_ham_precision(ctx, int(ham_bits))
+            if rc:
+                L.tbgpu_ctx_destroy(ctx)
+                raise TbgpuError(rc, "tbgpu_set_ham_precision")
         if build:
             self.build()
 
