@@ -198,14 +198,19 @@ int tbgpu_band_eigenvalues(int n, int kd, const double *ab, double vl, double vu
  * eigenvalues ascending; found_vb / found_cb the counts per window;
  * *iterations the block steps.  Returns the number of eigenvalues or a
  * negative error (TBGPU_E_NUMERIC when a block loses rank: deflation is not
- * supported).  Eigenvectors are not computed. */
+ * supported).  If vectors != NULL the eigenvectors of the first max_vectors
+ * eigenvalues (ascending) are rebuilt by a second pass
+ * (eigenvectorsBlockLanczos, lanczos_blk.c:1857-2145) from eigenvectors of
+ * the band matrix found by inverse iteration, into vectors[k][dimension];
+ * vectors of equal eigenvalues are made orthogonal. */
 int tbgpu_eigensolve_blk_lanczos(tbgpu_ctx *ctx, int ConvCheckStartIter,
                                  int ConvCheckSkipRate, int imax, int requested1,
                                  int requested2, double emin1, double emax1,
                                  double emin2, double emax2, double tolerance,
                                  int p, int max_no_success,
                                  const tbgpu_dcomplex *r0, double *values,
-                                 int *found_vb, int *found_cb, int *iterations);
+                                 int *found_vb, int *found_cb, int *iterations,
+                                 tbgpu_dcomplex *vectors, int max_vectors);
 int tbgpu_eigensolve_blk_lanczos_dev(tbgpu_ctx *ctx, int ConvCheckStartIter,
                                      int ConvCheckSkipRate, int imax,
                                      int requested1, int requested2,
@@ -213,7 +218,8 @@ int tbgpu_eigensolve_blk_lanczos_dev(tbgpu_ctx *ctx, int ConvCheckStartIter,
                                      double emax2, double tolerance, int p,
                                      int max_no_success, const double *r0_dev,
                                      double *values, int *found_vb,
-                                     int *found_cb, int *iterations);
+                                     int *found_cb, int *iterations,
+                                     double *vectors_dev, int max_vectors);
 
 /* Tridiagonal matrix of the last solve: alpha[n], beta[n] (n <= cap). */
 int tbgpu_get_tridiagonal(const tbgpu_ctx *ctx, double *alpha, double *beta,

@@ -206,6 +206,149 @@ void method4(const std::vector<double> &fresh, std::vector<double> &old, std::ve
   old = fresh;
 }
 
+// Eigenvector y of the Hermitian band matrix T (lower storage, kd) for the
+// eigenvalue lam by inverse iteration with a banded LU of T - lam I (partial
+// pivoting; U has 2 kd superdiagonals), orthogonalised in every step against
+// the vectors in `ortho` (the earlier members of a cluster of equal values)
+// so that degenerate eigenvalues get independent vectors.
+bool band_eigvec(int n, int kd, const std::vector<cplx> &ab, double lam,
+                 const std::vector<std::vector<cplx>> &ortho, unsigned long long seed,
+                 std::vector<cplx> &y) {
+  const int ld = kd + 1, w = 3 * kd + 1, off = 2 * kd;  // row i: columns i-kd .. i+2kd
+  std::vector<cplx> M(size_t(n) * w, cplx(0.0, 0.0));
+  auto at = [&](int i, int j) -> cplx & { return M[size_t(i) * w + (j - i + kd)]; };
+  double norm = 0.0;
+  for (int j = 0; j < n; j++)
+    for (int i = j; i <= std::min(n - 1, j + kd); i++) {
+      const cplx v = ab[size_t(j) * ld + (i - j)];
+      at(i, j) = v;
+      if (i != j) at(j, i) = std::conj(v);
+      norm = std::max(norm, std::abs(v));
+    }
+  for (int i = 0; i < n; i++) at(i, i) -= lam;
+  const double tiny = std::max(norm, 1.0) * 1e-14;
+  std::vector<int> piv(n);
+  for (int j = 0; j < n; j++) {  // LU with row pivoting inside the band
+    int pr = j;
+    double best = std::abs(at(j, j));
+    for (int i = j + 1; i <= std::min(n - 1, j + kd); i++)
+      if (std::abs(at(i, j)) > best) { best = std::abs(at(i, j)); pr = i; }
+    piv[j] = pr;
+    const int hi = std::min(n - 1, j + off);
+    if (pr != j)
+      for (int c = j; c <= hi; c++) std::swap(at(j, c), at(pr, c));
+    if (std::abs(at(j, j)) < tiny) at(j, j) = tiny;  // exact eigenvalue: perturb the pivot
+    for (int i = j + 1; i <= std::min(n - 1, j + kd); i++) {
+      const cplx l = at(i, j) / at(j, j);
+      at(i, j) = l;
+      if (l == cplx(0.0, 0.0)) continue;
+      for (int c = j + 1; c <= hi; c++) at(i, c) -= l * at(j, c);
+    }
+  }
+  unsigned long long st = seed * 6364136223846793005ULL + 1442695040888963407ULL;
+  auto urand = [&]() {
+    st = st * 6364136223846793005ULL + 1442695040888963407ULL;
+    return double(st >> 11) / double(1ULL << 53) - 0.5;
+  };
+  y.assign(n, cplx(0.0, 0.0));
+  for (int i = 0; i < n; i++) y[i] = cplx(urand(), urand());
+  auto orth_norm = [&]() -> bool {
+    for (const auto &u : ortho) {
+      cplx d(0.0, 0.0);
+      for (int i = 0; i < n; i++) d += std::conj(u[i]) * y[i];
+      for (int i = 0; i < n; i++) y[i] -= d * u[i];
+    }
+    double nn = 0.0;
+    for (int i = 0; i < n; i++) nn += std::norm(y[i]);
+    if (!(nn > 0.0)) return false;
+    nn = 1.0 / std::sqrt(nn);
+    for (int i = 0; i < n; i++) y[i] *= nn;
+    return true;
+  };
+  if (!orth_norm()) return false;
+  for (int itr = 0; itr < 4; itr++) {
+    for (int j = 0; j < n; j++) {  // forward: apply the row swaps and L
+      if (piv[j] != j) std::swap(y[j], y[piv[j]]);
+      for (int i = j + 1; i <= std::min(n - 1, j + kd); i++) y[i] -= at(i, j) * y[j];
+    }
+    for (int i = n - 1; i >= 0; i--) {  // back: U
+      cplx v = y[i];
+      for (int c = i + 1; c <= std::min(n - 1, i + off); c++) v -= at(i, c) * y[c];
+      y[i] = v / at(i, i);
+    }
+    if (!orth_norm()) return false;
+  }
+  return true;
+}
+
+// Eigenpairs of a small Hermitian m x m matrix G (row-major), largest first:
+// cyclic Jacobi on the real symmetric embedding [[Re, -Im], [Im, Re]], whose
+// eigenvalues are those of G twice over; one complex vector is kept per pair.
+void herm_eig_desc(int m, const Mat &G, std::vector<double> &w, std::vector<std::vector<cplx>> &U) {
+  const int n = 2 * m;
+  std::vector<double> A(size_t(n) * n), V(size_t(n) * n, 0.0);
+  for (int i = 0; i < m; i++)
+    for (int j = 0; j < m; j++) {
+      const cplx g = G[i * m + j];
+      A[i * n + j] = g.real();
+      A[(i + m) * n + (j + m)] = g.real();
+      A[i * n + (j + m)] = -g.imag();
+      A[(i + m) * n + j] = g.imag();
+    }
+  for (int i = 0; i < n; i++) V[i * n + i] = 1.0;
+  for (int sweep = 0; sweep < 60; sweep++) {
+    double off = 0.0;
+    for (int i = 0; i < n; i++)
+      for (int j = i + 1; j < n; j++) off += A[i * n + j] * A[i * n + j];
+    if (off < 1e-30) break;
+    for (int p = 0; p < n; p++)
+      for (int q = p + 1; q < n; q++) {
+        const double apq = A[p * n + q];
+        if (std::fabs(apq) < 1e-300) continue;
+        const double th = 0.5 * (A[q * n + q] - A[p * n + p]) / apq;
+        const double t = (th >= 0 ? 1.0 : -1.0) / (std::fabs(th) + std::sqrt(th * th + 1.0));
+        const double c = 1.0 / std::sqrt(t * t + 1.0), sn = t * c;
+        for (int k = 0; k < n; k++) {  // A <- J^T A J, V <- V J
+          const double akp = A[k * n + p], akq = A[k * n + q];
+          A[k * n + p] = c * akp - sn * akq;
+          A[k * n + q] = sn * akp + c * akq;
+        }
+        for (int k = 0; k < n; k++) {
+          const double apk = A[p * n + k], aqk = A[q * n + k];
+          A[p * n + k] = c * apk - sn * aqk;
+          A[q * n + k] = sn * apk + c * aqk;
+        }
+        for (int k = 0; k < n; k++) {
+          const double vkp = V[k * n + p], vkq = V[k * n + q];
+          V[k * n + p] = c * vkp - sn * vkq;
+          V[k * n + q] = sn * vkp + c * vkq;
+        }
+      }
+  }
+  std::vector<int> ord(n);
+  for (int i = 0; i < n; i++) ord[i] = i;
+  std::sort(ord.begin(), ord.end(), [&](int a, int b) { return A[a * n + a] > A[b * n + b]; });
+  w.clear();
+  U.clear();
+  for (int idx : ord) {
+    std::vector<cplx> z(m);
+    for (int i = 0; i < m; i++) z[i] = cplx(V[i * n + idx], V[(i + m) * n + idx]);
+    for (const auto &u : U) {
+      cplx d(0.0, 0.0);
+      for (int i = 0; i < m; i++) d += std::conj(u[i]) * z[i];
+      for (int i = 0; i < m; i++) z[i] -= d * u[i];
+    }
+    double nn = 0.0;
+    for (int i = 0; i < m; i++) nn += std::norm(z[i]);
+    if (nn < 0.25) continue;  // the partner of a vector already kept
+    nn = 1.0 / std::sqrt(nn);
+    for (int i = 0; i < m; i++) z[i] *= nn;
+    U.push_back(z);
+    w.push_back(A[idx * n + idx]);
+    if (int(U.size()) == m) break;
+  }
+}
+
 }  // namespace
 
 struct BlkArgs {
@@ -215,7 +358,8 @@ struct BlkArgs {
 
 template <int P>
 static int blk_run(Ctx &c, const BlkArgs &A, const double *r0_dev, std::vector<double> &values,
-                   int &found1_out, int &found2_out, int &iters_out) {
+                   int &found1_out, int &found2_out, int &iters_out, double *V_dev,
+                   int maxvec) {
   const long n2 = c.natoms * c.nb;
   const size_t vbytes = sizeof(double2) * n2;
   cudaStream_t s = c.stream;
@@ -298,34 +442,41 @@ static int blk_run(Ctx &c, const BlkArgs &A, const double *r0_dev, std::vector<d
   std::vector<double> old1, old2, conv1, conv2;
   int nos1 = 0, nos2 = 0, skip = 0, it = 0;
   const int added = 1;
-  // start block: R = r0, Q = qr(R)
-  if (cudaMemcpyAsync(R, r0_dev, vbytes * P, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
-    rc = TBGPU_E_CUDA;
-  Mat B;
-  if (!rc) qr(B);
-  bool converged = false;
-  while (!rc) {
-    if (it != 0 && qr(B)) break;
+  // one block step (single_iteration); the current block ends up in Qo
+  auto step = [&](Mat &B, Mat &Al) -> int {
+    if (it != 0 && qr(B)) return rc;
     // R_i = H Q_i, the block at once
     if (launch_spmm(c, P, reinterpret_cast<const double *>(Q), 2 * n2,
                     reinterpret_cast<double *>(R), 2 * n2, 0.0, s))
-      rc = TBGPU_E_CUDA;
-    if (rc) break;
+      return fail(TBGPU_E_CUDA);
     if (it != 0) {  // R -= Qold B^H
       Mat M(size_t(P) * P);
       for (int k = 0; k < P; k++)
         for (int i = 0; i < P; i++) M[k * P + i] = -std::conj(B[i * P + k]);
-      if (combine(Qo, M, R, 1.0, R)) break;
+      if (combine(Qo, M, R, 1.0, R)) return rc;
     }
-    Mat Al;
-    if (dots(Q, R, Al)) break;  // Al[i][j] = Q_i^H R_j
-    {                           // R -= Q A, A[k][i] = Q_k^H R_i
+    if (dots(Q, R, Al)) return rc;  // Al[i][j] = Q_i^H R_j
+    {                               // R -= Q A, A[k][i] = Q_k^H R_i
       Mat M(size_t(P) * P);
       for (int k = 0; k < P; k++)
         for (int i = 0; i < P; i++) M[k * P + i] = -Al[k * P + i];
-      if (combine(Q, M, R, 1.0, R)) break;
+      if (combine(Q, M, R, 1.0, R)) return rc;
     }
     std::swap(Q, Qo);
+    return TBGPU_OK;
+  };
+  // start block: R = r0, Q = qr(R)
+  auto restart = [&]() -> int {
+    if (cudaMemcpyAsync(R, r0_dev, vbytes * P, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+      return fail(TBGPU_E_CUDA);
+    Mat B0;
+    return qr(B0);
+  };
+  Mat B, Al;
+  if (!rc) restart();
+  bool converged = false;
+  while (!rc) {
+    if (step(B, Al)) break;
     // band entries of this block: B couples it to the previous block
     band.resize(size_t(tsize + P) * ld, cplx(0.0, 0.0));
     if (it != 0)
@@ -369,13 +520,145 @@ static int blk_run(Ctx &c, const BlkArgs &A, const double *r0_dev, std::vector<d
     }
     if (it + 1 >= A.imax) break;
   }
+  values.assign(conv1.begin(), conv1.end());
+  values.insert(values.end(), conv2.begin(), conv2.end());
+  std::sort(values.begin(), values.end());
+  const int it0_steps = it;
+  // ---- eigenvectors: Ritz vectors of the band matrix, second pass ---------
+  // (eigenvectorsBlockLanczos, lanczos_blk.c:1857-2145: the recurrence is
+  // repeated from the start block, which the deterministic kernels reproduce
+  // bit for bit, and every block is accumulated with its rows of the band
+  // matrix's eigenvectors)
+  const int nvec = V_dev ? std::min(int(values.size()), std::max(maxvec, 0)) : 0;
+  double2 *Cand = nullptr;
+  if (!rc && nvec > 0) {
+    // Clusters of equal values (within 100x the tolerance, e.g. Kramers
+    // pairs).  Without reorthogonalisation the band matrix also carries
+    // copies ("ghosts") of converged values whose Ritz vectors repeat true
+    // ones, so every band eigenvector of a cluster's window is rebuilt and
+    // the cluster's vectors are the orthonormal directions of largest
+    // weight among those candidates (the reference instead Gram-Schmidts
+    // the rebuilt vectors of close values, lanczos_blk.c:2117-2128).
+    struct Cluster {
+      int e0, r;                 // first value index, members
+      std::vector<std::vector<cplx>> y;  // band eigenvectors (candidates)
+      int c0;                    // first candidate index
+    };
+    std::vector<Cluster> cl;
+    for (int e = 0; e < nvec;) {
+      int f = e + 1;
+      while (f < nvec && values[f] - values[f - 1] < 100.0 * A.tol) f++;
+      cl.push_back({e, f - e, {}, 0});
+      e = f;
+    }
+    int ncand = 0;
+    for (auto &C : cl) {
+      const double lo = values[C.e0] - 100.0 * A.tol, hi = values[C.e0 + C.r - 1] + 100.0 * A.tol;
+      std::vector<double> wv;
+      band_eigenvalues(tsize, P, band.data(), lo, hi, A.tol, wv);
+      if (int(wv.size()) < C.r) wv.assign(values.begin() + C.e0, values.begin() + C.e0 + C.r);
+      if (wv.size() > 8) wv.resize(8);
+      for (size_t k = 0; k < wv.size() && !rc; k++) {
+        std::vector<cplx> y;
+        if (!band_eigvec(tsize, P, band, wv[k], C.y, 977ULL + 31ULL * ncand + k, y))
+          rc = TBGPU_E_NUMERIC;
+        else
+          C.y.push_back(y);
+      }
+      C.c0 = ncand;
+      ncand += int(C.y.size());
+    }
+    if (!rc && cudaMalloc(&Cand, vbytes * ncand) != cudaSuccess) rc = TBGPU_E_NOMEM;
+    if (!rc && cudaMemsetAsync(Cand, 0, vbytes * ncand, s) != cudaSuccess) rc = TBGPU_E_CUDA;
+    std::vector<const std::vector<cplx> *> Y;
+    for (auto &C : cl)
+      for (auto &y : C.y) Y.push_back(&y);
+    if (!rc) {
+      it = 0;
+      restart();
+    }
+    const int nsteps = it0_steps;
+    for (int k = 0; k < nsteps && !rc; k++) {
+      if (step(B, Al)) break;
+      ++it;
+      // Cand_j += sum_i Qo_i * Y_j[k*P + i], in groups of up to P candidates
+      for (int e0 = 0; e0 < ncand && !rc; e0 += P) {
+        const int ne = std::min(P, ncand - e0);
+        SmallMat sm{};
+        for (int i = 0; i < P; i++)
+          for (int e = 0; e < ne; e++) {
+            const cplx v = (*Y[e0 + e])[size_t(k) * P + i];
+            sm.m[i][e] = make_double2(v.real(), v.imag());
+          }
+        BlockOut vo{};
+        BlockPtrs vi{};
+        for (int e = 0; e < ne; e++) {
+          vo.v[e] = Cand + size_t(e0 + e) * n2;
+          vi.v[e] = Cand + size_t(e0 + e) * n2;
+        }
+        k_bcombine<P><<<grid, 256, 0, s>>>(n2, P, ptrs(Qo), sm, ne, vo, 1.0, vi);
+        if (cudaGetLastError() != cudaSuccess) rc = TBGPU_E_CUDA;
+      }
+    }
+    // each cluster: Gram matrix of its candidates, keep the r directions of
+    // largest weight, orthonormal, as the cluster's eigenvectors
+    for (auto &C : cl) {
+      if (rc) break;
+      const int m = int(C.y.size());
+      BlockPtrs cp{};
+      for (int j = 0; j < 8; j++) cp.v[j] = Cand + size_t(C.c0 + std::min(j, m - 1)) * n2;
+      constexpr int K8 = 8 * 9 / 2;
+      double *part8 = nullptr, *res8 = nullptr;
+      if (cudaMalloc(&part8, sizeof(double) * 2 * K8 * grid) != cudaSuccess ||
+          cudaMalloc(&res8, sizeof(double) * 2 * K8) != cudaSuccess) {
+        cudaFree(part8);
+        rc = TBGPU_E_NOMEM;
+        break;
+      }
+      k_bdots<8><<<grid, kDotThreads, 0, s>>>(n2, cp, cp, part8, counter, res8);
+      double h[2 * K8];
+      if (cudaGetLastError() != cudaSuccess ||
+          cudaMemcpyAsync(h, res8, sizeof(h), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+          cudaStreamSynchronize(s) != cudaSuccess)
+        rc = TBGPU_E_CUDA;
+      cudaFree(part8);
+      cudaFree(res8);
+      if (rc) break;
+      Mat G(size_t(m) * m);
+      int t = 0;
+      for (int i = 0; i < 8; i++)
+        for (int j = 0; j <= i; j++, t++)
+          if (i < m && j < m) {
+            G[i * m + j] = cplx(h[2 * t], h[2 * t + 1]);
+            G[j * m + i] = std::conj(G[i * m + j]);
+          }
+      std::vector<double> gw;
+      std::vector<std::vector<cplx>> gu;
+      herm_eig_desc(m, G, gw, gu);
+      const int keep = std::min(C.r, int(gu.size()));
+      if (keep < C.r || gw[keep - 1] <= 0.0) {
+        rc = TBGPU_E_NUMERIC;
+        break;
+      }
+      SmallMat sm{};
+      for (int j = 0; j < m; j++)
+        for (int e = 0; e < keep; e++) {
+          const cplx v = gu[e][j] / std::sqrt(gw[e]);
+          sm.m[j][e] = make_double2(v.real(), v.imag());
+        }
+      BlockOut vo{};
+      for (int e = 0; e < keep; e++)
+        vo.v[e] = reinterpret_cast<double2 *>(V_dev) + size_t(C.e0 + e) * n2;
+      k_bcombine<8><<<grid, 256, 0, s>>>(n2, m, cp, sm, keep, vo, 0.0, cp);
+      if (cudaGetLastError() != cudaSuccess) rc = TBGPU_E_CUDA;
+    }
+    it = nsteps;
+  }
+  cudaFree(Cand);
   (void)converged;
   cudaStreamSynchronize(s);
   cudaFree(Q); cudaFree(Qo); cudaFree(R); cudaFree(partial); cudaFree(dres); cudaFree(counter);
   if (rc) return set_error(rc);
-  values.assign(conv1.begin(), conv1.end());
-  values.insert(values.end(), conv2.begin(), conv2.end());
-  std::sort(values.begin(), values.end());
   found1_out = int(conv1.size());
   found2_out = int(conv2.size());
   iters_out = it;
@@ -383,16 +666,16 @@ static int blk_run(Ctx &c, const BlkArgs &A, const double *r0_dev, std::vector<d
 }
 
 int solve_block(Ctx &c, const BlkArgs &A, const double *r0_dev, std::vector<double> &values,
-                int &f1, int &f2, int &iters) {
+                int &f1, int &f2, int &iters, double *V_dev, int maxvec) {
   switch (A.p) {
-    case 1: return blk_run<1>(c, A, r0_dev, values, f1, f2, iters);
-    case 2: return blk_run<2>(c, A, r0_dev, values, f1, f2, iters);
-    case 3: return blk_run<3>(c, A, r0_dev, values, f1, f2, iters);
-    case 4: return blk_run<4>(c, A, r0_dev, values, f1, f2, iters);
-    case 5: return blk_run<5>(c, A, r0_dev, values, f1, f2, iters);
-    case 6: return blk_run<6>(c, A, r0_dev, values, f1, f2, iters);
-    case 7: return blk_run<7>(c, A, r0_dev, values, f1, f2, iters);
-    case 8: return blk_run<8>(c, A, r0_dev, values, f1, f2, iters);
+    case 1: return blk_run<1>(c, A, r0_dev, values, f1, f2, iters, V_dev, maxvec);
+    case 2: return blk_run<2>(c, A, r0_dev, values, f1, f2, iters, V_dev, maxvec);
+    case 3: return blk_run<3>(c, A, r0_dev, values, f1, f2, iters, V_dev, maxvec);
+    case 4: return blk_run<4>(c, A, r0_dev, values, f1, f2, iters, V_dev, maxvec);
+    case 5: return blk_run<5>(c, A, r0_dev, values, f1, f2, iters, V_dev, maxvec);
+    case 6: return blk_run<6>(c, A, r0_dev, values, f1, f2, iters, V_dev, maxvec);
+    case 7: return blk_run<7>(c, A, r0_dev, values, f1, f2, iters, V_dev, maxvec);
+    case 8: return blk_run<8>(c, A, r0_dev, values, f1, f2, iters, V_dev, maxvec);
     default: return set_error(TBGPU_E_ARG);
   }
 }
@@ -405,9 +688,9 @@ extern "C" int tbgpu_eigensolve_blk_lanczos_dev(
     tbgpu_ctx *ctx, int ConvCheckStartIter, int ConvCheckSkipRate, int imax, int requested1,
     int requested2, double emin1, double emax1, double emin2, double emax2, double tolerance,
     int p, int max_no_success, const double *r0_dev, double *values, int *found_vb,
-    int *found_cb, int *iterations) {
+    int *found_cb, int *iterations, double *vectors_dev, int max_vectors) {
   if (!ctx || !r0_dev || !values || p < 1 || p > kMaxP || imax < 2 || ConvCheckSkipRate < 1 ||
-      requested1 < 0 || requested2 < 0 || tolerance <= 0.0)
+      requested1 < 0 || requested2 < 0 || tolerance <= 0.0 || max_vectors < 0)
     return set_error(TBGPU_E_ARG);
   Ctx &c = *reinterpret_cast<Ctx *>(ctx);
   if (!c.built) return set_error(TBGPU_E_STATE);
@@ -417,7 +700,7 @@ extern "C" int tbgpu_eigensolve_blk_lanczos_dev(
             emin1, emax1, emin2, emax2, tolerance};
   std::vector<double> vals;
   int f1 = 0, f2 = 0, it = 0;
-  int rc = solve_block(c, A, r0_dev, vals, f1, f2, it);
+  int rc = solve_block(c, A, r0_dev, vals, f1, f2, it, vectors_dev, max_vectors);
   if (rc) return rc;
   for (size_t k = 0; k < vals.size(); k++) values[k] = vals[k];
   if (found_vb) *found_vb = f1;
@@ -430,22 +713,33 @@ extern "C" int tbgpu_eigensolve_blk_lanczos(
     tbgpu_ctx *ctx, int ConvCheckStartIter, int ConvCheckSkipRate, int imax, int requested1,
     int requested2, double emin1, double emax1, double emin2, double emax2, double tolerance,
     int p, int max_no_success, const tbgpu_dcomplex *r0, double *values, int *found_vb,
-    int *found_cb, int *iterations) {
-  if (!ctx || !r0 || p < 1 || p > kMaxP) return set_error(TBGPU_E_ARG);
+    int *found_cb, int *iterations, tbgpu_dcomplex *vectors, int max_vectors) {
+  if (!ctx || !r0 || p < 1 || p > kMaxP || max_vectors < 0) return set_error(TBGPU_E_ARG);
   Ctx &c = *reinterpret_cast<Ctx *>(ctx);
   if (!c.built) return set_error(TBGPU_E_STATE);
-  const size_t bytes = sizeof(double2) * size_t(c.natoms) * c.nb * p;
-  double *d = nullptr;
-  if (cudaMalloc(&d, bytes) != cudaSuccess) return set_error(TBGPU_E_NOMEM);
+  const size_t vb = sizeof(double2) * size_t(c.natoms) * c.nb;
+  const int nv = vectors ? std::min(max_vectors, requested1 + requested2) : 0;
+  double *d = nullptr, *dv = nullptr;
+  if (cudaMalloc(&d, vb * p) != cudaSuccess) return set_error(TBGPU_E_NOMEM);
+  if (nv > 0 && cudaMalloc(&dv, vb * nv) != cudaSuccess) {
+    cudaFree(d);
+    return set_error(TBGPU_E_NOMEM);
+  }
   int rc = TBGPU_OK;
-  if (cudaMemcpyAsync(d, r0, bytes, cudaMemcpyHostToDevice, c.stream) != cudaSuccess)
+  if (cudaMemcpyAsync(d, r0, vb * p, cudaMemcpyHostToDevice, c.stream) != cudaSuccess)
     rc = set_error(TBGPU_E_CUDA);
   if (!rc)
     rc = tbgpu_eigensolve_blk_lanczos_dev(ctx, ConvCheckStartIter, ConvCheckSkipRate, imax,
                                           requested1, requested2, emin1, emax1, emin2, emax2,
                                           tolerance, p, max_no_success, d, values, found_vb,
-                                          found_cb, iterations);
+                                          found_cb, iterations, dv, nv);
+  if (rc > 0 && nv > 0) {
+    const int got = std::min(rc, nv);
+    if (cudaMemcpyAsync(vectors, dv, vb * got, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess)
+      rc = set_error(TBGPU_E_CUDA);
+  }
   cudaStreamSynchronize(c.stream);
   cudaFree(d);
+  cudaFree(dv);
   return rc;
 }

@@ -72,7 +72,7 @@ def _lib():
         L.tbgpu_set_ham_precision.argtypes = [vp, ip]
         L.tbgpu_hx_block_dev.argtypes = [vp, ip, dp, vp, vp]
         L.tbgpu_eigensolve_blk_lanczos.argtypes = [vp, ip, ip, ip, ip, ip, dp, dp, dp, dp, dp,
-                                                   ip, ip, vp, vp, vp, vp, vp]
+                                                   ip, ip, vp, vp, vp, vp, vp, vp, ip]
         L.tbgpu_ctx_create.argtypes = [C.POINTER(_Geom), C.POINTER(_Model), C.POINTER(vp)]
         L.tbgpu_ctx_create_dev.argtypes = [C.POINTER(_Geom), C.POINTER(_Model), C.POINTER(vp)]
         L.tbgpu_ctx_destroy.argtypes = [vp]
@@ -306,24 +306,33 @@ class Hamiltonian:
 
     def eigensolve_blk_lanczos(self, r0_block, ConvCheckStartIter=200, ConvCheckSkipRate=50,
                                imax=2000, requested1=1, requested2=1, emin1=-0.6, emax1=0.2,
-                               emin2=1.4, emax2=2.0, tolerance=1e-7, max_no_success=0):
+                               emin2=1.4, emax2=2.0, tolerance=1e-7, max_no_success=0,
+                               vectors=0):
         """Block Lanczos (eigensolve_blk_lanczos).  r0_block: host start block,
         shape (p, 2*dimension) doubles.  Returns values (ascending),
-        found_vb, found_cb, iterations."""
+        found_vb, found_cb, iterations and, when ``vectors`` > 0, the
+        eigenvectors (complex, [k, dimension])."""
         r0 = np.ascontiguousarray(r0_block, np.float64)
         p = r0.shape[0]
         if r0.ndim != 2 or r0.shape[1] != 2 * self.n:
             raise ValueError("r0_block must have shape (p, 2*dimension)")
         vals = np.zeros(max(1, requested1 + requested2))
+        nv = min(vectors, requested1 + requested2)
+        vec = np.zeros(2 * self.n * max(nv, 1)) if nv > 0 else None
         f1, f2, it = C.c_int(), C.c_int(), C.c_int()
         rc = _lib().tbgpu_eigensolve_blk_lanczos(
             self._ctx, ConvCheckStartIter, ConvCheckSkipRate, imax, requested1, requested2,
             emin1, emax1, emin2, emax2, tolerance, p, max_no_success, _p(r0), _p(vals),
-            C.byref(f1), C.byref(f2), C.byref(it))
+            C.byref(f1), C.byref(f2), C.byref(it), _p(vec), nv)
         if rc < 0:
             raise TbgpuError(rc, "tbgpu_eigensolve_blk_lanczos")
-        return {"values": vals[:rc].copy(), "found_vb": f1.value, "found_cb": f2.value,
-                "iterations": it.value}
+        out = {"values": vals[:rc].copy(), "found_vb": f1.value, "found_cb": f2.value,
+               "iterations": it.value}
+        if nv > 0:
+            k = min(rc, nv)
+            v = vec[:2 * self.n * k].reshape(k, self.n, 2)
+            out["vectors"] = v[..., 0] + 1j * v[..., 1]
+        return out
 
     def set_bloch_k(self, k):
         """Bloch vector (reference units) for periodic structures; None or

@@ -97,3 +97,28 @@ def test_block_hx_matches_oracle(model, p):
     scale = max(np.abs(o.onsite).max(), np.abs(o.blocks).max())
     for v in range(p):
         assert np.abs(Y[v] - o.hx(X[v], shift=0.3)).max() <= 45e-12 * scale, v
+
+
+@pytest.mark.parametrize("model,cube,p", [("sp3d5s*_so", 2, 4), ("sp3s*", 3, 3)])
+def test_block_lanczos_eigenvectors(model, cube, p):
+    """Second pass: ||H v - lambda v|| < 1e-4 |lambda| scale, orthonormal set
+    (degenerate Kramers pairs included)."""
+    fam = "spds" if model.startswith("sp3d5s") else "sps"
+    mats = [materials.MATERIALS[f"GaAs_{fam}"]]
+    g, o = _case(model, workloads.gaas_cube(cube), mats)
+    ev = np.linalg.eigvalsh(o.dense())
+    w1 = (ev[0] - 0.5, ev[0] + 1.0)
+    w2 = (ev[-1] - 1.0, ev[-1] + 0.5)
+    r0 = np.random.default_rng(11).uniform(-1, 1, size=(p, 2 * g.n))
+    res = g.eigensolve_blk_lanczos(r0, imax=min(300, g.n // p - 2), requested1=3,
+                                   requested2=3, emin1=w1[0], emax1=w1[1], emin2=w2[0],
+                                   emax2=w2[1], tolerance=1e-7, ConvCheckStartIter=30,
+                                   ConvCheckSkipRate=10, vectors=6)
+    V = res["vectors"]
+    assert V.shape[0] == len(res["values"]) > 0
+    hx = _hx(o)
+    for lam, v in zip(res["values"], V):
+        r = hx(v) - lam * v
+        assert np.linalg.norm(r) < 1e-4 * max(1.0, abs(lam)), lam
+    G = V.conj() @ V.T
+    assert np.abs(G - np.eye(len(V))).max() < 1e-6
