@@ -262,6 +262,20 @@ int tbgpu_hx_dot_noalloc(tbgpu_ctx *ctx, double shift, const double *x_dev,
  * 7 warps x 2 stages. */
 int tbgpu_set_spmv_variant(tbgpu_ctx *ctx, int variant);
 
+/* Result files in the reference's <HDR> format (nemo3d/src/io/fileformat.c:
+ * 182-204), readable by its post-processing tools.
+ * tbgpu_write_eigenvalues: the nd_Ek file (writeEigenvalues,
+ * nemo3d/src/io/i_3dout_files.c:1886-1975): mode 'i' empties the file, 'a'
+ * appends n records {kx, ky, kz, E} and rewrites the header's count.
+ * tbgpu_write_eigenvector: one nd_evec file (writeEigenvector,
+ * i_3dout_files.c:1342-1357) with records {wf.r, wf.i} for every basis state
+ * of the context; crystal_structure is the reference's enum (2: zincblende).
+ * Host code; TBGPU_OK, or TBGPU_E_ARG for an I/O error or a malformed file. */
+int tbgpu_write_eigenvalues(const char *path, char mode, const double *k, int n,
+                            const double *E);
+int tbgpu_write_eigenvector(const tbgpu_ctx *ctx, const char *path,
+                            const tbgpu_dcomplex *wf, int crystal_structure);
+
 /* Timing of the last solve / build (ms, CUDA events on the context stream). */
 typedef struct {
   double build_ms;            /* topology + assembly                          */

@@ -70,6 +70,8 @@ def _lib():
         L.tbgpu_prepare_params.argtypes = [ip, ip, vp, vp, dp, dp, vp]
         L.tbgpu_set_bloch_k.argtypes = [vp, C.POINTER(C.c_double)]
         L.tbgpu_set_ham_precision.argtypes = [vp, ip]
+        L.tbgpu_write_eigenvalues.argtypes = [C.c_char_p, C.c_char, vp, ip, vp]
+        L.tbgpu_write_eigenvector.argtypes = [vp, C.c_char_p, vp, ip]
         L.tbgpu_hx_block_dev.argtypes = [vp, ip, dp, vp, vp]
         L.tbgpu_eigensolve_blk_lanczos.argtypes = [vp, ip, ip, ip, ip, ip, dp, dp, dp, dp, dp,
                                                    ip, ip, vp, vp, vp, vp, vp, vp, ip]
@@ -101,6 +103,17 @@ def _lib():
 
 def _p(a):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def write_eigenvalues(path: str, mode: str, k, E):
+    """nd_Ek file (tbgpu_write_eigenvalues): mode 'i' empties it, 'a' appends
+    the eigenvalues E at Bloch vector k."""
+    e = np.ascontiguousarray(np.asarray(E, np.float64))
+    kv = np.ascontiguousarray(np.asarray(k if k is not None else (0, 0, 0), np.float64))
+    rc = _lib().tbgpu_write_eigenvalues(path.encode(), mode.encode(), _p(kv), int(e.size),
+                                        _p(e))
+    if rc:
+        raise TbgpuError(rc, "tbgpu_write_eigenvalues")
 
 
 def prepare_params(mat: dict, include_strain: bool = True) -> np.ndarray:
@@ -333,6 +346,17 @@ class Hamiltonian:
             v = vec[:2 * self.n * k].reshape(k, self.n, 2)
             out["vectors"] = v[..., 0] + 1j * v[..., 1]
         return out
+
+    def write_eigenvector(self, path: str, vec, crystal_structure: int = 2):
+        """Write one eigenvector (complex [dimension]) as the reference's
+        nd_evec file (tbgpu_write_eigenvector)."""
+        v = np.ascontiguousarray(np.asarray(vec, np.complex128))
+        if v.size != self.n:
+            raise ValueError("vector must hold dimension complex entries")
+        rc = _lib().tbgpu_write_eigenvector(self._ctx, path.encode(), _p(v.view(np.float64)),
+                                            int(crystal_structure))
+        if rc:
+            raise TbgpuError(rc, "tbgpu_write_eigenvector")
 
     def set_bloch_k(self, k):
         """Bloch vector (reference units) for periodic structures; None or

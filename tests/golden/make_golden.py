@@ -4,6 +4,9 @@ Reads, from a NEMO-3D source tree (default /root/reference/NEMO_3D):
   nemo3d/example/TestRun/GaAs_bulk.old_nd_Ek_ascii  (6400 eigenvalues, 40 k)
   nemo3d/example/TestRun/Si_Bulk.old_nd_Ek_ascii    (358 Lanczos eigenvalues)
   nemo3d/bin/Si_Bulk.nd_nbrIndx                      (8x4 neighbour table)
+  nemo3d/example/TestRun/Si_Bulk.nd_Ek               (binary <HDR> file: its
+                                                      header and first 16
+                                                      records)
 and writes tests/golden/reference_golden.npz.  Run it where the reference is
 mounted; the fixture then travels with the repository.
 """
@@ -31,9 +34,12 @@ def main():
     gaas = read_ek(os.path.join(tr, "GaAs_bulk.old_nd_Ek_ascii"))
     si = read_ek(os.path.join(tr, "Si_Bulk.old_nd_Ek_ascii"))
     nbr = read_nbr(os.path.join(ROOT, "nemo3d", "bin", "Si_Bulk.nd_nbrIndx"))
+    raw = open(os.path.join(tr, "Si_Bulk.nd_Ek"), "rb").read()
+    head = raw[:raw.index(b"<\\HDR>") + 6 + 16 * 32]
     np.savez_compressed(os.path.join(HERE, "reference_golden.npz"),
-                        gaas_bulk_kE=gaas, si_bulk_kE=si, si_bulk_nbr=nbr)
-    print("wrote", gaas.shape, si.shape, nbr.shape)
+                        gaas_bulk_kE=gaas, si_bulk_kE=si, si_bulk_nbr=nbr,
+                        si_bulk_nd_ek_head=np.frombuffer(head, np.uint8))
+    print("wrote", gaas.shape, si.shape, nbr.shape, len(head))
 
 
 if __name__ == "__main__":
