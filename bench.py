@@ -167,6 +167,16 @@ def run_reference(args, rank, world):
 
 
 # ------------------------------------------------------------------------------
+def max_over_ranks(value, dist, device):
+    """The largest of one float across the ranks (the job's time is that of
+    its slowest replica); `dist` is torch.distributed or None for one rank."""
+    import torch
+    t = torch.tensor([float(value)], device=device, dtype=torch.float64)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     from nemo3d_b200 import tbgpu
@@ -223,11 +233,7 @@ def run_ours(args, rank, world, local_rank):
         e1.record(stream)
         torch.cuda.synchronize()
     barrier()
-    ms = e0.elapsed_time(e1) / args.steps
-    t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms = float(t.item())
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, dist, "cuda")
 
     # end to end through the host-pointer C ABI
     e2e_s = None
@@ -243,10 +249,7 @@ def run_ours(args, rank, world, local_rank):
             H.close()
             torch.cuda.synchronize()
             times.append(time.perf_counter() - t0)
-        tt = torch.tensor([float(np.mean(times))], device="cuda", dtype=torch.float64)
-        if dist is not None:
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_s = float(tt.item())
+        e2e_s = max_over_ranks(float(np.mean(times)), dist, "cuda")
         h2d = st.types.nbytes + st.dsp.nbytes + r0_h.nbytes + 8 * 8 * 68
         d2h = len(out["vectors"]) * 16 * n + 8 * len(out["values"])
 
