@@ -124,6 +124,18 @@ void tbgpu_matvect_mult(const int **argList, tbgpu_dcomplex *y,
  * the Hamiltonian's bytes; entries carry float rounding (~6e-8 relative). */
 int tbgpu_set_ham_precision(tbgpu_ctx *ctx, int bits);
 
+/* Storage of the bond blocks, set before tbgpu_build_hamiltonian: 0 (default)
+ * assembles and stores them once (the reference's HamCompute=SparseStore,
+ * XMLtoC/apps/ioNemo3D/src/ElAlg_struct.H:25);
+ * 1 recomputes each block inside every H*x from the geometry and the
+ * parameters (HamCompute=Recompute, Hmult_spds_col multiplying on the fly,
+ * nemo3d/src/base/h_cvectr_mult.c:1134-1886): only the on-site records are
+ * stored, for structures whose blocks would not fit in device memory, at the
+ * price of the Slater-Koster arithmetic in every product.  Not combined with
+ * the 32-bit store (TBGPU_E_UNSUPPORTED at build); tbgpu_hx_dot_noalloc
+ * refuses recompute contexts with TBGPU_E_UNSUPPORTED. */
+int tbgpu_set_ham_storage(tbgpu_ctx *ctx, int recompute);
+
 /* Bloch vector for periodic structures (geo_struct::phasePeriodic,
  * nemo3d/src/base/geo_struct.h:811-826, used by Hmult_stored.c:386-437): a
  * bond that crosses the periodic boundary by images w (-1/0/+1 per axis)

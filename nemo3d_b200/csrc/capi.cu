@@ -287,8 +287,19 @@ int tbgpu_export_hamiltonian(const tbgpu_ctx *ctx, double *onsite, double *block
     for (size_t i = 0; i < count; i++) dst[i] = tmp[i];
     return true;
   };
-  if (blocks && !fetch(blocks, c.d_blocks, c.d_blocks32, n * 4 * norb * norb))
+  if (blocks && c.recompute) {  // not stored: compute them for the export
+    double *tmp = nullptr;
+    const size_t cnt = n * 4 * norb * norb;
+    if (cudaMalloc(&tmp, cnt * sizeof(double)) != cudaSuccess) return set_error(TBGPU_E_NOMEM);
+    int rc = compute_blocks(const_cast<Ctx &>(c), tmp);
+    if (!rc && (cudaStreamSynchronize(c.stream) != cudaSuccess ||
+                cudaMemcpy(blocks, tmp, cnt * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess))
+      rc = set_error(TBGPU_E_CUDA);
+    cudaFree(tmp);
+    if (rc) return rc;
+  } else if (blocks && !fetch(blocks, c.d_blocks, c.d_blocks32, n * 4 * norb * norb)) {
     return set_error(TBGPU_E_CUDA);
+  }
   if (!onsite) return TBGPU_OK;
   std::vector<double> rec(n * c.ons);
   if (!fetch(rec.data(), c.d_onsite, c.d_onsite32, rec.size())) return set_error(TBGPU_E_CUDA);
@@ -333,6 +344,14 @@ int tbgpu_set_ham_precision(tbgpu_ctx *ctx, int bits) {
   Ctx &c = *C(ctx);
   if (c.built) return set_error(TBGPU_E_STATE);
   c.ham_fp32 = bits == 32;
+  return TBGPU_OK;
+}
+
+int tbgpu_set_ham_storage(tbgpu_ctx *ctx, int recompute) {
+  if (!ctx || (recompute != 0 && recompute != 1)) return set_error(TBGPU_E_ARG);
+  Ctx &c = *C(ctx);
+  if (c.built) return set_error(TBGPU_E_STATE);
+  c.recompute = recompute == 1;
   return TBGPU_OK;
 }
 

@@ -256,7 +256,8 @@ int launch_ns(Ctx &c, int p, const double *x, long xs, double *y, long ys, doubl
 int launch_spmm(Ctx &c, int p, const double *x, long xstride, double *y, long ystride,
                 double shift, cudaStream_t s) {
   if (p < 1 || p > 8) return set_error(TBGPU_E_ARG);
-  if (p >= 2 && c.norb == kNorb && !c.bloch && !c.ham_fp32 && c.spmv_variant != 1)
+  if (p >= 2 && c.norb == kNorb && !c.bloch && !c.ham_fp32 && !c.recompute &&
+      c.spmv_variant != 1)
     return c.nspin == 2 ? launch_ns<2>(c, p, x, xstride, y, ystride, shift, s)
                         : launch_ns<1>(c, p, x, xstride, y, ystride, shift, s);
   for (int v = 0; v < p; v++) {

@@ -213,6 +213,7 @@ static int launch_t(Ctx &c, const double *x, double *y, double shift,
 
 int launch_spmv(Ctx &c, const double *x, double *y, double shift, const double *xnorm,
                 int xidx, double *alpha_out, int aidx, cudaStream_t s) {
+  if (c.recompute) return launch_spmv_recompute(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
   // the warp-staged kernel has no phase support: periodic structures away
   // from Gamma take the lane-gather kernel
   if (c.norb == 10 && c.spmv_variant != 1 && !c.bloch)
@@ -258,6 +259,7 @@ static int launch_scratch_t(Ctx &c, const double *x, double *y, double shift, do
 
 int launch_spmv_scratch(Ctx &c, const double *x, double *y, double shift, double *partial,
                         unsigned int *counter, int cap, double *dot_out, cudaStream_t s) {
+  if (c.recompute) return set_error(TBGPU_E_UNSUPPORTED);
   if (c.norb == 10 && !c.bloch)
     return launch_spmv_async_scratch(c, x, y, shift, partial, counter, cap, dot_out, s);
   if (c.norb == 10 && c.nspin == 2)

@@ -69,6 +69,8 @@ struct Ctx {
   // single-precision store (the reference's HamMemorySave build): the same
   // arrays in float, and d_onsite / d_blocks released after assembly
   bool ham_fp32 = false;
+  // blocks recomputed inside every H*x instead of stored (HamCompute=Recompute)
+  bool recompute = false;
   float *d_onsite32 = nullptr;
   float *d_blocks32 = nullptr;
   // H*x work order: groups of up to 3 consecutive atoms of one k-pencil of
@@ -124,6 +126,10 @@ int build_topology(Ctx &c);
 int build_phases(Ctx &c);  // fills d_phase for c.kvec
 // build.cu
 int assemble(Ctx &c);
+int compute_blocks(Ctx &c, double *blocks);
+int launch_spmv_recompute(Ctx &c, const double *x, double *y, double shift,
+                          const double *xnorm, int xidx, double *alpha_out, int aidx,
+                          cudaStream_t s);
 // spmv.cu
 int launch_spmv(Ctx &c, const double *x, double *y, double shift,
                 const double *xscale_dev, int scale_index, double *alpha_out,

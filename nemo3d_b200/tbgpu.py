@@ -70,6 +70,7 @@ def _lib():
         L.tbgpu_prepare_params.argtypes = [ip, ip, vp, vp, dp, dp, vp]
         L.tbgpu_set_bloch_k.argtypes = [vp, C.POINTER(C.c_double)]
         L.tbgpu_set_ham_precision.argtypes = [vp, ip]
+        L.tbgpu_set_ham_storage.argtypes = [vp, ip]
         L.tbgpu_write_eigenvalues.argtypes = [C.c_char_p, C.c_char, vp, ip, vp]
         L.tbgpu_write_eigenvector.argtypes = [vp, C.c_char_p, vp, ip]
         L.tbgpu_hx_block_dev.argtypes = [vp, ip, dp, vp, vp]
@@ -150,7 +151,7 @@ class Hamiltonian:
 
     def __init__(self, structure, model="sp3d5s*_so", materials=None, include_strain=True,
                  passivate=True, dangling_shift=30.0, device_inputs=None, build=True,
-                 ham_bits=64):
+                 ham_bits=64, recompute=False):
         L = _lib()
         self.structure = structure
         self.model = model
@@ -184,6 +185,11 @@ class Hamiltonian:
             raise TbgpuError(rc, "tbgpu_ctx_create")
         self._ctx = ctx
         self._built = False
+        if recompute:
+            rc = L.tbgpu_set_ham_storage(ctx, 1)
+            if rc:
+                L.tbgpu_ctx_destroy(ctx)
+                raise TbgpuError(rc, "tbgpu_set_ham_storage")
         if ham_bits != 64:
             rc = L.tbgpu_set_ham_precision(ctx, int(ham_bits))
             if rc:
