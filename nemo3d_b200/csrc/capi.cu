@@ -31,7 +31,7 @@ static void free_ctx(Ctx *c) {
   void *ptrs[] = {c->d_type, c->d_dsp, c->d_par, c->d_par_ok, c->d_site_index, c->d_atom_site,
                   c->d_nbr, c->d_site_m, c->d_surface, c->d_onsite, c->d_blocks, c->d_partial,
                   c->d_counter, c->d_status, c->d_x, c->d_y, c->d_phase, c->d_groups,
-                  c->d_blocks32, c->d_onsite32};
+                  c->d_blocks32, c->d_onsite32, c->d_rc_order};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);

@@ -71,6 +71,10 @@ struct Ctx {
   bool ham_fp32 = false;
   // blocks recomputed inside every H*x instead of stored (HamCompute=Recompute)
   bool recompute = false;
+  // recompute work order: eight cations per warp, then eight anions per
+  // warp, padded with -1 (rc_cat_warps warps of cations, rc_warps in all)
+  int *d_rc_order = nullptr;
+  long rc_cat_warps = 0, rc_warps = 0;
   float *d_onsite32 = nullptr;
   float *d_blocks32 = nullptr;
   // H*x work order: groups of up to 3 consecutive atoms of one k-pencil of
@@ -127,6 +131,8 @@ int build_phases(Ctx &c);  // fills d_phase for c.kvec
 // build.cu
 int assemble(Ctx &c);
 int compute_blocks(Ctx &c, double *blocks);
+// recompute.cu
+int build_recompute_order(Ctx &c);
 int launch_spmv_recompute(Ctx &c, const double *x, double *y, double shift,
                           const double *xnorm, int xidx, double *alpha_out, int aidx,
                           cudaStream_t s);
