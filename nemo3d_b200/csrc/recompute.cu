@@ -30,6 +30,12 @@ namespace tbgpu {
 namespace {
 
 constexpr int kRcAtoms = 8;  // atoms per warp in the recompute work order
+// resident blocks per SM asked of the compiler: the 20-state model trades a
+// few spilled registers for 12 warps per SM (1.81 -> 1.40 ms at 1.02M atoms),
+// the 10-state ones fit 16 warps without spills (1.10 -> 0.92 ms)
+__host__ __device__ constexpr int rc_min_blocks(int norb, int nspin) {
+  return norb == 10 && nspin == 2 ? 3 : 4;
+}
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -100,7 +106,7 @@ __device__ __forceinline__ void bond_from_anion(const double d[3], const double 
 }
 
 template <int NORB, int NSPIN, int WPB, bool DOT, bool PHASE>
-__global__ void __launch_bounds__(WPB * 32)
+__global__ void __launch_bounds__(WPB * 32, rc_min_blocks(NORB, NSPIN))
     k_spmv_recompute(long cat_warps, long nwarps, const int *__restrict__ order,
                      const int4 *__restrict__ nbr, const unsigned char *__restrict__ site_m,
                      const int *__restrict__ atom_site, const unsigned char *__restrict__ type,
