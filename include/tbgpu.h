@@ -136,6 +136,29 @@ int tbgpu_set_ham_precision(tbgpu_ctx *ctx, int bits);
  * refuses recompute contexts with TBGPU_E_UNSUPPORTED. */
 int tbgpu_set_ham_storage(tbgpu_ctx *ctx, int recompute);
 
+/* Precision of the Lanczos vectors, set before tbgpu_build_hamiltonian: 64
+ * (default) or 32.  32 is the mixed-precision solve (no counterpart in the
+ * reference; it needs the 32-bit store, tbgpu_set_ham_precision(ctx, 32),
+ * and a 10-orbital model, else TBGPU_E_UNSUPPORTED at build): the
+ * recurrence vectors are complex float and H*x accumulates in float, while
+ * alpha, beta, their reductions, the tridiagonal eigenvalues, the
+ * convergence test and the eigenvector accumulation stay double.  The
+ * eigenvectors a solve returns are then refined in double: H*v with the
+ * double-precision recompute product (bit-identical blocks to the stored
+ * assembly), a Rayleigh-Ritz step over groups of up to 8 vectors, and the
+ * refined eigenvalues replace the Lanczos ones; the residual
+ * ||H v - lambda v|| and the change of each eigenvalue are returned by
+ * tbgpu_get_state_errors.  Eigenvalues without a requested vector keep the
+ * float recurrence's accuracy.  Not with Bloch phases (TBGPU_E_UNSUPPORTED
+ * at solve). */
+int tbgpu_set_lanczos_precision(tbgpu_ctx *ctx, int bits);
+
+/* Per state of the last solve of a mixed-precision context, for the n
+ * states that had eigenvectors: residual[i] = ||H v_i - lambda_i v_i|| (eV,
+ * unit v_i) and delta[i] = lambda_i(refined) - lambda_i(Lanczos).  Either
+ * pointer may be NULL.  Returns the number of states written (<= cap). */
+int tbgpu_get_state_errors(const tbgpu_ctx *ctx, int cap, double *residual, double *delta);
+
 /* Bloch vector for periodic structures (geo_struct::phasePeriodic,
  * nemo3d/src/base/geo_struct.h:811-826, used by Hmult_stored.c:386-437): a
  * bond that crosses the periodic boundary by images w (-1/0/+1 per axis)
@@ -148,6 +171,13 @@ int tbgpu_set_bloch_k(tbgpu_ctx *ctx, const double *k);
 /* y = (H - shift) x on device vectors (asynchronous on the context stream). */
 int tbgpu_hx_dev(tbgpu_ctx *ctx, double shift, const double *x_dev,
                  double *y_dev);
+
+/* The mixed-precision product: y = (H - shift) x on complex-float device
+ * vectors ({float re, im} per entry) over the 32-bit store, accumulated in
+ * float (the H*x of a tbgpu_set_lanczos_precision(ctx, 32) solve; no
+ * counterpart in the reference).  10-orbital models with the 32-bit store
+ * only, at the Gamma point; else TBGPU_E_UNSUPPORTED. */
+int tbgpu_hx_dev_f32(tbgpu_ctx *ctx, double shift, const float *x_dev, float *y_dev);
 
 /* Y_v = (H - shift) X_v for a block of p <= 8 device vectors stored one
  * after the other ([p][dimension] complex): the block product the block
@@ -297,6 +327,7 @@ typedef struct {
   long spmv_launches;
   long lanczos_iterations;
   long kernel_launches;       /* all kernels launched by the last solve       */
+  double refine_ms;           /* double-precision refinement (mixed solve)    */
 } tbgpu_stats;
 int tbgpu_set_profiling(tbgpu_ctx *ctx, int on);
 int tbgpu_get_stats(const tbgpu_ctx *ctx, tbgpu_stats *out);

@@ -224,6 +224,7 @@ static int to_float(Ctx &c, long n, const double *in, float **out) {
 int assemble(Ctx &c) {
   const long na = c.natoms;
   if (c.recompute && c.ham_fp32) return set_error(TBGPU_E_UNSUPPORTED);
+  if (c.lanczos_f32 && (!c.ham_fp32 || c.norb != 10)) return set_error(TBGPU_E_UNSUPPORTED);
   // recompute: the blocks are not stored; the assembly still runs the bond
   // kernel for the on-site strain corrections
   if (!c.recompute)
@@ -235,15 +236,17 @@ int assemble(Ctx &c) {
   else if (c.norb == 5 && c.nspin == 2) rc = assemble_t<5, 2>(c);
   else if (c.norb == 5 && c.nspin == 1) rc = assemble_t<5, 1>(c);
   else return set_error(rc);
-  if (!rc && c.recompute) rc = build_recompute_order(c);
+  if (!rc && (c.recompute || c.lanczos_f32)) rc = build_recompute_order(c);
   if (rc || !c.ham_fp32) return rc;
   if ((rc = to_float(c, na * 4 * c.norb * c.norb, c.d_blocks, &c.d_blocks32))) return rc;
   if ((rc = to_float(c, na * c.ons, c.d_onsite, &c.d_onsite32))) return rc;
   TB_CUDA(cudaStreamSynchronize(c.stream));
   cudaFree(c.d_blocks);
-  cudaFree(c.d_onsite);
   c.d_blocks = nullptr;
-  c.d_onsite = nullptr;
+  if (!c.lanczos_f32) {  // the mixed solve refines with the double records
+    cudaFree(c.d_onsite);
+    c.d_onsite = nullptr;
+  }
   return TBGPU_OK;
 }
 

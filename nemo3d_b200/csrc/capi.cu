@@ -1,4 +1,5 @@
 // C ABI entry points of libtbgpu.so (declared in include/tbgpu.h).
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -170,6 +171,14 @@ int tbgpu_hx_dev(tbgpu_ctx *ctx, double shift, const double *x_dev, double *y_de
   Ctx &c = *C(ctx);
   if (!c.built) return set_error(TBGPU_E_STATE);
   return launch_spmv(c, x_dev, y_dev, shift, nullptr, 0, nullptr, 0, c.stream);
+}
+
+int tbgpu_hx_dev_f32(tbgpu_ctx *ctx, double shift, const float *x_dev, float *y_dev) {
+  if (!ctx || !x_dev || !y_dev) return set_error(TBGPU_E_ARG);
+  Ctx &c = *C(ctx);
+  if (!c.built) return set_error(TBGPU_E_STATE);
+  if (c.bloch || c.recompute) return set_error(TBGPU_E_UNSUPPORTED);
+  return launch_spmv_async_f32(c, x_dev, y_dev, shift, nullptr, 0, nullptr, 0, c.stream);
 }
 
 void tbgpu_matvect_mult(const int **argList, tbgpu_dcomplex *y, const tbgpu_dcomplex *x) {
@@ -353,6 +362,25 @@ int tbgpu_set_ham_storage(tbgpu_ctx *ctx, int recompute) {
   if (c.built) return set_error(TBGPU_E_STATE);
   c.recompute = recompute == 1;
   return TBGPU_OK;
+}
+
+int tbgpu_set_lanczos_precision(tbgpu_ctx *ctx, int bits) {
+  if (!ctx || (bits != 32 && bits != 64)) return set_error(TBGPU_E_ARG);
+  Ctx &c = *C(ctx);
+  if (c.built) return set_error(TBGPU_E_STATE);
+  c.lanczos_f32 = bits == 32;
+  return TBGPU_OK;
+}
+
+int tbgpu_get_state_errors(const tbgpu_ctx *ctx, int cap, double *residual, double *delta) {
+  if (!ctx || cap < 0) return set_error(TBGPU_E_ARG);
+  const Ctx &c = *reinterpret_cast<const Ctx *>(ctx);
+  const int n = std::min(cap, int(c.state_resid.size()));
+  for (int i = 0; i < n; i++) {
+    if (residual) residual[i] = c.state_resid[i];
+    if (delta) delta[i] = c.state_delta[i];
+  }
+  return n;
 }
 
 int tbgpu_set_bloch_k(tbgpu_ctx *ctx, const double *k) {

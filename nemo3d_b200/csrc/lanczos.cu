@@ -51,35 +51,51 @@ static unsigned red_grid(const Ctx &c, long n2) {
   return unsigned(std::max<long>(g, 1));
 }
 
+// Vector kernels for complex double (double2) or, in the mixed-precision
+// solve, complex float (float2) Lanczos vectors; arithmetic and the norms
+// are double in both.
+__device__ __forceinline__ double2 widen(double2 v) { return v; }
+__device__ __forceinline__ double2 widen(float2 v) { return make_double2(v.x, v.y); }
+template <typename VT> __device__ __forceinline__ VT narrow(double x, double y);
+template <> __device__ __forceinline__ double2 narrow<double2>(double x, double y) {
+  return make_double2(x, y);
+}
+template <> __device__ __forceinline__ float2 narrow<float2>(double x, double y) {
+  return make_float2(float(x), float(y));
+}
+
 // out[idx] = sqrt(sum |x|^2)
+template <typename VT>
 __global__ void __launch_bounds__(kRedThreads)
-    k_norm(long n2, const double2 *__restrict__ x, double *partial, unsigned *counter,
+    k_norm(long n2, const VT *__restrict__ x, double *partial, unsigned *counter,
            double *out, int idx) {
   double s = 0.0;
   for (long j = blockIdx.x * (long)blockDim.x + threadIdx.x; j < n2;
        j += (long)gridDim.x * blockDim.x) {
-    const double2 v = x[j];
+    const double2 v = widen(x[j]);
     s += v.x * v.x + v.y * v.y;
   }
   grid_reduce<kRedThreads>(s, partial, counter, out, idx, true);
 }
 
 // y = x / (*den)   (lanczos_initialize divides by the norm, eigsys3d_par.c:199-211)
+template <typename VT>
 __global__ void k_divide(long n2, const double2 *__restrict__ x, const double *den,
-                         double2 *__restrict__ y) {
+                         VT *__restrict__ y) {
   const double d = *den;
   for (long j = blockIdx.x * (long)blockDim.x + threadIdx.x; j < n2;
        j += (long)gridDim.x * blockDim.x) {
     const double2 v = x[j];
-    y[j] = make_double2(v.x / d, v.y / d);
+    y[j] = narrow<VT>(v.x / d, v.y / d);
   }
 }
 
 // r_n = w - (alpha q + beta_prev q_prev), q = rc/bet[it], q_prev = rp/bet[it-1];
 // bet[it+1] = ||r_n||.  bet[0] is the norm of the start vector.
+template <typename VT>
 __global__ void __launch_bounds__(kRedThreads)
-    k_update(long n2, const double2 *__restrict__ w, const double2 *__restrict__ rc,
-             const double2 *__restrict__ rp, double2 *__restrict__ rout,
+    k_update(long n2, const VT *__restrict__ w, const VT *__restrict__ rc,
+             const VT *__restrict__ rp, VT *__restrict__ rout,
              const double *alpha, double *bet, int it, double *partial, unsigned *counter) {
   const double al = alpha[it], bprev = bet[it];
   const double iq = 1.0 / bprev;
@@ -87,26 +103,26 @@ __global__ void __launch_bounds__(kRedThreads)
   double s = 0.0;
   for (long j = blockIdx.x * (long)blockDim.x + threadIdx.x; j < n2;
        j += (long)gridDim.x * blockDim.x) {
-    const double2 wv = w[j], cv = rc[j];
+    const double2 wv = widen(w[j]), cv = widen(rc[j]);
     const double2 q = make_double2(cv.x * iq, cv.y * iq);
     double2 p = make_double2(0.0, 0.0);
     if (it > 0) {
-      const double2 pv = rp[j];
+      const double2 pv = widen(rp[j]);
       p = make_double2(pv.x * ip, pv.y * ip);
     }
-    double2 r;
-    r.x = wv.x - (al * q.x + bprev * p.x);
-    r.y = wv.y - (al * q.y + bprev * p.y);
+    const VT r = narrow<VT>(wv.x - (al * q.x + bprev * p.x), wv.y - (al * q.y + bprev * p.y));
     rout[j] = r;
-    s += r.x * r.x + r.y * r.y;
+    const double2 rw = widen(r);  // the norm of the vector as stored
+    s += rw.x * rw.x + rw.y * rw.y;
   }
   grid_reduce<kRedThreads>(s, partial, counter, bet, it + 1, true);
 }
 
 constexpr int kMaxChunk = 32;
 constexpr int kVecGroup = 16;
+template <typename VT>
 struct ChunkPtrs {
-  const double2 *r[kMaxChunk];
+  const VT *r[kMaxChunk];
 };
 
 // Coefficients of one chunk, passed by value: the kernel reads them from the
@@ -117,9 +133,9 @@ struct ChunkCoef {
 
 // V[e] += sum_k coef[k][e] * R_k for one group of NV vectors (memory bound:
 // the chunk's nk r-vectors and the NV eigenvectors are streamed once)
-template <int NV>
+template <int NV, typename VT>
 __global__ void __launch_bounds__(256)
-    k_accum(long n2, int nk, ChunkPtrs R, ChunkCoef C, double2 *__restrict__ V) {
+    k_accum(long n2, int nk, ChunkPtrs<VT> R, ChunkCoef C, double2 *__restrict__ V) {
   for (long j = blockIdx.x * (long)blockDim.x + threadIdx.x; j < n2;
        j += (long)gridDim.x * blockDim.x) {
     double2 acc[NV];
@@ -128,7 +144,7 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
     for (int k = 0; k < kMaxChunk; k++) {
       if (k < nk) {
-        const double2 r = __ldg(R.r[k] + j);
+        const double2 r = widen(__ldg(R.r[k] + j));
 #pragma unroll
         for (int e = 0; e < NV; e++) {
           acc[e].x = fma(C.c[k][e], r.x, acc[e].x);
@@ -141,11 +157,12 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+template <typename VT>
 static void launch_accum(int nv, unsigned grid, cudaStream_t s, long n2, int nk,
-                         const ChunkPtrs &R, const ChunkCoef &C, double2 *V) {
+                         const ChunkPtrs<VT> &R, const ChunkCoef &C, double2 *V) {
   switch (nv) {
 #define TBGPU_ACCUM_CASE(N) \
-  case N: k_accum<N><<<grid, 256, 0, s>>>(n2, nk, R, C, V); break;
+  case N: k_accum<N, VT><<<grid, 256, 0, s>>>(n2, nk, R, C, V); break;
     TBGPU_ACCUM_CASE(1) TBGPU_ACCUM_CASE(2) TBGPU_ACCUM_CASE(3) TBGPU_ACCUM_CASE(4)
     TBGPU_ACCUM_CASE(5) TBGPU_ACCUM_CASE(6) TBGPU_ACCUM_CASE(7) TBGPU_ACCUM_CASE(8)
     TBGPU_ACCUM_CASE(9) TBGPU_ACCUM_CASE(10) TBGPU_ACCUM_CASE(11) TBGPU_ACCUM_CASE(12)
@@ -300,12 +317,31 @@ struct Timers {
   cudaEvent_t t0, t1, t2, t3;
 };
 
-int solve(Ctx &c, const SolveArgs &A, const double *r0_dev, double *values, int *conv_iters,
-          int *iterations, double *V_dev, int maxvec) {
+// H*x of one Lanczos step on the context's stored Hamiltonian
+static int spmv_step(Ctx &c, const double2 *x, double2 *y, const double *bet, int it,
+                     double *alpha, cudaStream_t s) {
+  return launch_spmv(c, reinterpret_cast<const double *>(x), reinterpret_cast<double *>(y), 0.0,
+                     bet, it, alpha, it, s);
+}
+static int spmv_step(Ctx &c, const float2 *x, float2 *y, const double *bet, int it,
+                     double *alpha, cudaStream_t s) {
+  return launch_spmv_async_f32(c, reinterpret_cast<const float *>(x), reinterpret_cast<float *>(y),
+                               0.0, bet, it, alpha, it, s);
+}
+
+template <typename VT>
+static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *values,
+                   int *conv_iters, int *iterations, double *V_dev, int maxvec) {
+  constexpr bool kMixed = sizeof(VT) == sizeof(float2);
   if (!c.built) return set_error(TBGPU_E_STATE);
   if (A.imax < 2 || A.conv_skip < 1 || !values || !r0_dev) return set_error(TBGPU_E_ARG);
+  if (kMixed && c.bloch) return set_error(TBGPU_E_UNSUPPORTED);
+  c.state_resid.clear();
+  c.state_delta.clear();
+  c.stats.refine_ms = 0.0;
   const long n2 = c.natoms * c.nb;  // complex entries
-  const size_t vbytes = sizeof(double2) * n2;
+  const size_t vbytes = sizeof(VT) * n2;        // one Lanczos vector
+  const size_t ebytes = sizeof(double2) * n2;   // one eigenvector (always double)
   cudaStream_t s = c.stream;
   const unsigned rg = red_grid(c, n2);
   int rc = ensure_partials(c, int(rg));
@@ -316,8 +352,8 @@ int solve(Ctx &c, const SolveArgs &A, const double *r0_dev, double *values, int 
 
   // device state
   const int S1 = 3;  // ring of r's for the first pass
-  double2 *ring[kMaxChunk + 1] = {nullptr};
-  double2 *W = nullptr;
+  VT *ring[kMaxChunk + 1] = {nullptr};
+  VT *W = nullptr;
   double *d_alpha = nullptr, *d_bet = nullptr, *d_tmp = nullptr;
   double *h_alpha = nullptr, *h_bet = nullptr;
   std::vector<cudaEvent_t> spmv_ev;
@@ -362,33 +398,32 @@ int solve(Ctx &c, const SolveArgs &A, const double *r0_dev, double *values, int 
 
   // start vector: r = r0 / ||r0||; bet[0] = ||r||
   auto start = [&](double *bet) -> int {
-    k_norm<<<rg, kRedThreads, 0, s>>>(n2, reinterpret_cast<const double2 *>(r0_dev),
-                                      c.d_partial, c.d_counter, d_tmp, 0);
-    k_divide<<<rg, kRedThreads, 0, s>>>(n2, reinterpret_cast<const double2 *>(r0_dev), d_tmp,
-                                        ring[0]);
-    k_norm<<<rg, kRedThreads, 0, s>>>(n2, ring[0], c.d_partial, c.d_counter, bet, 0);
+    k_norm<double2><<<rg, kRedThreads, 0, s>>>(n2, reinterpret_cast<const double2 *>(r0_dev),
+                                              c.d_partial, c.d_counter, d_tmp, 0);
+    k_divide<VT><<<rg, kRedThreads, 0, s>>>(n2, reinterpret_cast<const double2 *>(r0_dev), d_tmp,
+                                            ring[0]);
+    k_norm<VT><<<rg, kRedThreads, 0, s>>>(n2, ring[0], c.d_partial, c.d_counter, bet, 0);
     launches += 3;
     return cudaGetLastError() == cudaSuccess ? TBGPU_OK : set_error(TBGPU_E_CUDA);
   };
   // one Lanczos iteration with ring size S
   auto step = [&](int it, int S, double *bet) -> int {
-    double2 *rc_ = ring[it % S], *rp_ = ring[(it + S - 1) % S], *ro = ring[(it + 1) % S];
+    VT *rc_ = ring[it % S], *rp_ = ring[(it + S - 1) % S], *ro = ring[(it + 1) % S];
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (c.profiling) {
       cudaEventCreate(&e0);
       cudaEventCreate(&e1);
       cudaEventRecord(e0, s);
     }
-    int r_ = launch_spmv(c, reinterpret_cast<const double *>(rc_), reinterpret_cast<double *>(W),
-                         0.0, bet, it, d_alpha, it, s);
+    int r_ = spmv_step(c, rc_, W, bet, it, d_alpha, s);
     if (r_) return r_;
     if (c.profiling) {
       cudaEventRecord(e1, s);
       spmv_ev.push_back(e0);
       spmv_ev.push_back(e1);
     }
-    k_update<<<rg, kRedThreads, 0, s>>>(n2, W, rc_, it > 0 ? rp_ : nullptr, ro, d_alpha, bet, it,
-                                        c.d_partial, c.d_counter);
+    k_update<VT><<<rg, kRedThreads, 0, s>>>(n2, W, rc_, it > 0 ? rp_ : nullptr, ro, d_alpha, bet,
+                                            it, c.d_partial, c.d_counter);
     launches += 2;
     return cudaGetLastError() == cudaSuccess ? TBGPU_OK : set_error(TBGPU_E_CUDA);
   };
@@ -542,14 +577,14 @@ int solve(Ctx &c, const SolveArgs &A, const double *r0_dev, double *values, int 
     while (K > 2 && size_t(K + 1 - S1) * vbytes + (256ull << 20) > fre) K /= 2;
     const int S2 = K + 1;
     for (int i = S1; i < S2; i++) SOLVE_CUDA(cudaMalloc(&ring[i], vbytes));
-    SOLVE_CUDA(cudaMemsetAsync(V_dev, 0, vbytes * nvec, s));
+    SOLVE_CUDA(cudaMemsetAsync(V_dev, 0, ebytes * nvec, s));
     cudaEventRecord(tm.t2, s);
     SOLVE_RC(start(d_bet));
     int it0 = 0;
     for (int it = 0; it < maxit; it++) {
       SOLVE_RC(step(it, S2, d_bet));
       if ((it + 1 - it0) == K || it == maxit - 1) {
-        ChunkPtrs P{};
+        ChunkPtrs<VT> P{};
         const int nk = it + 1 - it0;
         for (int k = 0; k < nk; k++) P.r[k] = ring[(it0 + k) % S2];
         for (int g = 0; g < nvec; g += kVecGroup) {
@@ -557,7 +592,7 @@ int solve(Ctx &c, const SolveArgs &A, const double *r0_dev, double *values, int 
           ChunkCoef C{};
           for (int k = 0; k < nk; k++)
             for (int e = 0; e < nv; e++) C.c[k][e] = coef[size_t(it0 + k) * nvec + g + e];
-          launch_accum(nv, rg, s, n2, nk, P, C, reinterpret_cast<double2 *>(V_dev) + size_t(g) * n2);
+          launch_accum<VT>(nv, rg, s, n2, nk, P, C, reinterpret_cast<double2 *>(V_dev) + size_t(g) * n2);
           launches++;
         }
         it0 = it + 1;
@@ -567,6 +602,14 @@ int solve(Ctx &c, const SolveArgs &A, const double *r0_dev, double *values, int 
     SOLVE_CUDA(cudaStreamSynchronize(s));
     cudaEventElapsedTime(&ms, tm.t2, tm.t3);
     c.stats.vectors_ms = ms;
+    if (kMixed) {  // double-precision Rayleigh-Ritz of the Ritz vectors
+      cudaEventRecord(tm.t2, s);
+      SOLVE_RC(refine_ritz(c, V_dev, nvec, values, c.state_resid, c.state_delta, s));
+      cudaEventRecord(tm.t3, s);
+      SOLVE_CUDA(cudaStreamSynchronize(s));
+      cudaEventElapsedTime(&ms, tm.t2, tm.t3);
+      c.stats.refine_ms = ms;
+    }
   }
   if (c.profiling) {
     SOLVE_CUDA(cudaStreamSynchronize(s));
@@ -588,6 +631,13 @@ int solve(Ctx &c, const SolveArgs &A, const double *r0_dev, double *values, int 
 #undef SOLVE_CUDA
 #undef SOLVE_RC
   return ne;
+}
+
+int solve(Ctx &c, const SolveArgs &A, const double *r0_dev, double *values, int *conv_iters,
+          int *iterations, double *V_dev, int maxvec) {
+  if (c.lanczos_f32)
+    return solve_t<float2>(c, A, r0_dev, values, conv_iters, iterations, V_dev, maxvec);
+  return solve_t<double2>(c, A, r0_dev, values, conv_iters, iterations, V_dev, maxvec);
 }
 
 }  // namespace tbgpu

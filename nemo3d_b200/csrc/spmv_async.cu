@@ -33,37 +33,47 @@ namespace {
 
 using namespace stage;
 constexpr int kNorb = 10;
+constexpr int kWarpsF32 = 16;  // warps per SM of the float-vector kernel
 
-__device__ __forceinline__ void cfma_r(double2 &acc, double v, double2 a) {
+template <typename T, typename V>
+__device__ __forceinline__ void cfma_r(V &acc, T v, V a) {
   acc.x = fma(v, a.x, acc.x);
   acc.y = fma(v, a.y, acc.y);
 }
-__device__ __forceinline__ void cfma_i(double2 &acc, double lam, double2 a) {
+template <typename T, typename V>
+__device__ __forceinline__ void cfma_i(V &acc, T lam, V a) {
   acc.x -= lam * a.y;
   acc.y += lam * a.x;
 }
+template <typename V> struct Scalar;
+template <> struct Scalar<double2> { using T = double; };
+template <> struct Scalar<float2> { using T = float; };
 
 // HT: element type of the stored Hamiltonian (double, or float for the
-// single-precision store)
-template <int NSPIN, int WARPS, int STAGES, typename HT_ = double>
+// single-precision store); VT: vector element (double2, or float2 for the
+// mixed-precision Lanczos, whose products accumulate in float)
+template <int NSPIN, int WARPS, int STAGES, typename HT_ = double, typename VT_ = double2>
 struct Layout {
   using HT = HT_;
+  using VT = VT_;
+  using RT = typename Scalar<VT>::T;
   static constexpr int HS = int(sizeof(HT));
+  static constexpr int VS = int(sizeof(VT));
   static constexpr int NB = kNorb * NSPIN;
   static constexpr int ONS = onsite_len(NB);
   static constexpr int BLK = kNorb * kNorb;      // elements per bond block
   static constexpr int BLK_CH = BLK * HS / 16;   // 16-byte chunks per block (50 or 25)
-  static constexpr int X_CH = NB * 16 / 16;      // chunks per vector segment
+  static constexpr int X_CH = NB * VS / 16;      // chunks per vector segment
   static constexpr int ONS_CH = ONS * HS / 16;   // chunks per on-site record
   // per-atom stride, padded by 48 bytes so the three atoms of a warp start
   // on different shared-memory banks
-  static constexpr int ATOM = 4 * BLK * HS + 5 * NB * 16 + ONS * HS + 48;
+  static constexpr int ATOM = 4 * BLK * HS + 5 * NB * VS + ONS * HS + 48;
   static constexpr int STAGE = kAPW * ATOM;
   static constexpr int WARP = STAGES * STAGE;
   static constexpr int SMEM = WARPS * WARP;
   static __device__ __forceinline__ int blk(int i) { return i * ATOM; }
   static __device__ __forceinline__ int xs(int i) { return i * ATOM + 4 * BLK * HS; }
-  static __device__ __forceinline__ int ons(int i) { return i * ATOM + 4 * BLK * HS + 5 * NB * 16; }
+  static __device__ __forceinline__ int ons(int i) { return i * ATOM + 4 * BLK * HS + 5 * NB * VS; }
 };
 
 // Issue the copies of group g into one stage (all lanes; no wait).
@@ -71,7 +81,7 @@ template <class L>
 __device__ __forceinline__ void issue(unsigned char *st, long g, const Meta &M, int lane,
                                       const typename L::HT *__restrict__ onsite,
                                       const typename L::HT *__restrict__ blocks,
-                                      const double2 *__restrict__ x) {
+                                      const typename L::VT *__restrict__ x) {
   constexpr int NB = L::NB;
 #pragma unroll
   for (int i = 0; i < kAPW; i++) {
@@ -100,11 +110,11 @@ __device__ __forceinline__ void issue(unsigned char *st, long g, const Meta &M, 
     unsigned char *xs = st + L::xs(i);
     // own segment in slot 4, neighbours in slots 0..3; one lane per chunk
     if (lane < L::X_CH) {
-      cp16(xs + 4 * NB * 16 + lane * 16, reinterpret_cast<const unsigned char *>(x + a * NB) + lane * 16);
+      cp16(xs + 4 * NB * L::VS + lane * 16, reinterpret_cast<const unsigned char *>(x + a * NB) + lane * 16);
 #pragma unroll
       for (int n = 0; n < 4; n++) {
         const int b = M.nb[i][n];
-        cp16z(xs + n * NB * 16 + lane * 16,
+        cp16z(xs + n * NB * L::VS + lane * 16,
               reinterpret_cast<const unsigned char *>(x + long(b >= 0 ? b : a) * NB) + lane * 16,
               b >= 0 ? 16 : 0);
       }
@@ -115,21 +125,24 @@ __device__ __forceinline__ void issue(unsigned char *st, long g, const Meta &M, 
   }
 }
 
-template <int NSPIN, bool DOT, int WARPS, int STAGES, typename HT = double>
+template <int NSPIN, bool DOT, int WARPS, int STAGES, typename HT = double,
+          typename VT = double2>
 __global__ void __launch_bounds__(WARPS * 32, 1)
     k_spmv_async(long ngroups, const int2 *__restrict__ groups, const int4 *__restrict__ nbr,
                  const unsigned char *__restrict__ site_m, const HT *__restrict__ onsite,
-                 const HT *__restrict__ blocks, const double2 *__restrict__ x,
-                 double2 *__restrict__ y, double shift, const double *__restrict__ xnorm,
+                 const HT *__restrict__ blocks, const VT *__restrict__ x,
+                 VT *__restrict__ y, double shift_d, const double *__restrict__ xnorm,
                  int xnorm_idx, double *partial, unsigned int *counter, double *alpha_out,
                  int alpha_idx) {
-  using L = Layout<NSPIN, WARPS, STAGES, HT>;
+  using L = Layout<NSPIN, WARPS, STAGES, HT, VT>;
+  using RT = typename L::RT;
   constexpr int NB = L::NB;
   extern __shared__ __align__(128) unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   unsigned char *wbase = smem + warp * L::WARP;
   const int ai = lane / kNorb, o = lane - ai * kNorb;
-  const double scale = xnorm ? 1.0 / xnorm[xnorm_idx] : 1.0;
+  const RT scale = RT(xnorm ? 1.0 / xnorm[xnorm_idx] : 1.0);
+  const RT shift = RT(shift_d);
   double dot = 0.0;
   const long nw = long(gridDim.x) * WARPS;
   long g = long(blockIdx.x) * WARPS + warp;
@@ -162,21 +175,22 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
     if (ai < kAPW && m >= 0) {
       const bool cat = m < 4;
       const long a = long(cur.a0) + ai;
-      const double2 *xs = reinterpret_cast<const double2 *>(st + L::xs(ai));
-      const double2 *X0 = xs + 4 * NB;
+      const VT *xs = reinterpret_cast<const VT *>(st + L::xs(ai));
+      const VT *X0 = xs + 4 * NB;
       const HT *rec = reinterpret_cast<const HT *>(st + L::ons(ai));
       const HT *bk = reinterpret_cast<const HT *>(st + L::blk(ai));
-      double2 acc[NSPIN];
+      VT acc[NSPIN];
 #pragma unroll
       for (int sp = 0; sp < NSPIN; sp++) {
-        const double2 v = X0[sp * kNorb + o];
-        const double dg = rec[sp * kNorb + o];
-        acc[sp] = make_double2(dg * v.x, dg * v.y);
+        const VT v = X0[sp * kNorb + o];
+        const RT dg = rec[sp * kNorb + o];
+        acc[sp].x = dg * v.x;
+        acc[sp].y = dg * v.y;
       }
       if (o >= 1 && o <= 4 && rec[NB + 1] != HT(0)) {  // dangling-bond sp3 couplings
-        const double sx = rec[NB + 2], sy = rec[NB + 3], sz = rec[NB + 4];
-        const double cxy = rec[NB + 5], cxz = rec[NB + 6], cyz = rec[NB + 7];
-        double c1, c2, c3;
+        const RT sx = rec[NB + 2], sy = rec[NB + 3], sz = rec[NB + 4];
+        const RT cxy = rec[NB + 5], cxz = rec[NB + 6], cyz = rec[NB + 7];
+        RT c1, c2, c3;
         int k1, k2, k3;
         if (o == 1) { c1 = sx; k1 = 2; c2 = sy; k2 = 3; c3 = sz; k3 = 4; }
         else if (o == 2) { c1 = sx; k1 = 1; c2 = cxy; k2 = 3; c3 = cxz; k3 = 4; }
@@ -190,8 +204,8 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
         }
       }
       if (NSPIN == 2 && o >= 2 && o <= 4) {  // on-site spin-orbit (mb_ham_spds_so.h)
-        const double Lm = rec[NB];
-        const double2 *U = X0, *D = X0 + kNorb;
+        const RT Lm = rec[NB];
+        const VT *U = X0, *D = X0 + kNorb;
         if (o == 2) {
           cfma_i(acc[0], -Lm, U[3]); cfma_r(acc[0], Lm, D[4]);
           cfma_i(acc[NSPIN - 1], Lm, D[3]); cfma_r(acc[NSPIN - 1], -Lm, U[4]);
@@ -207,11 +221,11 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
       // consecutive FMAs feed independent chains; the lane's block element
       // (o, k) is row o of a cation's own block or column o of the block an
       // anion reads from its cation neighbour
-      double2 part[4][NSPIN];
+      VT part[4][NSPIN];
 #pragma unroll
       for (int n = 0; n < 4; n++)
 #pragma unroll
-        for (int sp = 0; sp < NSPIN; sp++) part[n][sp] = make_double2(0.0, 0.0);
+        for (int sp = 0; sp < NSPIN; sp++) part[n][sp].x = part[n][sp].y = RT(0);
       const HT *Mb = bk + (cat ? o * kNorb : o);
       const int bstride = cat ? 1 : kNorb;
 #pragma unroll
@@ -219,25 +233,25 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
 #pragma unroll
         for (int n = 0; n < 4; n++) {
           if (nbv[n] < 0) continue;
-          const double r = Mb[n * L::BLK + kk * bstride];
+          const RT r = Mb[n * L::BLK + kk * bstride];
 #pragma unroll
           for (int sp = 0; sp < NSPIN; sp++) cfma_r(part[n][sp], r, xs[n * NB + sp * kNorb + kk]);
         }
 #pragma unroll
       for (int sp = 0; sp < NSPIN; sp++) {
-        const double2 bsum = make_double2((part[0][sp].x + part[1][sp].x) + (part[2][sp].x + part[3][sp].x),
-                                          (part[0][sp].y + part[1][sp].y) + (part[2][sp].y + part[3][sp].y));
-        acc[sp].x += bsum.x;
-        acc[sp].y += bsum.y;
+        acc[sp].x += (part[0][sp].x + part[1][sp].x) + (part[2][sp].x + part[3][sp].x);
+        acc[sp].y += (part[0][sp].y + part[1][sp].y) + (part[2][sp].y + part[3][sp].y);
       }
 #pragma unroll
       for (int sp = 0; sp < NSPIN; sp++) {
-        const double2 xv = X0[sp * kNorb + o];
-        const double2 xo = make_double2(scale * xv.x, scale * xv.y);
-        const double2 out = make_double2(scale * acc[sp].x - shift * xo.x,
-                                         scale * acc[sp].y - shift * xo.y);
+        const VT xv = X0[sp * kNorb + o];
+        VT xo, out;
+        xo.x = scale * xv.x;
+        xo.y = scale * xv.y;
+        out.x = scale * acc[sp].x - shift * xo.x;
+        out.y = scale * acc[sp].y - shift * xo.y;
         y[a * NB + sp * kNorb + o] = out;
-        dot += xo.x * out.x + xo.y * out.y;
+        dot += double(xo.x) * double(out.x) + double(xo.y) * double(out.y);
       }
     }
     __syncwarp();  // stage k is free before the next iteration overwrites it
@@ -248,14 +262,14 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
   if (DOT) grid_reduce<WARPS * 32>(dot, partial, counter, alpha_out, alpha_idx, false);
 }
 
-template <int NSPIN, bool DOT, int WARPS, int STAGES, typename HT>
-int launch_async_t(Ctx &c, const double *x, double *y, double shift, const double *xnorm,
+template <int NSPIN, bool DOT, int WARPS, int STAGES, typename HT, typename VT = double2>
+int launch_async_t(Ctx &c, const void *x, void *y, double shift, const double *xnorm,
                    int xidx, double *alpha_out, int aidx, cudaStream_t s) {
-  using L = Layout<NSPIN, WARPS, STAGES, HT>;
+  using L = Layout<NSPIN, WARPS, STAGES, HT, VT>;
   static int sms = 0;
   if (!sms) {
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device);
-    if (cudaFuncSetAttribute(k_spmv_async<NSPIN, DOT, WARPS, STAGES, HT>,
+    if (cudaFuncSetAttribute(k_spmv_async<NSPIN, DOT, WARPS, STAGES, HT, VT>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM) != cudaSuccess)
       return set_error(TBGPU_E_CUDA);
   }
@@ -264,9 +278,9 @@ int launch_async_t(Ctx &c, const double *x, double *y, double shift, const doubl
     int rc = ensure_partials(c, int(grid));
     if (rc) return rc;
   }
-  k_spmv_async<NSPIN, DOT, WARPS, STAGES, HT><<<grid, WARPS * 32, L::SMEM, s>>>(
+  k_spmv_async<NSPIN, DOT, WARPS, STAGES, HT, VT><<<grid, WARPS * 32, L::SMEM, s>>>(
       c.ngroups, c.d_groups, c.d_nbr, c.d_site_m, ham_onsite<HT>(c), ham_blocks<HT>(c),
-      reinterpret_cast<const double2 *>(x), reinterpret_cast<double2 *>(y), shift, xnorm, xidx,
+      reinterpret_cast<const VT *>(x), reinterpret_cast<VT *>(y), shift, xnorm, xidx,
       DOT ? c.d_partial : nullptr, DOT ? c.d_counter : nullptr, alpha_out, aidx);
   TB_CUDA(cudaGetLastError());
   return TBGPU_OK;
@@ -284,6 +298,21 @@ int launch_cfg(Ctx &c, const double *x, double *y, double shift, const double *x
   return alpha_out
              ? launch_async_t<1, true, WARPS, STAGES, HT>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s)
              : launch_async_t<1, false, WARPS, STAGES, HT>(c, x, y, shift, xnorm, xidx, nullptr, 0, s);
+}
+
+// complex-float vectors over the single-precision store, float accumulation
+// (the mixed-precision Lanczos); alpha is still reduced in double
+int launch_spmv_async_f32(Ctx &c, const float *x, float *y, double shift, const double *xnorm,
+                          int xidx, double *alpha_out, int aidx, cudaStream_t s) {
+  if (c.norb != kNorb || !c.ham_fp32) return set_error(TBGPU_E_UNSUPPORTED);
+  constexpr int W = kWarpsF32;
+  if (c.nspin == 2)
+    return alpha_out
+               ? launch_async_t<2, true, W, 1, float, float2>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s)
+               : launch_async_t<2, false, W, 1, float, float2>(c, x, y, shift, xnorm, xidx, nullptr, 0, s);
+  return alpha_out
+             ? launch_async_t<1, true, W, 1, float, float2>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s)
+             : launch_async_t<1, false, W, 1, float, float2>(c, x, y, shift, xnorm, xidx, nullptr, 0, s);
 }
 
 int launch_spmv_async(Ctx &c, const double *x, double *y, double shift, const double *xnorm,

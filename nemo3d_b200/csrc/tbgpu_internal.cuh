@@ -75,6 +75,12 @@ struct Ctx {
   // warp, padded with -1 (rc_cat_warps warps of cations, rc_warps in all)
   int *d_rc_order = nullptr;
   long rc_cat_warps = 0, rc_warps = 0;
+  // mixed-precision Lanczos: complex-float vectors over the single-precision
+  // store, then a double-precision Rayleigh-Ritz refinement of the Ritz
+  // vectors through the recompute product (the double on-site records and
+  // the recompute work order are kept for it)
+  bool lanczos_f32 = false;
+  std::vector<double> state_resid, state_delta;  // per state of the last solve
   float *d_onsite32 = nullptr;
   float *d_blocks32 = nullptr;
   // H*x work order: groups of up to 3 consecutive atoms of one k-pencil of
@@ -144,6 +150,9 @@ int launch_spmv(Ctx &c, const double *x, double *y, double shift,
 int launch_spmv_async(Ctx &c, const double *x, double *y, double shift,
                       const double *xscale_dev, int scale_index, double *alpha_out,
                       int alpha_index, cudaStream_t s);
+int launch_spmv_async_f32(Ctx &c, const float *x, float *y, double shift,
+                          const double *xscale_dev, int scale_index, double *alpha_out,
+                          int alpha_index, cudaStream_t s);
 // caller-provided reduction scratch (noalloc.cu)
 int launch_spmv_scratch(Ctx &c, const double *x, double *y, double shift, double *partial,
                         unsigned int *counter, int cap, double *dot_out, cudaStream_t s);
@@ -158,5 +167,8 @@ struct SolveArgs {
 };
 int solve(Ctx &c, const SolveArgs &A, const double *r0_dev, double *values, int *conv_iters,
           int *iterations, double *V_dev, int maxvec);
+// blk_lanczos.cu: double-precision Rayleigh-Ritz of nvec eigenvectors
+int refine_ritz(Ctx &c, double *V_dev, int nvec, double *values, std::vector<double> &resid,
+                std::vector<double> &delta, cudaStream_t s);
 
 }  // namespace tbgpu

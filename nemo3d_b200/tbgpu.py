@@ -48,7 +48,7 @@ class Stats(C.Structure):
     _fields_ = [("build_ms", C.c_double), ("solve_ms", C.c_double),
                 ("vectors_ms", C.c_double), ("spmv_ms", C.c_double),
                 ("spmv_launches", C.c_long), ("lanczos_iterations", C.c_long),
-                ("kernel_launches", C.c_long)]
+                ("kernel_launches", C.c_long), ("refine_ms", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -71,6 +71,9 @@ def _lib():
         L.tbgpu_set_bloch_k.argtypes = [vp, C.POINTER(C.c_double)]
         L.tbgpu_set_ham_precision.argtypes = [vp, ip]
         L.tbgpu_set_ham_storage.argtypes = [vp, ip]
+        L.tbgpu_set_lanczos_precision.argtypes = [vp, ip]
+        L.tbgpu_get_state_errors.argtypes = [vp, ip, vp, vp]
+        L.tbgpu_hx_dev_f32.argtypes = [vp, dp, vp, vp]
         L.tbgpu_write_eigenvalues.argtypes = [C.c_char_p, C.c_char, vp, ip, vp]
         L.tbgpu_write_eigenvector.argtypes = [vp, C.c_char_p, vp, ip]
         L.tbgpu_hx_block_dev.argtypes = [vp, ip, dp, vp, vp]
@@ -146,12 +149,15 @@ class Hamiltonian:
 
     ``structure``: a ``workloads.Structure``; ``model``: one of
     ``materials.BAND_MODELS``; ``materials``: parameter sets (default: every
-    shipped set of the model's family).
+    shipped set of the model's family).  ``ham_bits=32``: single-precision
+    store; ``recompute=True``: blocks recomputed in every H*x;
+    ``lanczos_bits=32`` (with ``ham_bits=32``): mixed-precision Lanczos with
+    a double-precision refinement of the returned eigenpairs.
     """
 
     def __init__(self, structure, model="sp3d5s*_so", materials=None, include_strain=True,
                  passivate=True, dangling_shift=30.0, device_inputs=None, build=True,
-                 ham_bits=64, recompute=False):
+                 ham_bits=64, recompute=False, lanczos_bits=64):
         L = _lib()
         self.structure = structure
         self.model = model
@@ -185,18 +191,26 @@ class Hamiltonian:
             raise TbgpuError(rc, "tbgpu_ctx_create")
         self._ctx = ctx
         self._built = False
+        # a failed option or build releases the context here, once (close()
+        # clears the handle, so the destructor does not release it again)
+        options = []
         if recompute:
-            rc = L.tbgpu_set_ham_storage(ctx, 1)
-            if rc:
-                L.tbgpu_ctx_destroy(ctx)
-                raise TbgpuError(rc, "tbgpu_set_ham_storage")
+            options.append(("tbgpu_set_ham_storage", 1))
         if ham_bits != 64:
-            rc = L.tbgpu_set_ham_precision(ctx, int(ham_bits))
+            options.append(("tbgpu_set_ham_precision", int(ham_bits)))
+        if lanczos_bits != 64:
+            options.append(("tbgpu_set_lanczos_precision", int(lanczos_bits)))
+        for name, value in options:
+            rc = getattr(L, name)(ctx, value)
             if rc:
-                L.tbgpu_ctx_destroy(ctx)
-                raise TbgpuError(rc, "tbgpu_set_ham_precision")
+                self.close()
+                raise TbgpuError(rc, name)
         if build:
-            self.build()
+            try:
+                self.build()
+            except TbgpuError:
+                self.close()
+                raise
 
     # -- lifecycle --------------------------------------------------------
     def close(self):
@@ -243,6 +257,13 @@ class Hamiltonian:
         rc = _lib().tbgpu_hx_dev(self._ctx, float(shift), C.c_void_p(x_ptr), C.c_void_p(y_ptr))
         if rc:
             raise TbgpuError(rc, "tbgpu_hx_dev")
+
+    def hx_dev_f32(self, x_ptr: int, y_ptr: int, shift: float = 0.0):
+        """Mixed-precision product on complex-float device vectors."""
+        rc = _lib().tbgpu_hx_dev_f32(self._ctx, float(shift), C.c_void_p(x_ptr),
+                                     C.c_void_p(y_ptr))
+        if rc:
+            raise TbgpuError(rc, "tbgpu_hx_dev_f32")
 
     def hx_block_dev(self, p: int, x_ptr: int, y_ptr: int, shift: float = 0.0):
         """Y_v = (H - shift) X_v for p device vectors stored back to back."""
@@ -380,6 +401,17 @@ class Hamiltonian:
 
     def set_profiling(self, on=True):
         _lib().tbgpu_set_profiling(self._ctx, int(bool(on)))
+
+    def state_errors(self):
+        """Mixed-precision solve: per state with an eigenvector, the residual
+        ||H v - lambda v|| of the refined pair and the change of the eigenvalue
+        made by the double-precision refinement."""
+        cap = 4096
+        r, d = np.zeros(cap), np.zeros(cap)
+        n = _lib().tbgpu_get_state_errors(self._ctx, cap, _p(r), _p(d))
+        if n < 0:
+            raise TbgpuError(n, "tbgpu_get_state_errors")
+        return r[:n].copy(), d[:n].copy()
 
     def stats(self) -> dict:
         s = Stats()
