@@ -318,6 +318,22 @@ int tbgpu_write_eigenvalues(const char *path, char mode, const double *k, int n,
 int tbgpu_write_eigenvector(const tbgpu_ctx *ctx, const char *path,
                             const tbgpu_dcomplex *wf, int crystal_structure);
 
+/* Momentum (optical) matrix elements of n eigenstates psi_dev ([n][dimension]
+ * complex, device) and their Kramers partners, for x, y and z: the
+ * reference's MOMENTUM_MATRIX block (nemo3d/src/base/eigsys3d_par.c:410-640,
+ * COMPUTE_Px/Py/Pz), p = i(<a|H r b> - <a|r H b>) with r the strained atom
+ * coordinate (nm) and (a, b) = (psi_i, psi_f), (psi_i, psi'_f), (psi'_i,
+ * psi_f), (psi'_i, psi'_f), psi' = (-conj(psi_down), conj(psi_up)).
+ * P (host, or NULL): [3][n][8n] complex in the reference's pXmatrix layout,
+ * entry [d][i][8f + 2c] = label (+-(i+1), +-(f+1)), a minus sign marking
+ * the partner, [8f + 2c + 1] = p.  trans (host, or NULL; needs E, the n
+ * eigenvalues): [3][n(n-1)/2][4] = (istate, fstate, E_i - E_f, sum of |p|^2
+ * over the four pairs) for istate > fstate, fstate outer (TransProbX).
+ * Spin models only, at the Gamma point (else TBGPU_E_UNSUPPORTED); 2n H*x
+ * products and one fused pass over the vectors. */
+int tbgpu_momentum_matrix(tbgpu_ctx *ctx, int n, const double *psi_dev, const double *E,
+                          double *P, double *trans);
+
 /* Timing of the last solve / build (ms, CUDA events on the context stream). */
 typedef struct {
   double build_ms;            /* topology + assembly                          */

@@ -74,6 +74,7 @@ def _lib():
         L.tbgpu_set_lanczos_precision.argtypes = [vp, ip]
         L.tbgpu_get_state_errors.argtypes = [vp, ip, vp, vp]
         L.tbgpu_hx_dev_f32.argtypes = [vp, dp, vp, vp]
+        L.tbgpu_momentum_matrix.argtypes = [vp, ip, vp, vp, vp, vp]
         L.tbgpu_write_eigenvalues.argtypes = [C.c_char_p, C.c_char, vp, ip, vp]
         L.tbgpu_write_eigenvector.argtypes = [vp, C.c_char_p, vp, ip]
         L.tbgpu_hx_block_dev.argtypes = [vp, ip, dp, vp, vp]
@@ -401,6 +402,29 @@ class Hamiltonian:
 
     def set_profiling(self, on=True):
         _lib().tbgpu_set_profiling(self._ctx, int(bool(on)))
+
+    def momentum_matrix(self, psi, E=None):
+        """Optical momentum matrix elements of the states ``psi`` (complex
+        [n, dimension], host or a CUDA tensor of 2*n*dimension doubles):
+        returns P [3, n, 8n] complex in the reference's pXmatrix layout and,
+        with eigenvalues ``E``, the transition table [3, n(n-1)/2, 4]."""
+        import torch
+        if isinstance(psi, torch.Tensor) and psi.is_cuda:
+            dev = psi.contiguous()
+            n = dev.numel() // (2 * self.n)
+        else:
+            a = np.asarray(psi, complex).reshape(-1, self.n)
+            n = a.shape[0]
+            dev = torch.from_numpy(np.stack([a.real, a.imag], -1).reshape(-1).copy()).cuda()
+        P = np.zeros((3, n, 8 * n, 2))
+        T = np.zeros((3, max(n * (n - 1) // 2, 1), 4)) if E is not None else None
+        e = np.ascontiguousarray(E, np.float64) if E is not None else None
+        rc = _lib().tbgpu_momentum_matrix(self._ctx, n, C.c_void_p(dev.data_ptr()), _p(e),
+                                          _p(P), _p(T))
+        if rc:
+            raise TbgpuError(rc, "tbgpu_momentum_matrix")
+        P = P[..., 0] + 1j * P[..., 1]
+        return (P, T[:, :n * (n - 1) // 2] if T is not None else None)
 
     def state_errors(self):
         """Mixed-precision solve: per state with an eigenvector, the residual

@@ -324,3 +324,61 @@ def block_lanczos(hx, r0_block, imax=400, req=(1, 1), erange1=(-1, 0), erange2=(
             break
     return dict(evals=np.sort(np.array(conv1 + conv2)), found_vb=len(conv1),
                 found_cb=len(conv2), iterations=it)
+
+
+def kramers_partner(v, norb):
+    """Time-reversal partner of a spin state as eigsys3d_par.c:461-475 writes
+    it: up <- -conj(down), down <- conj(up), per atom."""
+    v = np.asarray(v, complex).reshape(-1, 2 * norb)
+    w = np.empty_like(v)
+    w[:, norb:] = np.conj(v[:, :norb])
+    w[:, :norb] = -np.conj(v[:, norb:])
+    return w.reshape(-1)
+
+
+def momentum_matrix(o, psi, E=None):
+    """Momentum (optical) matrix elements, literally as the reference's
+    MOMENTUM_MATRIX block computes them (eigsys3d_par.c:410-640, the same code
+    for Px, Py, Pz): for final state f, H psi_f, H psi'_f, x H psi, x H psi',
+    x psi, x psi', H x psi, H x psi' (psi' the Kramers partner, x the strained
+    atom coordinate); for initial state i, temp1 = <a|x H b>, temp2 = <a|H x b>
+    and p = i (temp2 - temp1) for (a, b) in (psi_i, psi_f), (psi_i, psi'_f),
+    (psi'_i, psi_f), (psi'_i, psi'_f).  Returns P [3][n][8n] complex in the
+    pXmatrix layout (labels (+-(i+1), +-(f+1)) before each value) and, when E
+    is given, the transition table [3][n(n-1)/2][4] (istate, fstate,
+    E_i - E_f, sum of |p|^2 over the four pairs) for istate > fstate in the
+    order the reference fills TransProbX (fstate outer)."""
+    psi = [np.asarray(p, complex).reshape(-1) for p in psi]
+    n, nb, norb = len(psi), o.nb, o.norb
+    pos = o.st.site_positions().reshape(-1, 3)[o.atom_slot]
+    if o.st.dsp is not None:
+        pos = pos + np.asarray(o.st.dsp, np.float64).reshape(-1, 3)[o.atom_slot]
+
+    def H(v):
+        x = np.stack([v.real, v.imag], -1).reshape(-1)
+        y = o.hx(x).reshape(-1, 2)
+        return y[:, 0] + 1j * y[:, 1]
+
+    P = np.zeros((3, n, 8 * n), complex)
+    T = np.zeros((3, n * (n - 1) // 2, 4)) if E is not None else None
+    for d in range(3):
+        r = np.repeat(pos[:, d], nb)
+        k = 0
+        for f in range(n):
+            bf = [psi[f], kramers_partner(psi[f], norb)]
+            Hb = [H(b) for b in bf]
+            xHb = [r * h for h in Hb]
+            Hxb = [H(r * b) for b in bf]
+            for i in range(n):
+                ai = [psi[i], kramers_partner(psi[i], norb)]
+                for c, (ia, fb) in enumerate(((0, 0), (0, 1), (1, 0), (1, 1))):
+                    t1 = np.vdot(ai[ia], xHb[fb])
+                    t2 = np.vdot(ai[ia], Hxb[fb])
+                    P[d, i, 8 * f + 2 * c] = complex((i + 1) * (-1 if ia else 1),
+                                                     (f + 1) * (-1 if fb else 1))
+                    P[d, i, 8 * f + 2 * c + 1] = complex(t1.imag - t2.imag, t2.real - t1.real)
+                if T is not None and i > f:
+                    vals = P[d, i, 8 * f + 1:8 * f + 8:2]
+                    T[d, k] = (i + 1, f + 1, E[i] - E[f], float(np.sum(np.abs(vals) ** 2)))
+                    k += 1
+    return P, T
