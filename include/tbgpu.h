@@ -318,6 +318,28 @@ int tbgpu_write_eigenvalues(const char *path, char mode, const double *k, int n,
 int tbgpu_write_eigenvector(const tbgpu_ctx *ctx, const char *path,
                             const tbgpu_dcomplex *wf, int crystal_structure);
 
+/* Keating valence-force-field strain (the reference's min_estrain with
+ * StrainModel = VFF_keating: calc_estrain, nemo3d/src/base/strain3d.c:
+ * 1361-2080, minimised by macoptII_par, NEMO_3D/eigen/src/macopt_par.c:
+ * 121-475).  Both act on a context before tbgpu_build_hamiltonian
+ * (TBGPU_E_STATE after it).  vff: [nspecies][nspecies][3] = (a0 nm, alpha,
+ * beta) per species pair, symmetric (the reference's amat, alpha, beta); a
+ * pair present in the structure with a0 <= 0 is TBGPU_E_MATERIAL.
+ * Displacements are per site, [nx*ny*nz*8][3] nm like tbgpu_geom.dsp.
+ * tbgpu_vff_energy: the energy at the context's displacements (zero when it
+ * has none) and, if grad is not NULL, the reference's gradient dp (the
+ * bond-stretching term counted from each bond's atoms for the energy, moving
+ * only the vertex atom in the gradient).  tbgpu_vff_relax: macopt from the
+ * context's displacements with the reference's boundary conditions bc
+ * (0 AllFree, 1 FixOne, 2 FixSurfaceAll, 3 FixZmin, 4 FixInterior), stopping
+ * when the mean step (end_if_small_step = 1, ConvCrit = Step) or the squared
+ * gradient norm (0) falls to tol, or after max_iter iterations; the relaxed
+ * displacements replace the context's (the build then uses them) and are
+ * copied to dsp if it is not NULL; *energy at the result, *iterations. */
+int tbgpu_vff_energy(tbgpu_ctx *ctx, const double *vff, double *energy, double *grad);
+int tbgpu_vff_relax(tbgpu_ctx *ctx, const double *vff, int bc, int max_iter, double tol,
+                    int end_if_small_step, double *energy, int *iterations, double *dsp);
+
 /* Momentum (optical) matrix elements of n eigenstates psi_dev ([n][dimension]
  * complex, device) and their Kramers partners, for x, y and z: the
  * reference's MOMENTUM_MATRIX block (nemo3d/src/base/eigsys3d_par.c:410-640,

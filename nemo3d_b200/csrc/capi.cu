@@ -142,7 +142,11 @@ int tbgpu_build_hamiltonian(tbgpu_ctx *ctx) {
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   cudaEventRecord(e0, c.stream);
-  int rc = build_topology(c);
+  int rc = TBGPU_OK;
+  if (!c.topo_built) {
+    rc = build_topology(c);
+    if (rc == TBGPU_OK) c.topo_built = true;
+  }
   if (rc == TBGPU_OK) rc = assemble(c);
   if (rc == TBGPU_OK) rc = ensure_partials(c, int(c.natoms / 8 + 65536));
   cudaEventRecord(e1, c.stream);

@@ -51,6 +51,7 @@ struct Ctx {
   long nsites = 0;
   long natoms = 0;
   bool built = false;
+  bool topo_built = false;  // topology done (by the build or a strain relaxation)
   int device = 0;
   cudaStream_t stream = nullptr;
   bool own_stream = false;

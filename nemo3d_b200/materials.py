@@ -88,6 +88,28 @@ MATERIALS = {
 }
 
 
+# Keating valence-force-field constants per (cation, anion) compound: the
+# unstrained cubic cell length a0 (nm) and alpha, beta (the strain_alpha and
+# strain_beta entries of the same XML material blocks; strain3d.c reads them
+# through StrainParam::amat/alpha/beta).
+VFF = {
+    ("Ga", "As"): dict(a0=0.56532, alpha=41.49, beta=8.94, source="ioNemo3D.xml:658-673"),
+    ("In", "As"): dict(a0=0.60583, alpha=35.18, beta=5.49, source="ioNemo3D.xml:809-824"),
+    ("Si", "Si"): dict(a0=0.543095, alpha=48.5, beta=13.8, source="ioNemo3D.xml:1111-1126"),
+}
+
+
+def vff_table(pairs=None, nspecies=8):
+    """[nspecies, nspecies, 3] table (a0, alpha, beta) for the compounds in
+    ``pairs`` (default: all of ``VFF``), symmetric in the two species."""
+    import numpy as np
+    t = np.zeros((nspecies, nspecies, 3))
+    for (c, a) in (pairs or VFF):
+        v = VFF[(c, a)]
+        t[SPECIES[c], SPECIES[a]] = t[SPECIES[a], SPECIES[c]] = (v["a0"], v["alpha"], v["beta"])
+    return t
+
+
 def material_family(model: str) -> str:
     """Parameter family a band model draws on ("sp3s*" or "sp3d5s*")."""
     return SP3S if model.startswith("sp3s*") else SP3D5S

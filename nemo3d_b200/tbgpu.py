@@ -75,6 +75,8 @@ def _lib():
         L.tbgpu_get_state_errors.argtypes = [vp, ip, vp, vp]
         L.tbgpu_hx_dev_f32.argtypes = [vp, dp, vp, vp]
         L.tbgpu_momentum_matrix.argtypes = [vp, ip, vp, vp, vp, vp]
+        L.tbgpu_vff_energy.argtypes = [vp, vp, vp, vp]
+        L.tbgpu_vff_relax.argtypes = [vp, vp, ip, ip, dp, ip, vp, vp, vp]
         L.tbgpu_write_eigenvalues.argtypes = [C.c_char_p, C.c_char, vp, ip, vp]
         L.tbgpu_write_eigenvector.argtypes = [vp, C.c_char_p, vp, ip]
         L.tbgpu_hx_block_dev.argtypes = [vp, ip, dp, vp, vp]
@@ -402,6 +404,36 @@ class Hamiltonian:
 
     def set_profiling(self, on=True):
         _lib().tbgpu_set_profiling(self._ctx, int(bool(on)))
+
+    # -- Keating strain (before build) ---------------------------------------
+    def vff_energy(self, vff=None, grad=False):
+        """Keating energy at the current displacements and, with ``grad``,
+        the reference's gradient per site ([nx, ny, nz, 8, 3])."""
+        t = np.ascontiguousarray(_mat.vff_table() if vff is None else vff, np.float64)
+        e = np.zeros(1)
+        g = np.zeros(self.structure.nsites * 3) if grad else None
+        rc = _lib().tbgpu_vff_energy(self._ctx, _p(t), _p(e), _p(g))
+        if rc:
+            raise TbgpuError(rc, "tbgpu_vff_energy")
+        if grad:
+            st = self.structure
+            return float(e[0]), g.reshape(st.nx, st.ny, st.nz, 8, 3)
+        return float(e[0])
+
+    def vff_relax(self, vff=None, bc=0, max_iter=10000, tol=1e-9, end_if_small_step=1):
+        """Relax the displacements with the Keating model (macopt); returns
+        (displacements [nx, ny, nz, 8, 3], energy, iterations).  The build
+        that follows uses the relaxed displacements."""
+        t = np.ascontiguousarray(_mat.vff_table() if vff is None else vff, np.float64)
+        st = self.structure
+        d = np.zeros(st.nsites * 3)
+        e = np.zeros(1)
+        its = np.zeros(1, np.int32)
+        rc = _lib().tbgpu_vff_relax(self._ctx, _p(t), int(bc), int(max_iter), float(tol),
+                                    int(end_if_small_step), _p(e), _p(its), _p(d))
+        if rc:
+            raise TbgpuError(rc, "tbgpu_vff_relax")
+        return d.reshape(st.nx, st.ny, st.nz, 8, 3), float(e[0]), int(its[0])
 
     def momentum_matrix(self, psi, E=None):
         """Optical momentum matrix elements of the states ``psi`` (complex

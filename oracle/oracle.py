@@ -82,6 +82,14 @@ def lib():
         L.orc_onsite_block.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
         L.orc_bond.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                                C.c_int, C.c_double, C.c_void_p, C.c_void_p]
+        L.orc_vff_energy.restype = C.c_double
+        L.orc_vff_energy.argtypes = [C.POINTER(_Geom), C.c_long, C.c_void_p, C.c_void_p,
+                                     C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_vff_free_mask.argtypes = [C.POINTER(_Geom), C.c_long, C.c_void_p, C.c_void_p,
+                                        C.c_int, C.c_void_p]
+        L.orc_vff_relax.argtypes = [C.POINTER(_Geom), C.c_long, C.c_void_p, C.c_void_p,
+                                    C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int,
+                                    C.c_double, C.c_int, C.c_void_p, C.c_void_p]
     return _lib
 
 
@@ -382,3 +390,64 @@ def momentum_matrix(o, psi, E=None):
                     T[d, k] = (i + 1, f + 1, E[i] - E[f], float(np.sum(np.abs(vals) ** 2)))
                     k += 1
     return P, T
+
+
+class OracleVFF:
+    """Keating valence-force-field strain of a structure (the reference's
+    min_estrain with StrainModel = VFF_keating; see tb_oracle.h).
+    ``vff``: [ns, ns, 3] (a0 nm, alpha, beta) per species pair.  Displacements
+    are per atom ([natoms, 3], nm) or, through ``to_sites``, per site as
+    ``Structure.dsp``."""
+
+    def __init__(self, st, vff):
+        self.st = st
+        self.vff = np.ascontiguousarray(vff, np.float64)
+        self.ns = self.vff.shape[0]
+        self.types = np.ascontiguousarray(st.types, dtype=np.uint8).reshape(-1)
+        g = _Geom()
+        g.nx, g.ny, g.nz = st.nx, st.ny, st.nz
+        g.periodic[:] = [int(bool(x)) for x in st.periodic]
+        g.lattice[:] = list(st.lattice)
+        g.type = _p(self.types)
+        g.dsp = None
+        self._g = g
+        ns = st.nsites
+        slot = np.zeros(ns, np.int32)
+        nbr = np.zeros(ns * 4, np.int32)
+        wrap = np.zeros(ns * 12, np.int8)
+        surf = np.zeros(ns, np.uint8)
+        na = int(lib().orc_topology(C.byref(g), ns, _p(slot), _p(nbr), _p(wrap), _p(surf)))
+        self.natoms = na
+        self.atom_slot, self.nbr, self.surface = slot[:na].copy(), nbr[:na * 4].copy(), surf[:na].copy()
+
+    def from_sites(self, dsp):
+        if dsp is None:
+            return np.zeros((self.natoms, 3))
+        return np.asarray(dsp, np.float64).reshape(-1, 3)[self.atom_slot].copy()
+
+    def to_sites(self, u):
+        out = np.zeros((self.st.nsites, 3))
+        out[self.atom_slot] = np.asarray(u).reshape(-1, 3)
+        return out.reshape(self.st.nx, self.st.ny, self.st.nz, 8, 3)
+
+    def energy(self, u):
+        u = np.ascontiguousarray(u, np.float64).reshape(-1)
+        grad = np.zeros_like(u)
+        e = lib().orc_vff_energy(C.byref(self._g), self.natoms, _p(self.atom_slot), _p(self.nbr),
+                                 self.ns, _p(self.vff), _p(u), _p(grad))
+        return float(e), grad.reshape(-1, 3)
+
+    def free_mask(self, bc):
+        m = np.zeros(self.natoms, np.uint8)
+        lib().orc_vff_free_mask(C.byref(self._g), self.natoms, _p(self.atom_slot),
+                                _p(self.surface), int(bc), _p(m))
+        return m.astype(bool)
+
+    def relax(self, u0=None, bc=0, itmax=10000, tol=1e-9, end_if_small_step=1):
+        u = np.ascontiguousarray(np.zeros((self.natoms, 3)) if u0 is None else u0,
+                                 np.float64).reshape(-1).copy()
+        e = np.zeros(1)
+        its = lib().orc_vff_relax(C.byref(self._g), self.natoms, _p(self.atom_slot), _p(self.nbr),
+                                  _p(self.surface), self.ns, _p(self.vff), int(bc), int(itmax),
+                                  float(tol), int(end_if_small_step), _p(u), _p(e))
+        return u.reshape(-1, 3), float(e[0]), int(its)

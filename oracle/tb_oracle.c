@@ -881,3 +881,234 @@ int orc_eigensolve_lanczos(orc_matvec_fn mv, void *ctx, long n, const double *r0
   free(r); free(q); free(qp); free(c1); free(c2); free(i1); free(i2);
   return ne;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Keating valence force field, StrainModel = VFF_keating (no anharmonic
+ * corrections, no lattice-constant minimisation).
+ *
+ * calc_estrain (base/strain3d.c:1361-2080): for every atom m and its
+ * neighbours n, p (all present), nnv = a_latt*eta + (u_nbr - u_m) with eta
+ * the neighbour's cell offset plus the in-cell position difference, nnv0 =
+ * alat(m, n)*eta.  Bond stretching 0.5*alpha/d0^2*(d^2 - d0^2)^2 per atom and
+ * bond (each bond thus counted from both ends), bond bending
+ * sqrt(beta_n beta_p)/sqrt(d0_p^2 d0_n^2)*(nnv_n.nnv_p - nnv0_n.nnv0_p)^2 per
+ * atom and neighbour pair; the gradient as the reference accumulates it. */
+double orc_vff_energy(const orc_geom *g, long natoms, const int *atom_slot, const int *nbr,
+                      int ns, const double *vff, const double *u, double *grad) {
+  double bld = 0.0, bbd = 0.0;
+  long a;
+  int n, p, q;
+  memset(grad, 0, sizeof(double) * 3 * natoms);
+  for (a = 0; a < natoms; a++) {
+    const long s = atom_slot[a];
+    const int m = (int)(s % 8);
+    const int tm = g->type[s];
+    double nnv[4][3], nnv0[4][3], alpha[4], beta[4];
+    int stat[4], nb[4];
+    for (n = 0; n < 4; n++) {
+      nb[n] = nbr[a * 4 + n];
+      stat[n] = nb[n] >= 0;
+      if (!stat[n]) continue;
+      const long sn = atom_slot[nb[n]];
+      const int tn = g->type[sn];
+      const int mn = nnmap[m][n][3];
+      const double *vp = vff + ((long)tm * ns + tn) * 3;
+      const double alat = vp[0];
+      for (q = 0; q < 3; q++) {
+        const double disp = u[nb[n] * 3 + q] - u[a * 3 + q];
+        const double r1 = (double)nnmap[m][n][q] + (pin[mn][q] - pin[m][q]);
+        nnv[n][q] = g->lattice[q] * r1 + disp;
+        nnv0[n][q] = alat * r1;
+      }
+      alpha[n] = vp[1];
+      beta[n] = vp[2];
+    }
+    for (n = 0; n < 4; n++) {
+      if (!stat[n]) continue;
+      const double dssq = nnv[n][0] * nnv[n][0] + nnv[n][1] * nnv[n][1] + nnv[n][2] * nnv[n][2];
+      const double d0sq =
+          nnv0[n][0] * nnv0[n][0] + nnv0[n][1] * nnv0[n][1] + nnv0[n][2] * nnv0[n][2];
+      const double bldc = 0.5 * alpha[n] / d0sq;
+      const double bldl = dssq - d0sq;
+      bld += bldc * bldl * bldl;
+      const double r1 = 4 * bldc * bldl;
+      for (q = 0; q < 3; q++) grad[a * 3 + q] -= r1 * nnv[n][q];
+      for (p = n + 1; p < 4; p++) {
+        if (!stat[p]) continue;
+        const double d0dot =
+            nnv0[n][0] * nnv0[p][0] + nnv0[n][1] * nnv0[p][1] + nnv0[n][2] * nnv0[p][2];
+        const double dsdot = nnv[n][0] * nnv[p][0] + nnv[n][1] * nnv[p][1] + nnv[n][2] * nnv[p][2];
+        const double den =
+            nnv0[p][0] * nnv0[p][0] + nnv0[p][1] * nnv0[p][1] + nnv0[p][2] * nnv0[p][2];
+        const double Beta = sqrt(beta[n] * beta[p]);
+        const double bbdc = Beta / sqrt(den * d0sq);
+        const double bbdl = dsdot - d0dot;
+        const double bb_mul = bbdc * bbdl;
+        bbd += bb_mul * bbdl;
+        const double bb2 = 2 * bb_mul;
+        for (q = 0; q < 3; q++) {
+          grad[nb[n] * 3 + q] += nnv[p][q] * bb2;
+          grad[a * 3 + q] -= nnv[p][q] * bb2;
+        }
+        for (q = 0; q < 3; q++) {
+          grad[nb[p] * 3 + q] += nnv[n][q] * bb2;
+          grad[a * 3 + q] -= nnv[n][q] * bb2;
+        }
+      }
+    }
+  }
+  return bld + bbd;
+}
+
+/* Which atoms move under the reference's Keating boundary conditions
+ * (calc_estrain_macopt, base/strain3d.c:846-1000, 1242-1340): 0 AllFree,
+ * 1 FixOne (the first atom fixed), 2 FixSurfaceAll (surface atoms fixed),
+ * 3 FixZmin (atoms of the two lowest cell layers fixed, isInZ_min: bit 64 of
+ * FindSurfaceAtoms, geo_struct.c:1374-1410), 4 FixInterior (only surface
+ * atoms move). */
+void orc_vff_free_mask(const orc_geom *g, long natoms, const int *atom_slot,
+                       const unsigned char *surface, int bc, unsigned char *free_mask) {
+  long a;
+  for (a = 0; a < natoms; a++) {
+    const long cell = atom_slot[a] / 8;
+    const int k = (int)(cell % g->nz);
+    int f = 1;
+    if (bc == 1) f = a != 0;
+    else if (bc == 2) f = !surface[a];
+    else if (bc == 3) f = k > 1;
+    else if (bc == 4) f = surface[a] != 0;
+    free_mask[a] = (unsigned char)f;
+  }
+}
+
+/* macoptII_par / maclinminII_par / macprodII_par / macopt_restart
+ * (NEMO_3D/eigen/src/macopt_par.c:121-475, macopt.c:418-520) with the
+ * defaults of macopt_defaults (rich = 1, linmin g1 2.0, g2 1.25, g3 0.5,
+ * 20 line-search steps, lastx 0.01, grad_tol_tiny 1e-28, step_tol_tiny 0)
+ * driving the Keating gradient of the free atoms (calc_estrain_macopt).
+ * u: [natoms*3] displacements, updated in place.  Returns the iteration at
+ * which it stopped; *energy is the energy at the final u. */
+typedef struct {
+  const orc_geom *g;
+  long natoms;
+  const int *atom_slot, *nbr;
+  int ns;
+  const double *vff;
+  const unsigned char *free_mask;
+  double *tmp;
+  double value;
+} vff_ctx;
+
+static void vff_dfunc(vff_ctx *c, const double *u, double *xi) {
+  long i;
+  c->value = orc_vff_energy(c->g, c->natoms, c->atom_slot, c->nbr, c->ns, c->vff, u, c->tmp);
+  for (i = 0; i < 3 * c->natoms; i++) xi[i] = c->free_mask[i / 3] ? c->tmp[i] : 0.0;
+}
+
+int orc_vff_relax(const orc_geom *g, long natoms, const int *atom_slot, const int *nbr,
+                  const unsigned char *surface, int ns, const double *vff, int bc, int itmax,
+                  double tol, int end_if_small_step, double *u, double *energy) {
+  const long n = 3 * natoms;
+  double *gv = (double *)calloc(n, sizeof(double)), *h = (double *)calloc(n, sizeof(double));
+  double *xi = (double *)calloc(n, sizeof(double)), *pt = (double *)calloc(n, sizeof(double));
+  double *gx = (double *)calloc(n, sizeof(double)), *gy = (double *)calloc(n, sizeof(double));
+  unsigned char *fm = (unsigned char *)malloc(natoms);
+  vff_ctx c = {g, natoms, atom_slot, nbr, ns, vff, fm, (double *)calloc(n, sizeof(double)), 0.0};
+  const int end_if_small_grad = 1 - end_if_small_step;
+  int rich = 1, restart = 0, its;
+  double lastx = 0.01, gtyp = 0.0;
+  long j;
+  orc_vff_free_mask(g, natoms, atom_slot, surface, bc, fm);
+  vff_dfunc(&c, u, xi);
+  for (j = 0; j < n; j++) { /* macopt_restart(a, 1) */
+    gv[j] = -xi[j];
+    xi[j] = h[j] = gv[j];
+  }
+  for (its = 1; its <= itmax; ++its) {
+    double gg = 0.0;
+    for (j = 0; j < n; j++) gg += gv[j] * gv[j];
+    gtyp = sqrt(gg / (double)n);
+    if ((end_if_small_grad && gg <= tol) || gg <= 1e-28) break;
+    /* maclinmin */
+    double x = lastx / gtyp, y = 0.0, s, t, m, step = 0.0, *ga = gx, *gb = gy, *sw;
+    int lits = 1;
+#define MACPROD(yy, gout, res)                                   \
+    do {                                                         \
+      for (j = 0; j < n; j++) pt[j] = u[j] + (yy) * xi[j];       \
+      vff_dfunc(&c, pt, gout);                                   \
+      res = 0.0;                                                 \
+      for (j = 0; j < n; j++) res += gout[j] * xi[j];            \
+    } while (0)
+    MACPROD(x, ga, s);
+    if (s < 0) {
+      do {
+        y = x * 2.0;
+        MACPROD(y, gb, t);
+        if (t >= 0.0) break;
+        x = y; s = t; sw = ga; ga = gb; gb = sw;
+        ++lits;
+      } while (lits <= 20);
+    } else if (s > 0) {
+      do {
+        y = x * 0.5;
+        MACPROD(y, gb, t);
+        if (t <= 0.0) break;
+        x = y; s = t; sw = ga; ga = gb; gb = sw;
+        ++lits;
+      } while (lits <= 20);
+    } else {
+      t = 1.0;
+      y = x;
+    }
+    if (lits > 20) {
+      double tmpd;
+      MACPROD(0.0, gb, tmpd);
+      if (tmpd > 0 && rich == 0) rich = 1;
+      if (tmpd > 0) restart = 1;
+    }
+#undef MACPROD
+    if (s < 0.0) s = -s;
+    if (t < 0.0) t = -t;
+    m = s + t;
+    s /= m;
+    t /= m;
+    m = s * y + t * x;
+    for (j = 0; j < n; j++) {
+      const double tmpd = m * xi[j];
+      u[j] += tmpd;
+      step += fabs(tmpd);
+      xi[j] = s * gb[j] + t * ga[j];
+    }
+    lastx = m * 1.25 * gtyp;
+    step /= (double)n;
+    if (((end_if_small_step && step <= tol) || step <= 0.0) && restart == 0) break;
+    if (rich || restart) vff_dfunc(&c, u, xi);
+    if (restart) { /* macopt_restart(a, 0) */
+      lastx = 0.01;
+      for (j = 0; j < n; j++) {
+        if (restart != 2) gv[j] = -xi[j];
+        xi[j] = h[j] = gv[j];
+      }
+      restart = 0;
+    } else {
+      double dgg = 0.0, gam, tmpd = 0.0;
+      for (j = 0; j < n; j++) dgg += (xi[j] + gv[j]) * xi[j];
+      gam = dgg / gg;
+      for (j = 0; j < n; j++) {
+        gv[j] = -xi[j];
+        xi[j] = h[j] = gv[j] + gam * h[j];
+        tmpd -= xi[j] * gv[j];
+      }
+      if (tmpd > 0.0) {
+        rich = 1;
+        restart = 2;
+        lastx = 0.01;
+        for (j = 0; j < n; j++) xi[j] = h[j] = gv[j];
+        restart = 0;
+      }
+    }
+  }
+  *energy = orc_vff_energy(g, natoms, atom_slot, nbr, ns, vff, u, c.tmp);
+  free(gv); free(h); free(xi); free(pt); free(gx); free(gy); free(fm); free(c.tmp);
+  return its > itmax ? itmax : its;
+}

@@ -118,6 +118,22 @@ typedef struct {
 } orc_ham;
 void orc_ham_matvec(void *ham, const double *x, double *y);
 
+/* Keating VFF energy (StrainModel = VFF_keating, calc_estrain,
+ * base/strain3d.c:1361-2080) at displacements u[natoms*3] (nm, atom order);
+ * grad[natoms*3] = dE/du.  vff: [ns][ns][3] = (a0 nm, alpha, beta) per
+ * species pair. */
+double orc_vff_energy(const orc_geom *g, long natoms, const int *atom_slot, const int *nbr,
+                      int ns, const double *vff, const double *u, double *grad);
+/* Free atoms under boundary condition bc (0 AllFree, 1 FixOne,
+ * 2 FixSurfaceAll, 3 FixZmin, 4 FixInterior). */
+void orc_vff_free_mask(const orc_geom *g, long natoms, const int *atom_slot,
+                       const unsigned char *surface, int bc, unsigned char *free_mask);
+/* min_estrain with macoptII_par (eigen/src/macopt_par.c:121-475): u is
+ * relaxed in place; returns the iteration count, *energy at the result. */
+int orc_vff_relax(const orc_geom *g, long natoms, const int *atom_slot, const int *nbr,
+                  const unsigned char *surface, int ns, const double *vff, int bc, int itmax,
+                  double tol, int end_if_small_step, double *u, double *energy);
+
 #ifdef __cplusplus
 }
 #endif
