@@ -325,8 +325,10 @@ static int spmv_step(Ctx &c, const double2 *x, double2 *y, const double *bet, in
 }
 static int spmv_step(Ctx &c, const float2 *x, float2 *y, const double *bet, int it,
                      double *alpha, cudaStream_t s) {
-  return launch_spmv_async_f32(c, reinterpret_cast<const float *>(x), reinterpret_cast<float *>(y),
-                               0.0, bet, it, alpha, it, s);
+  const float *X = reinterpret_cast<const float *>(x);
+  float *Y = reinterpret_cast<float *>(y);
+  if (c.recompute) return launch_spmv_recompute_f32(c, X, Y, 0.0, bet, it, alpha, it, s);
+  return launch_spmv_async_f32(c, X, Y, 0.0, bet, it, alpha, it, s);
 }
 
 template <typename VT>

@@ -37,31 +37,42 @@ __host__ __device__ constexpr int rc_min_blocks(int norb, int nspin) {
   return norb == 10 && nspin == 2 ? 3 : 4;
 }
 
-__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
-  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+template <typename V>
+__device__ __forceinline__ V cmul(double2 a, V b) {
+  using T = decltype(b.x);
+  V r;
+  r.x = T(a.x) * b.x - T(a.y) * b.y;
+  r.y = T(a.x) * b.y + T(a.y) * b.x;
+  return r;
+}
+template <typename V> __device__ __forceinline__ V czero() {
+  V r;
+  r.x = r.y = 0;
+  return r;
 }
 
 // bond block (cation row c, anion column a) applied from a cation: out[c] =
 // sum_a B[c][a] xn[a] per spin, xn = the anion neighbour's segment
-template <int NORB, int NSPIN, bool PHASE>
-__device__ __forceinline__ void bond_from_cation(const double d[3], const double (&Vr)[21],
-                                                 const double2 *__restrict__ xn, double scale,
-                                                 double2 ph, double2 *out) {
+template <int NORB, int NSPIN, bool PHASE, typename T, typename VT>
+__device__ __forceinline__ void bond_from_cation(const T d[3], const T (&Vr)[21],
+                                                 const VT *__restrict__ xn, T scale,
+                                                 double2 ph, VT *out) {
   constexpr int NB = NORB * NSPIN;
-  double2 R[NB];
+  VT R[NB];
 #pragma unroll
   for (int e = 0; e < NB; e++) {
-    const double2 u = __ldg(xn + e);
-    R[e] = make_double2(scale * u.x, scale * u.y);
+    const VT u = __ldg(xn + e);
+    R[e].x = scale * u.x;
+    R[e].y = scale * u.y;
   }
   static_for<0, NORB>([&](auto Cc) {
     constexpr int c = decltype(Cc)::value;
-    double2 run[NSPIN];
+    VT run[NSPIN];
 #pragma unroll
-    for (int sp = 0; sp < NSPIN; sp++) run[sp] = make_double2(0.0, 0.0);
+    for (int sp = 0; sp < NSPIN; sp++) run[sp] = czero<VT>();
     static_for<0, NORB>([&](auto Aa) {
       constexpr int a = decltype(Aa)::value;
-      const double v = sk_elem<a, c>(d, Vr);
+      const T v = sk_elem<a, c>(d, Vr);
 #pragma unroll
       for (int sp = 0; sp < NSPIN; sp++) {
         run[sp].x = fma(v, R[sp * NORB + a].x, run[sp].x);
@@ -75,25 +86,26 @@ __device__ __forceinline__ void bond_from_cation(const double d[3], const double
 
 // the same block applied from an anion (transposed): out[a] = sum_c B[c][a]
 // xn[c], xn = the cation neighbour's segment
-template <int NORB, int NSPIN, bool PHASE>
-__device__ __forceinline__ void bond_from_anion(const double d[3], const double (&Vr)[21],
-                                                const double2 *__restrict__ xn, double scale,
-                                                double2 ph, double2 *out) {
+template <int NORB, int NSPIN, bool PHASE, typename T, typename VT>
+__device__ __forceinline__ void bond_from_anion(const T d[3], const T (&Vr)[21],
+                                                const VT *__restrict__ xn, T scale,
+                                                double2 ph, VT *out) {
   constexpr int NB = NORB * NSPIN;
-  double2 R[NB];
+  VT R[NB];
 #pragma unroll
-  for (int e = 0; e < NB; e++) R[e] = make_double2(0.0, 0.0);
+  for (int e = 0; e < NB; e++) R[e] = czero<VT>();
   static_for<0, NORB>([&](auto Cc) {
     constexpr int c = decltype(Cc)::value;
-    double2 xc[NSPIN];
+    VT xc[NSPIN];
 #pragma unroll
     for (int sp = 0; sp < NSPIN; sp++) {
-      const double2 u = __ldg(xn + sp * NORB + c);
-      xc[sp] = make_double2(scale * u.x, scale * u.y);
+      const VT u = __ldg(xn + sp * NORB + c);
+      xc[sp].x = scale * u.x;
+      xc[sp].y = scale * u.y;
     }
     static_for<0, NORB>([&](auto Aa) {
       constexpr int a = decltype(Aa)::value;
-      const double v = sk_elem<a, c>(d, Vr);
+      const T v = sk_elem<a, c>(d, Vr);
 #pragma unroll
       for (int sp = 0; sp < NSPIN; sp++) {
         R[sp * NORB + a].x = fma(v, xc[sp].x, R[sp * NORB + a].x);
@@ -105,31 +117,36 @@ __device__ __forceinline__ void bond_from_anion(const double d[3], const double 
   for (int e = 0; e < NB; e++) out[e] = PHASE ? cmul(ph, R[e]) : R[e];
 }
 
-template <int NORB, int NSPIN, int WPB, bool DOT, bool PHASE>
+// T: arithmetic of the elements and products (double, or float with
+// complex-float vectors VT for the mixed-precision solve); the bond geometry
+// is double in both
+template <int NORB, int NSPIN, int WPB, bool DOT, bool PHASE, typename T = double,
+          typename VT = double2>
 __global__ void __launch_bounds__(WPB * 32, rc_min_blocks(NORB, NSPIN))
     k_spmv_recompute(long cat_warps, long nwarps, const int *__restrict__ order,
                      const int4 *__restrict__ nbr, const unsigned char *__restrict__ site_m,
                      const int *__restrict__ atom_site, const unsigned char *__restrict__ type,
                      const double *__restrict__ dsp, const double *__restrict__ par, int ns,
                      double lx, double ly, double lz, int include_strain,
-                     const double *__restrict__ onsite, const double2 *__restrict__ x,
-                     double2 *__restrict__ y, double shift, const double *__restrict__ xnorm,
+                     const double *__restrict__ onsite, const VT *__restrict__ x,
+                     VT *__restrict__ y, double shift_d, const double *__restrict__ xnorm,
                      int xnorm_idx, double *partial, unsigned int *counter, double *alpha_out,
                      int alpha_idx, const double2 *__restrict__ phase) {
   constexpr int NB = NORB * NSPIN;
-  constexpr int PS = NB + 1;  // padded row: conflict-free 16-byte accesses
+  constexpr int PS = NB + 1;  // padded row: conflict-free accesses
   constexpr int ONS = onsite_len(NB);
-  __shared__ double2 part[WPB][kRcAtoms][4][PS];
+  __shared__ VT part[WPB][kRcAtoms][4][PS];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const long gw = long(blockIdx.x) * WPB + w;
   const bool live = gw < nwarps;  // warp-uniform
-  const double scale = xnorm ? 1.0 / xnorm[xnorm_idx] : 1.0;
+  const T scale = T(xnorm ? 1.0 / xnorm[xnorm_idx] : 1.0);
+  const T shift = T(shift_d);
   // phase 1: lane = (atom, bond)
   if (live) {
     const bool cat = gw < cat_warps;  // warp-uniform
     const int ai = lane >> 2, n = lane & 3;
     const int a = order[gw * kRcAtoms + ai];
-    double2 *out = part[w][ai][n];
+    VT *out = part[w][ai][n];
     int b = -1;
     if (a >= 0) {
       const int4 v = nbr[a];
@@ -141,12 +158,13 @@ __global__ void __launch_bounds__(WPB * 32, rc_min_blocks(NORB, NSPIN))
       const int ts = type[s], tn = type[sn];
       const int cs = cat ? ts : tn, as = cat ? tn : ts;
       const double *P = par + (long(cs < ns ? cs : 0) * ns + (as < ns ? as : 0)) * kNPAR;
-      double d[3], d0[3], r;
+      double dd[3], d0[3], r;
       if (cat)
-        bond_geometry(s, n, sn, P[pA0], dsp, lx, ly, lz, d, d0, r);
+        bond_geometry(s, n, sn, P[pA0], dsp, lx, ly, lz, dd, d0, r);
       else
-        bond_geometry(sn, c_rev_slot[m][n], s, P[pA0], dsp, lx, ly, lz, d, d0, r);
-      double Vr[21];
+        bond_geometry(sn, c_rev_slot[m][n], s, P[pA0], dsp, lx, ly, lz, dd, d0, r);
+      const T d[3] = {T(dd[0]), T(dd[1]), T(dd[2])};
+      T Vr[21];
       scaled_integrals<NORB>(P, include_strain, r, Vr);
       const double2 ph = PHASE ? __ldg(phase + long(a) * 4 + n) : make_double2(1.0, 0.0);
       if (cat)
@@ -155,7 +173,7 @@ __global__ void __launch_bounds__(WPB * 32, rc_min_blocks(NORB, NSPIN))
         bond_from_anion<NORB, NSPIN, PHASE>(d, Vr, x + long(b) * NB, scale, ph, out);
     } else {
 #pragma unroll
-      for (int e = 0; e < NB; e++) out[e] = make_double2(0.0, 0.0);
+      for (int e = 0; e < NB; e++) out[e] = czero<VT>();
     }
   }
   __syncwarp();
@@ -170,22 +188,26 @@ __global__ void __launch_bounds__(WPB * 32, rc_min_blocks(NORB, NSPIN))
     const int a = order[gw * kRcAtoms + ai];
     if (a < 0) continue;
     const double *rec = onsite + long(a) * ONS;
-    const double2 *X0 = x + long(a) * NB;
+    const VT *X0 = x + long(a) * NB;
     auto xo = [&](int e) {
-      const double2 u = __ldg(X0 + e);
-      return make_double2(scale * u.x, scale * u.y);
+      const VT u = __ldg(X0 + e);
+      VT r;
+      r.x = scale * u.x;
+      r.y = scale * u.y;
+      return r;
     };
-    double2 acc[NSPIN];
+    VT acc[NSPIN];
 #pragma unroll
     for (int sp = 0; sp < NSPIN; sp++) {
-      const double2 v0 = xo(sp * NORB + o);
-      const double dg = rec[sp * NORB + o];
-      acc[sp] = make_double2(dg * v0.x, dg * v0.y);
+      const VT v0 = xo(sp * NORB + o);
+      const T dg = T(rec[sp * NORB + o]);
+      acc[sp].x = dg * v0.x;
+      acc[sp].y = dg * v0.y;
     }
     if (o >= 1 && o <= 4 && rec[NB + 1] != 0.0) {  // dangling-bond sp3 couplings
-      const double sx = rec[NB + 2], sy = rec[NB + 3], sz = rec[NB + 4];
-      const double cxy = rec[NB + 5], cxz = rec[NB + 6], cyz = rec[NB + 7];
-      double c1, c2, c3;
+      const T sx = T(rec[NB + 2]), sy = T(rec[NB + 3]), sz = T(rec[NB + 4]);
+      const T cxy = T(rec[NB + 5]), cxz = T(rec[NB + 6]), cyz = T(rec[NB + 7]);
+      T c1, c2, c3;
       int k1, k2, k3;
       if (o == 1) { c1 = sx; k1 = 2; c2 = sy; k2 = 3; c3 = sz; k3 = 4; }
       else if (o == 2) { c1 = sx; k1 = 1; c2 = cxy; k2 = 3; c3 = cxz; k3 = 4; }
@@ -193,29 +215,29 @@ __global__ void __launch_bounds__(WPB * 32, rc_min_blocks(NORB, NSPIN))
       else { c1 = sz; k1 = 1; c2 = cxz; k2 = 2; c3 = cyz; k3 = 3; }
 #pragma unroll
       for (int sp = 0; sp < NSPIN; sp++) {
-        const double2 u1 = xo(sp * NORB + k1), u2 = xo(sp * NORB + k2), u3 = xo(sp * NORB + k3);
+        const VT u1 = xo(sp * NORB + k1), u2 = xo(sp * NORB + k2), u3 = xo(sp * NORB + k3);
         acc[sp].x = fma(c1, u1.x, acc[sp].x); acc[sp].y = fma(c1, u1.y, acc[sp].y);
         acc[sp].x = fma(c2, u2.x, acc[sp].x); acc[sp].y = fma(c2, u2.y, acc[sp].y);
         acc[sp].x = fma(c3, u3.x, acc[sp].x); acc[sp].y = fma(c3, u3.y, acc[sp].y);
       }
     }
     if (NSPIN == 2 && o >= 2 && o <= 4) {  // on-site spin-orbit (mb_ham_spds_so.h)
-      const double L = rec[NB];
-      double2 &a0 = acc[0], &a1 = acc[NSPIN - 1];
+      const T L = T(rec[NB]);
+      VT &a0 = acc[0], &a1 = acc[NSPIN - 1];
       if (o == 2) {
-        const double2 U3 = xo(3), D4 = xo(NORB + 4), D3 = xo(NORB + 3), U4 = xo(4);
+        const VT U3 = xo(3), D4 = xo(NORB + 4), D3 = xo(NORB + 3), U4 = xo(4);
         a0.x += L * U3.y; a0.y -= L * U3.x;
         a0.x += L * D4.x; a0.y += L * D4.y;
         a1.x -= L * D3.y; a1.y += L * D3.x;
         a1.x -= L * U4.x; a1.y -= L * U4.y;
       } else if (o == 3) {
-        const double2 U2 = xo(2), D4 = xo(NORB + 4), D2 = xo(NORB + 2), U4 = xo(4);
+        const VT U2 = xo(2), D4 = xo(NORB + 4), D2 = xo(NORB + 2), U4 = xo(4);
         a0.x -= L * U2.y; a0.y += L * U2.x;
         a0.x += L * D4.y; a0.y -= L * D4.x;
         a1.x += L * D2.y; a1.y -= L * D2.x;
         a1.x += L * U4.y; a1.y -= L * U4.x;
       } else {
-        const double2 D2 = xo(NORB + 2), D3 = xo(NORB + 3), U2 = xo(2), U3 = xo(3);
+        const VT D2 = xo(NORB + 2), D3 = xo(NORB + 3), U2 = xo(2), U3 = xo(3);
         a0.x -= L * D2.x; a0.y -= L * D2.y;
         a0.x -= L * D3.y; a0.y += L * D3.x;
         a1.x += L * U2.x; a1.y += L * U2.y;
@@ -226,44 +248,52 @@ __global__ void __launch_bounds__(WPB * 32, rc_min_blocks(NORB, NSPIN))
     for (int n = 0; n < 4; n++) {
 #pragma unroll
       for (int sp = 0; sp < NSPIN; sp++) {
-        const double2 t = part[w][ai][n][sp * NORB + o];
+        const VT t = part[w][ai][n][sp * NORB + o];
         acc[sp].x += t.x;
         acc[sp].y += t.y;
       }
     }
 #pragma unroll
     for (int sp = 0; sp < NSPIN; sp++) {
-      const double2 x0 = xo(sp * NORB + o);
-      const double2 out = make_double2(acc[sp].x - shift * x0.x, acc[sp].y - shift * x0.y);
+      const VT x0 = xo(sp * NORB + o);
+      VT out;
+      out.x = acc[sp].x - shift * x0.x;
+      out.y = acc[sp].y - shift * x0.y;
       y[long(a) * NB + sp * NORB + o] = out;
-      dot += x0.x * out.x + x0.y * out.y;
+      dot += double(x0.x) * double(out.x) + double(x0.y) * double(out.y);
     }
   }
   if (DOT) grid_reduce<WPB * 32>(dot, partial, counter, alpha_out, alpha_idx, false);
 }
 
-template <int NORB, int NSPIN>
-int launch_t(Ctx &c, const double *x, double *y, double shift, const double *xnorm, int xidx,
+template <int NORB, int NSPIN, typename T, typename VT>
+int launch_t(Ctx &c, const void *x, void *y, double shift, const double *xnorm, int xidx,
              double *alpha_out, int aidx, cudaStream_t s) {
   constexpr int WPB = 4;
   if (c.rc_warps <= 0) return set_error(TBGPU_E_STATE);
   const unsigned grid = unsigned((c.rc_warps + WPB - 1) / WPB);
-  const double2 *X = reinterpret_cast<const double2 *>(x);
-  double2 *Y = reinterpret_cast<double2 *>(y);
+  const VT *X = reinterpret_cast<const VT *>(x);
+  VT *Y = reinterpret_cast<VT *>(y);
   if (alpha_out) {
     int rc = ensure_partials(c, int(grid));
     if (rc) return rc;
   }
 #define TBGPU_RECOMPUTE(DOT, PH)                                                               \
-  k_spmv_recompute<NORB, NSPIN, WPB, DOT, PH><<<grid, WPB * 32, 0, s>>>(                      \
+  k_spmv_recompute<NORB, NSPIN, WPB, DOT, PH, T, VT><<<grid, WPB * 32, 0, s>>>(               \
       c.rc_cat_warps, c.rc_warps, c.d_rc_order, c.d_nbr, c.d_site_m, c.d_atom_site, c.d_type, \
       c.d_dsp, c.d_par, c.nspecies, c.lattice[0], c.lattice[1], c.lattice[2],                 \
       c.include_strain, c.d_onsite, X, Y, shift, xnorm, xidx, DOT ? c.d_partial : nullptr,    \
       DOT ? c.d_counter : nullptr, alpha_out, aidx, c.d_phase)
-  if (alpha_out && c.bloch) TBGPU_RECOMPUTE(true, true);
-  else if (alpha_out) TBGPU_RECOMPUTE(true, false);
-  else if (c.bloch) TBGPU_RECOMPUTE(false, true);
-  else TBGPU_RECOMPUTE(false, false);
+  if constexpr (sizeof(T) == sizeof(double)) {
+    if (alpha_out && c.bloch) TBGPU_RECOMPUTE(true, true);
+    else if (alpha_out) TBGPU_RECOMPUTE(true, false);
+    else if (c.bloch) TBGPU_RECOMPUTE(false, true);
+    else TBGPU_RECOMPUTE(false, false);
+  } else {  // the float product serves the mixed-precision solve at Gamma
+    if (c.bloch) return set_error(TBGPU_E_UNSUPPORTED);
+    if (alpha_out) TBGPU_RECOMPUTE(true, false);
+    else TBGPU_RECOMPUTE(false, false);
+  }
 #undef TBGPU_RECOMPUTE
   TB_CUDA(cudaGetLastError());
   return TBGPU_OK;
@@ -299,10 +329,23 @@ int build_recompute_order(Ctx &c) {
 
 int launch_spmv_recompute(Ctx &c, const double *x, double *y, double shift, const double *xnorm,
                           int xidx, double *alpha_out, int aidx, cudaStream_t s) {
-  if (c.norb == 10 && c.nspin == 2) return launch_t<10, 2>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
-  if (c.norb == 10 && c.nspin == 1) return launch_t<10, 1>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
-  if (c.norb == 5 && c.nspin == 2) return launch_t<5, 2>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
-  if (c.norb == 5 && c.nspin == 1) return launch_t<5, 1>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
+#define TBGPU_RC_CASE(NO, NS)                                                                  \
+  if (c.norb == NO && c.nspin == NS)                                                           \
+    return launch_t<NO, NS, double, double2>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
+  TBGPU_RC_CASE(10, 2) TBGPU_RC_CASE(10, 1) TBGPU_RC_CASE(5, 2) TBGPU_RC_CASE(5, 1)
+#undef TBGPU_RC_CASE
+  return set_error(TBGPU_E_UNSUPPORTED);
+}
+
+// complex-float vectors, float elements and accumulation (mixed precision)
+int launch_spmv_recompute_f32(Ctx &c, const float *x, float *y, double shift,
+                              const double *xnorm, int xidx, double *alpha_out, int aidx,
+                              cudaStream_t s) {
+#define TBGPU_RC_CASE(NO, NS)                                                                  \
+  if (c.norb == NO && c.nspin == NS)                                                           \
+    return launch_t<NO, NS, float, float2>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
+  TBGPU_RC_CASE(10, 2) TBGPU_RC_CASE(10, 1) TBGPU_RC_CASE(5, 2) TBGPU_RC_CASE(5, 1)
+#undef TBGPU_RC_CASE
   return set_error(TBGPU_E_UNSUPPORTED);
 }
 

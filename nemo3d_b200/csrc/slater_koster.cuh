@@ -74,39 +74,39 @@ __device__ __forceinline__ void static_for(F &&f) {
 // Slater-Koster element for orbital a on the first atom, b on the second,
 // ang(a) <= ang(b), cosines d[] from first to second (Slater & Koster 1954,
 // Table I, written with index permutations).
-__device__ __forceinline__ double sk_ordered(int a, int b, const double d[3], double Vs, double Vp,
-                             double Vd) {
+template <typename T>
+__device__ __forceinline__ T sk_ordered(int a, int b, const T d[3], T Vs, T Vp, T Vd) {
   const int la = ang_of(a), lb = ang_of(b);
-  const double s3 = kSqr3;
+  const T s3 = T(kSqr3);
   if (lb == 0) return Vs;                          // s/s* - s/s*
   if (la == 0 && lb == 1) return d[b - 2] * Vs;    // s - p
-  const double l2 = d[0] * d[0], m2 = d[1] * d[1], n2 = d[2] * d[2];
-  const double q = n2 - 0.5 * (l2 + m2);           // 3z2-r2 angular factor
-  const double lm2 = l2 - m2;
+  const T l2 = d[0] * d[0], m2 = d[1] * d[1], n2 = d[2] * d[2];
+  const T q = n2 - T(0.5) * (l2 + m2);           // 3z2-r2 angular factor
+  const T lm2 = l2 - m2;
   // t2g orbitals dxy, dyz, dzx as index pairs (u, v)
   const int tu[3] = {0, 1, 2}, tv[3] = {1, 2, 0};
   if (la == 0) {                                    // s - d
     if (b < 8) return s3 * d[tu[b - 5]] * d[tv[b - 5]] * Vs;
-    return (b == 8 ? 0.5 * s3 * lm2 : q) * Vs;
+    return (b == 8 ? T(0.5) * s3 * lm2 : q) * Vs;
   }
   if (la == 1 && lb == 1) {                         // p - p
-    const double di = d[a - 2], dj = d[b - 2];
-    return a == b ? di * di * Vs + (1.0 - di * di) * Vp : di * dj * Vs - di * dj * Vp;
+    const T di = d[a - 2], dj = d[b - 2];
+    return a == b ? di * di * Vs + (T(1.0) - di * di) * Vp : di * dj * Vs - di * dj * Vp;
   }
   if (la == 1) {                                    // p - d
     const int i = a - 2;
-    const double di = d[i];
+    const T di = d[i];
     if (b < 8) {
       const int u = tu[b - 5], v = tv[b - 5];
-      if (i == u) return s3 * d[u] * d[u] * d[v] * Vs + d[v] * (1.0 - 2.0 * d[u] * d[u]) * Vp;
-      if (i == v) return s3 * d[v] * d[v] * d[u] * Vs + d[u] * (1.0 - 2.0 * d[v] * d[v]) * Vp;
-      const double p3 = d[0] * d[1] * d[2];
-      return s3 * p3 * Vs - 2.0 * p3 * Vp;
+      if (i == u) return s3 * d[u] * d[u] * d[v] * Vs + d[v] * (T(1.0) - T(2.0) * d[u] * d[u]) * Vp;
+      if (i == v) return s3 * d[v] * d[v] * d[u] * Vs + d[u] * (T(1.0) - T(2.0) * d[v] * d[v]) * Vp;
+      const T p3 = d[0] * d[1] * d[2];
+      return s3 * p3 * Vs - T(2.0) * p3 * Vp;
     }
     if (b == 8) {
-      if (i == 0) return 0.5 * s3 * di * lm2 * Vs + di * (1.0 - lm2) * Vp;
-      if (i == 1) return 0.5 * s3 * di * lm2 * Vs - di * (1.0 + lm2) * Vp;
-      return 0.5 * s3 * di * lm2 * Vs - di * lm2 * Vp;
+      if (i == 0) return T(0.5) * s3 * di * lm2 * Vs + di * (T(1.0) - lm2) * Vp;
+      if (i == 1) return T(0.5) * s3 * di * lm2 * Vs - di * (T(1.0) + lm2) * Vp;
+      return T(0.5) * s3 * di * lm2 * Vs - di * lm2 * Vp;
     }
     if (i < 2) return di * q * Vs - s3 * di * n2 * Vp;
     return di * q * Vs + s3 * di * (l2 + m2) * Vp;
@@ -117,29 +117,29 @@ __device__ __forceinline__ double sk_ordered(int a, int b, const double d[3], do
     const int u1 = tu[x - 5], v1 = tv[x - 5];
     if (x == y) {
       const int w = 3 - u1 - v1;
-      const double pu = d[u1] * d[u1], pv = d[v1] * d[v1];
-      return 3.0 * pu * pv * Vs + (pu + pv - 4.0 * pu * pv) * Vp + (d[w] * d[w] + pu * pv) * Vd;
+      const T pu = d[u1] * d[u1], pv = d[v1] * d[v1];
+      return T(3.0) * pu * pv * Vs + (pu + pv - T(4.0) * pu * pv) * Vp + (d[w] * d[w] + pu * pv) * Vd;
     }
     const int u2 = tu[y - 5], v2 = tv[y - 5];
     const int sh = (u1 == u2 || u1 == v2) ? u1 : v1;  // shared index
     const int p = (u1 == sh) ? v1 : u1, r = (u2 == sh) ? v2 : u2;
-    const double ds2 = d[sh] * d[sh], pr = d[p] * d[r];
-    return 3.0 * pr * ds2 * Vs + pr * (1.0 - 4.0 * ds2) * Vp + pr * (ds2 - 1.0) * Vd;
+    const T ds2 = d[sh] * d[sh], pr = d[p] * d[r];
+    return T(3.0) * pr * ds2 * Vs + pr * (T(1.0) - T(4.0) * ds2) * Vp + pr * (ds2 - T(1.0)) * Vd;
   }
   if (x < 8) {                                      // t2g - eg
-    const double l = d[0], m = d[1], n = d[2];
+    const T l = d[0], m = d[1], n = d[2];
     if (y == 8) {
-      if (x == 5) return 1.5 * l * m * lm2 * Vs - 2.0 * l * m * lm2 * Vp + 0.5 * l * m * lm2 * Vd;
-      if (x == 6) return 1.5 * m * n * lm2 * Vs - m * n * (1.0 + 2.0 * lm2) * Vp + m * n * (1.0 + 0.5 * lm2) * Vd;
-      return 1.5 * n * l * lm2 * Vs + n * l * (1.0 - 2.0 * lm2) * Vp - n * l * (1.0 - 0.5 * lm2) * Vd;
+      if (x == 5) return T(1.5) * l * m * lm2 * Vs - T(2.0) * l * m * lm2 * Vp + T(0.5) * l * m * lm2 * Vd;
+      if (x == 6) return T(1.5) * m * n * lm2 * Vs - m * n * (T(1.0) + T(2.0) * lm2) * Vp + m * n * (T(1.0) + T(0.5) * lm2) * Vd;
+      return T(1.5) * n * l * lm2 * Vs + n * l * (T(1.0) - T(2.0) * lm2) * Vp - n * l * (T(1.0) - T(0.5) * lm2) * Vd;
     }
-    if (x == 5) return s3 * l * m * q * Vs - 2.0 * s3 * l * m * n2 * Vp + 0.5 * s3 * l * m * (1.0 + n2) * Vd;
-    const double uv = (x == 6) ? m * n : l * n;
-    return s3 * uv * q * Vs + s3 * uv * (l2 + m2 - n2) * Vp - 0.5 * s3 * uv * (l2 + m2) * Vd;
+    if (x == 5) return s3 * l * m * q * Vs - T(2.0) * s3 * l * m * n2 * Vp + T(0.5) * s3 * l * m * (T(1.0) + n2) * Vd;
+    const T uv = (x == 6) ? m * n : l * n;
+    return s3 * uv * q * Vs + s3 * uv * (l2 + m2 - n2) * Vp - T(0.5) * s3 * uv * (l2 + m2) * Vd;
   }
-  if (x == 8 && y == 8) return 0.75 * lm2 * lm2 * Vs + (l2 + m2 - lm2 * lm2) * Vp + (n2 + 0.25 * lm2 * lm2) * Vd;
-  if (x == 8) return 0.5 * s3 * lm2 * q * Vs - s3 * n2 * lm2 * Vp + 0.25 * s3 * (1.0 + n2) * lm2 * Vd;
-  return q * q * Vs + 3.0 * n2 * (l2 + m2) * Vp + 0.75 * (l2 + m2) * (l2 + m2) * Vd;
+  if (x == 8 && y == 8) return T(0.75) * lm2 * lm2 * Vs + (l2 + m2 - lm2 * lm2) * Vp + (n2 + T(0.25) * lm2 * lm2) * Vd;
+  if (x == 8) return T(0.5) * s3 * lm2 * q * Vs - s3 * n2 * lm2 * Vp + T(0.25) * s3 * (T(1.0) + n2) * lm2 * Vd;
+  return q * q * Vs + T(3.0) * n2 * (l2 + m2) * Vp + T(0.75) * (l2 + m2) * (l2 + m2) * Vd;
 }
 
 // <anion orbital a | H | cation orbital c>, cosines from anion to cation,
@@ -157,22 +157,22 @@ __device__ __forceinline__ double sk_bond(int a, int c, const double d[3], const
 // sk_bond for orbitals known at compile time, integrals Vr[k] = parameter
 // 10 + k: every table lookup and branch resolves in the compiler, so a warp
 // whose lanes hold different bonds evaluates one element without divergence.
-template <int I>
-__device__ __forceinline__ double vr_get(const double (&Vr)[21]) {
+template <int I, typename T>
+__device__ __forceinline__ T vr_get(const T (&Vr)[21]) {
   if constexpr (I >= 0) return Vr[I - 10];
-  else return 0.0;
+  else return T(0);
 }
-template <int A, int C>
-__device__ __forceinline__ double sk_elem(const double d[3], const double (&Vr)[21]) {
+template <int A, int C, typename T>
+__device__ __forceinline__ T sk_elem(const T d[3], const T (&Vr)[21]) {
   constexpr int ka = kind_of(A), kc = kind_of(C);
-  const double Vs = vr_get<vidx_of(ka, kc, 0)>(Vr);
-  const double Vp = vr_get<vidx_of(ka, kc, 1)>(Vr);
-  const double Vd = vr_get<vidx_of(ka, kc, 2)>(Vr);
+  const T Vs = vr_get<vidx_of(ka, kc, 0)>(Vr);
+  const T Vp = vr_get<vidx_of(ka, kc, 1)>(Vr);
+  const T Vd = vr_get<vidx_of(ka, kc, 2)>(Vr);
   constexpr int la = ang_of(A), lc = ang_of(C);
   if constexpr (la <= lc) {
     return sk_ordered(A, C, d, Vs, Vp, Vd);
   } else {
-    const double e = sk_ordered(C, A, d, Vs, Vp, Vd);
+    const T e = sk_ordered(C, A, d, Vs, Vp, Vd);
     return ((la + lc) & 1) ? -e : e;
   }
 }
@@ -205,27 +205,27 @@ __device__ __forceinline__ void bond_geometry(long s, int n, long sn, double a0,
 
 // The 21 two-centre integrals of the parameter vector P with Harrison's
 // scaling (d0/d)^eta, brat = (sqrt(3)/4 a0) / r, one pow per distinct
-// exponent; Vr[k] is parameter 10 + k.  NORB = 5 skips the d integrals
-// (left at zero).
-template <int NORB>
+// exponent, in precision T (the geometry stays double); Vr[k] is parameter
+// 10 + k.  NORB = 5 skips the d integrals (left at zero).
+template <int NORB, typename T>
 __device__ __forceinline__ void scaled_integrals(const double *P, int include_strain, double r,
-                                                 double (&Vr)[21]) {
+                                                 T (&Vr)[21]) {
   const double *S = P + kNPV;
   if (!include_strain) {
 #pragma unroll
-    for (int k = 0; k < 21; k++) Vr[k] = P[10 + k];
+    for (int k = 0; k < 21; k++) Vr[k] = T(P[10 + k]);
     return;
   }
-  const double brat = (0.25 * kSqr3 * P[pA0]) / r;
-  double pw[14];
+  const T brat = T((0.25 * kSqr3 * P[pA0]) / r);
+  T pw[14];
   static_for<0, 14>([&](auto J) {
     constexpr int j = decltype(J)::value;
-    if constexpr (NORB == 5 && slot_has_d(j)) pw[j] = 0.0;
-    else pw[j] = pow(brat, S[slot_eta(j)]);
+    if constexpr (NORB == 5 && slot_has_d(j)) pw[j] = T(0);
+    else pw[j] = pow(brat, T(S[slot_eta(j)]));
   });
   static_for<0, 21>([&](auto K) {
     constexpr int k = decltype(K)::value;
-    Vr[k] = P[10 + k] * pw[eta_slot(k)];
+    Vr[k] = T(P[10 + k]) * pw[eta_slot(k)];
   });
 }
 

@@ -140,6 +140,9 @@ int assemble(Ctx &c);
 int compute_blocks(Ctx &c, double *blocks);
 // recompute.cu
 int build_recompute_order(Ctx &c);
+int launch_spmv_recompute_f32(Ctx &c, const float *x, float *y, double shift,
+                              const double *xnorm, int xidx, double *alpha_out, int aidx,
+                              cudaStream_t s);
 int launch_spmv_recompute(Ctx &c, const double *x, double *y, double shift,
                           const double *xnorm, int xidx, double *alpha_out, int aidx,
                           cudaStream_t s);

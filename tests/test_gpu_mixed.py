@@ -6,7 +6,8 @@ eigenvector accumulation in double; the returned eigenpairs are refined by a
 double-precision Rayleigh-Ritz step over the recomputed (FP64) Hamiltonian.
 
 Bars: the float product equals the oracle's H*x over the float-rounded
-entries to float rounding (5e-6 of max|y|); each refined eigenvalue of the
+entries (float store) or over the exact entries (float elements recomputed
+from the double geometry) to float rounding (5e-6 of max|y|); each refined eigenvalue of the
 mixed solve agrees within 1e-6 eV with the FP64 solve of a narrow window
 around it, the error printed per state; the refined residuals
 ||Hv - lambda v|| are below 1e-3 eV and the refined vectors are
@@ -31,16 +32,24 @@ def _rounded(o):
     return r
 
 
-@pytest.mark.parametrize("model", ["sp3d5s*_so", "sp3d5s*"])
-def test_float_product_matches_oracle(model):
+@pytest.mark.parametrize("model,storage", [("sp3d5s*_so", "store"), ("sp3d5s*", "store"),
+                                           ("sp3d5s*_so", "recompute"),
+                                           ("sp3d5s*", "recompute"),
+                                           ("sp3s*_so", "recompute"), ("sp3s*", "recompute")])
+def test_float_product_matches_oracle(model, storage):
     import torch
     from nemo3d_b200.tbgpu import Hamiltonian
     st = workloads.dome_in_box(cells=(7, 6, 5), base_nm=2.4, height_nm=1.0, wl_z_nm=1.2,
                                sigma_frac=0.02, seed=3)
-    mats = [materials.MATERIALS[m] for m in SPDS]
+    fam = SPDS if model.startswith("sp3d5s") else ["GaAs_sps", "InAs_sps"]
+    mats = [materials.MATERIALS[m] for m in fam]
     norb, nspin = materials.BAND_MODELS[model]
-    g = Hamiltonian(st, model, mats, ham_bits=32, lanczos_bits=32)
-    o32 = _rounded(oracle.OracleHamiltonian(st, norb, nspin, mats))
+    if storage == "store":
+        g = Hamiltonian(st, model, mats, ham_bits=32, lanczos_bits=32)
+        o32 = _rounded(oracle.OracleHamiltonian(st, norb, nspin, mats))
+    else:  # float elements from the exact geometry: compare with the FP64 H
+        g = Hamiltonian(st, model, mats, recompute=True, lanczos_bits=32)
+        o32 = oracle.OracleHamiltonian(st, norb, nspin, mats)
     x = workloads.random_start(g.n, seed=5).astype(np.float32)
     xd = torch.from_numpy(x).cuda()
     yd = torch.empty_like(xd)
@@ -52,14 +61,16 @@ def test_float_product_matches_oracle(model):
     assert err <= 5e-6, err
 
 
-def test_mixed_solve_matches_fp64_per_state():
+@pytest.mark.parametrize("storage", ["store", "recompute"])
+def test_mixed_solve_matches_fp64_per_state(storage):
     from nemo3d_b200.tbgpu import Hamiltonian
     st = workloads.dome_in_box(cells=(8, 8, 6), base_nm=3.0, height_nm=1.2, wl_z_nm=1.2,
                                sigma_frac=0.01, seed=2)
     mats = [materials.MATERIALS[m] for m in SPDS]
     kw = dict(imax=5000, requested1=2, requested2=2, emin1=-0.6, emax1=0.3, emin2=0.8,
               emax2=2.2, tolerance=1e-7)
-    gm = Hamiltonian(st, "sp3d5s*_so", mats, ham_bits=32, lanczos_bits=32)
+    opts = dict(ham_bits=32) if storage == "store" else dict(recompute=True)
+    gm = Hamiltonian(st, "sp3d5s*_so", mats, lanczos_bits=32, **opts)
     r0 = workloads.random_start(gm.n, seed=0)
     mix = gm.eigensolve_lanczos(r0, vectors=8, **kw)
     vals = mix["values"]
@@ -99,7 +110,7 @@ def test_mixed_refusals():
     with pytest.raises(tbgpu.TbgpuError) as e:  # needs the 32-bit store
         tbgpu.Hamiltonian(st, "sp3d5s*", [materials.MATERIALS["GaAs_spds"]], lanczos_bits=32)
     assert e.value.code == -6
-    with pytest.raises(tbgpu.TbgpuError) as e:  # 10-orbital models only
+    with pytest.raises(tbgpu.TbgpuError) as e:  # the float store: 10-orbital models only
         tbgpu.Hamiltonian(st, "sp3s*", [materials.MATERIALS["GaAs_sps"]], ham_bits=32,
                           lanczos_bits=32)
     assert e.value.code == -6
