@@ -307,6 +307,32 @@ int tbgpu_hx_dot_noalloc(tbgpu_ctx *ctx, double shift, const double *x_dev,
  * 7 warps x 2 stages. */
 int tbgpu_set_spmv_variant(tbgpu_ctx *ctx, int variant);
 
+/* Lanczos for many independent dots at once (no counterpart in the
+ * reference, which solves one structure per run): the context's grid holds
+ * ndots dots side by side along x, dot d in the cells i in [dot_cells[d],
+ * dot_cells[d+1]) (ndots+1 ascending boundaries), separated by empty cells so
+ * that no bond joins two dots (TBGPU_E_ARG otherwise).  Each dot runs the
+ * reference's recurrence and convergence test (eigensolve_lanczos) on its own
+ * segment of the vectors with its own windows emin1[d]..emax2[d]; all dots
+ * iterate together, each iteration one product launch for all dots and
+ * segmented reductions, one check interval captured as a CUDA graph.
+ * r0_dev: the packed start vector (each dot's segment is normalised on its
+ * own).  values: [ndots][values_stride] ascending per dot; found[d],
+ * iterations[d] per dot.  vectors_dev ([max_vectors][dimension], or NULL):
+ * vector e holds every dot's e-th eigenvector in the dot's segment
+ * (max_vectors <= 16).  With tbgpu_set_lanczos_precision(ctx, 32) the dots'
+ * eigenpairs are refined in double as in tbgpu_eigensolve_lanczos, state
+ * errors [ndots][max_vectors] through tbgpu_get_state_errors.  Returns the
+ * total number of values, or a negative error code. */
+int tbgpu_eigensolve_lanczos_batched(tbgpu_ctx *ctx, int ndots, const int *dot_cells,
+                                     int ConvCheckStartIter, int ConvCheckSkipRate, int imax,
+                                     int requested1, int requested2, const double *emin1,
+                                     const double *emax1, const double *emin2,
+                                     const double *emax2, double tolerance,
+                                     const double *r0_dev, double *values, int values_stride,
+                                     int *found, int *iterations, double *vectors_dev,
+                                     int max_vectors);
+
 /* Result files in the reference's <HDR> format (nemo3d/src/io/fileformat.c:
  * 182-204), readable by its post-processing tools.
  * tbgpu_write_eigenvalues: the nd_Ek file (writeEigenvalues,

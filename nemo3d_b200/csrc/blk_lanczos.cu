@@ -681,44 +681,52 @@ int solve_block(Ctx &c, const BlkArgs &A, const double *r0_dev, std::vector<doub
 }
 
 // Double-precision Rayleigh-Ritz refinement of Ritz vectors (the final
-// pass of the mixed-precision solve).  For groups of up to 8 eigenvectors V
-// (double, [nvec][n2], ascending values): W = H V with the double-precision
-// recompute product, S = V^H V, G = V^H W, G y = lambda S y on the host
-// (Cholesky S = U^H U, Hermitian eigenproblem of U^-H G U^-1); V <- V Y with
-// S-orthonormal columns, values <- lambda (ascending), and per state the
-// residual ||H v - lambda v|| and the change of the eigenvalue.
-int refine_ritz(Ctx &c, double *V_dev, int nvec, double *values, std::vector<double> &resid,
-                std::vector<double> &delta, cudaStream_t s) {
-  resid.assign(nvec, 0.0);
-  delta.assign(nvec, 0.0);
-  if (nvec <= 0) return TBGPU_OK;
+// pass of the mixed-precision solves).  Vector e lives at V + e*stride
+// (double complex); nseg disjoint segments [off, off + len) of the vectors are
+// independent problems (one per dot of a batched solve; one segment of the
+// whole vector otherwise), and H never couples two segments.  For groups of
+// up to 8 vectors: W = H V with the double-precision recompute product (all
+// segments at once), then per segment S = V^H V, G = V^H W, G y = lambda S y
+// on the host (Cholesky S = U^H U, Hermitian eigenproblem of U^-H G U^-1);
+// V <- V Y with S-orthonormal columns, values <- lambda (ascending), and the
+// residual ||H v - lambda v|| and the change of each eigenvalue.  values,
+// resid, delta are [nseg][nvec]; seg_nvec (or NULL: nvec each) gives the
+// number of vectors a segment holds.
+int refine_ritz(Ctx &c, double *V_dev, int nvec, long stride, int nseg, const long *seg_off,
+                const long *seg_len, double *values, double *resid, double *delta,
+                cudaStream_t s, const int *seg_nvec) {
+  if (nvec <= 0 || nseg <= 0) return TBGPU_OK;
   if (!c.d_onsite || c.rc_warps <= 0) return set_error(TBGPU_E_STATE);
-  const long n2 = c.natoms * c.nb;
-  const size_t vb = sizeof(double2) * n2;
+  const long dim = c.natoms * c.nb;
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device);
-  const unsigned grid = unsigned(std::max<long>(1, std::min<long>((n2 + 255) / 256, long(sms) * 8)));
+  long maxlen = 0;
+  for (int q = 0; q < nseg; q++) maxlen = std::max(maxlen, seg_len[q]);
+  const unsigned gmax =
+      unsigned(std::max<long>(1, std::min<long>((maxlen + 255) / 256, long(sms) * 8)));
   constexpr int K8 = 8 * 9 / 2;
   const int mg = std::min(nvec, 8);
   double2 *W = nullptr, *T = nullptr;
   double *part = nullptr, *res = nullptr;
   unsigned *counter = nullptr;
   int rc = TBGPU_OK;
-  if (cudaMalloc(&W, vb * mg) != cudaSuccess || cudaMalloc(&T, vb * mg) != cudaSuccess ||
-      cudaMalloc(&part, sizeof(double) * 2 * K8 * grid) != cudaSuccess ||
+  if (cudaMalloc(&W, sizeof(double2) * dim * mg) != cudaSuccess ||
+      cudaMalloc(&T, sizeof(double2) * dim * mg) != cudaSuccess ||
+      cudaMalloc(&part, sizeof(double) * 2 * K8 * gmax) != cudaSuccess ||
       cudaMalloc(&res, sizeof(double) * 2 * K8 * 3) != cudaSuccess ||
       cudaMalloc(&counter, sizeof(unsigned)) != cudaSuccess)
     rc = TBGPU_E_NOMEM;
   if (!rc && cudaMemsetAsync(counter, 0, sizeof(unsigned), s) != cudaSuccess) rc = TBGPU_E_CUDA;
   double2 *V = reinterpret_cast<double2 *>(V_dev);
-  auto ptrs = [&](double2 *base, int m) {
+  // vectors j < m of a set with vector stride vs, offset off
+  auto ptrs = [&](double2 *base, long vs, long off, int m) {
     BlockPtrs b{};
-    for (int j = 0; j < 8; j++) b.v[j] = base + size_t(std::min(j, m - 1)) * n2;
+    for (int j = 0; j < 8; j++) b.v[j] = base + size_t(std::min(j, m - 1)) * vs + off;
     return b;
   };
-  auto outs = [&](double2 *base, int m) {
+  auto outs = [&](double2 *base, long vs, long off, int m) {
     BlockOut b{};
-    for (int j = 0; j < m; j++) b.v[j] = base + size_t(j) * n2;
+    for (int j = 0; j < m; j++) b.v[j] = base + size_t(j) * vs + off;
     return b;
   };
   // lower triangle of X^H Y as an m x m Hermitian matrix
@@ -734,85 +742,103 @@ int refine_ritz(Ctx &c, double *V_dev, int nvec, double *values, std::vector<dou
     return G;
   };
   for (int g0 = 0; g0 < nvec && !rc; g0 += 8) {
-    const int m = std::min(8, nvec - g0);
-    double2 *Vg = V + size_t(g0) * n2;
-    for (int i = 0; i < m && !rc; i++)
-      rc = launch_spmv_recompute(c, reinterpret_cast<const double *>(Vg + size_t(i) * n2),
-                                 reinterpret_cast<double *>(W + size_t(i) * n2), 0.0, nullptr, 0,
-                                 nullptr, 0, s);
-    if (rc) break;
-    k_bdots<8><<<grid, kDotThreads, 0, s>>>(n2, ptrs(Vg, m), ptrs(Vg, m), part, counter, res);
-    k_bdots<8><<<grid, kDotThreads, 0, s>>>(n2, ptrs(Vg, m), ptrs(W, m), part, counter,
-                                            res + 2 * K8);
-    double h[4 * K8];
-    if (cudaGetLastError() != cudaSuccess ||
-        cudaMemcpyAsync(h, res, sizeof(h), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-        cudaStreamSynchronize(s) != cudaSuccess) {
-      rc = TBGPU_E_CUDA;
-      break;
-    }
-    const Mat S = to_mat(h, m), G = to_mat(h + 2 * K8, m);
-    // Y (columns: refined vectors in the basis V) and lambda, ascending
-    Mat Y(size_t(m) * m, cplx(0.0, 0.0));
-    std::vector<double> lam(m);
-    Mat U;
-    if (cholesky_upper(m, S, U)) {
-      const Mat Ui = upper_inverse(m, U);
-      Mat UiH(size_t(m) * m);
-      for (int i = 0; i < m; i++)
-        for (int j = 0; j < m; j++) UiH[i * m + j] = std::conj(Ui[j * m + i]);
-      const Mat Gp = matmul(m, matmul(m, UiH, G), Ui);
-      std::vector<double> w;
-      std::vector<std::vector<cplx>> Z;
-      herm_eig_desc(m, Gp, w, Z);
-      if (int(Z.size()) != m) {
-        rc = TBGPU_E_NUMERIC;
+    const int m_all = std::min(8, nvec - g0);
+    double2 *Vg = V + size_t(g0) * stride;
+    for (int i = 0; i < m_all && !rc; i++)
+      rc = launch_spmv_recompute(c, reinterpret_cast<const double *>(Vg + size_t(i) * stride),
+                                 reinterpret_cast<double *>(W + size_t(i) * dim), 0.0, nullptr,
+                                 0, nullptr, 0, s);
+    for (int q = 0; q < nseg && !rc; q++) {
+      const long off = seg_off[q], n2 = seg_len[q];
+      // this segment's vectors of the group (segments may hold fewer)
+      const int m = std::min(m_all, (seg_nvec ? seg_nvec[q] : nvec) - g0);
+      if (n2 <= 0 || m <= 0) continue;
+      const unsigned grid =
+          unsigned(std::max<long>(1, std::min<long>((n2 + 255) / 256, long(sms) * 8)));
+      k_bdots<8><<<grid, kDotThreads, 0, s>>>(n2, ptrs(Vg, stride, off, m),
+                                              ptrs(Vg, stride, off, m), part, counter, res);
+      k_bdots<8><<<grid, kDotThreads, 0, s>>>(n2, ptrs(Vg, stride, off, m),
+                                              ptrs(W, dim, off, m), part, counter, res + 2 * K8);
+      double h[4 * K8];
+      if (cudaGetLastError() != cudaSuccess ||
+          cudaMemcpyAsync(h, res, sizeof(h), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+          cudaStreamSynchronize(s) != cudaSuccess) {
+        rc = TBGPU_E_CUDA;
         break;
       }
-      for (int e = 0; e < m; e++) {  // herm_eig_desc is descending
-        const int src = m - 1 - e;
-        lam[e] = w[src];
-        for (int i = 0; i < m; i++) {
-          cplx v(0.0, 0.0);
-          for (int k = 0; k < m; k++) v += Ui[i * m + k] * Z[src][k];
-          Y[i * m + e] = v;
-        }
-      }
-    } else {  // dependent vectors: plain Rayleigh quotients, one by one
-      for (int e = 0; e < m; e++) {
-        const double nn = S[e * m + e].real();
-        if (!(nn > 0.0)) {
+      const Mat S = to_mat(h, m), G = to_mat(h + 2 * K8, m);
+      // Y (columns: refined vectors in the basis V) and lambda, ascending
+      Mat Y(size_t(m) * m, cplx(0.0, 0.0));
+      std::vector<double> lam(m);
+      Mat U;
+      if (cholesky_upper(m, S, U)) {
+        const Mat Ui = upper_inverse(m, U);
+        Mat UiH(size_t(m) * m);
+        for (int i = 0; i < m; i++)
+          for (int j = 0; j < m; j++) UiH[i * m + j] = std::conj(Ui[j * m + i]);
+        const Mat Gp = matmul(m, matmul(m, UiH, G), Ui);
+        std::vector<double> w;
+        std::vector<std::vector<cplx>> Z;
+        herm_eig_desc(m, Gp, w, Z);
+        if (int(Z.size()) != m) {
           rc = TBGPU_E_NUMERIC;
           break;
         }
-        lam[e] = G[e * m + e].real() / nn;
-        Y[e * m + e] = 1.0 / std::sqrt(nn);
+        for (int e = 0; e < m; e++) {  // herm_eig_desc is descending
+          const int src = m - 1 - e;
+          lam[e] = w[src];
+          for (int i = 0; i < m; i++) {
+            cplx v(0.0, 0.0);
+            for (int k = 0; k < m; k++) v += Ui[i * m + k] * Z[src][k];
+            Y[i * m + e] = v;
+          }
+        }
+      } else {  // dependent vectors: plain Rayleigh quotients, one by one
+        for (int e = 0; e < m; e++) {
+          const double nn = S[e * m + e].real();
+          if (!(nn > 0.0)) {
+            rc = TBGPU_E_NUMERIC;
+            break;
+          }
+          lam[e] = G[e * m + e].real() / nn;
+          Y[e * m + e] = 1.0 / std::sqrt(nn);
+        }
+        if (rc) break;
       }
-      if (rc) break;
-    }
-    SmallMat My{}, Ml{};
-    for (int k = 0; k < m; k++)
-      for (int e = 0; e < m; e++) My.m[k][e] = make_double2(Y[k * m + e].real(), Y[k * m + e].imag());
-    for (int e = 0; e < m; e++) Ml.m[e][e] = make_double2(-lam[e], 0.0);
-    // T = W Y; W = V Y (refined vectors); T -= W diag(lambda) (residuals)
-    k_bcombine<8><<<grid, 256, 0, s>>>(n2, m, ptrs(W, m), My, m, outs(T, m), 0.0, ptrs(T, m));
-    k_bcombine<8><<<grid, 256, 0, s>>>(n2, m, ptrs(Vg, m), My, m, outs(W, m), 0.0, ptrs(W, m));
-    k_bcombine<8><<<grid, 256, 0, s>>>(n2, m, ptrs(W, m), Ml, m, outs(T, m), 1.0, ptrs(T, m));
-    k_bdots<8><<<grid, kDotThreads, 0, s>>>(n2, ptrs(T, m), ptrs(T, m), part, counter,
-                                            res + 4 * K8);
-    double hr[2 * K8];
-    if (cudaGetLastError() != cudaSuccess ||
-        cudaMemcpyAsync(Vg, W, vb * m, cudaMemcpyDeviceToDevice, s) != cudaSuccess ||
-        cudaMemcpyAsync(hr, res + 4 * K8, sizeof(hr), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-        cudaStreamSynchronize(s) != cudaSuccess) {
-      rc = TBGPU_E_CUDA;
-      break;
-    }
-    for (int e = 0; e < m; e++) {
-      const int t = e * (e + 1) / 2 + e;  // diagonal entry (e, e)
-      resid[g0 + e] = std::sqrt(std::max(hr[2 * t], 0.0));
-      delta[g0 + e] = lam[e] - values[g0 + e];
-      values[g0 + e] = lam[e];
+      SmallMat My{}, Ml{};
+      for (int k = 0; k < m; k++)
+        for (int e = 0; e < m; e++)
+          My.m[k][e] = make_double2(Y[k * m + e].real(), Y[k * m + e].imag());
+      for (int e = 0; e < m; e++) Ml.m[e][e] = make_double2(-lam[e], 0.0);
+      // T = W Y; V = V Y (in place through T's second half is not possible:
+      // the refined vectors go to T, the residuals to W, both segment-local)
+      k_bcombine<8><<<grid, 256, 0, s>>>(n2, m, ptrs(W, dim, off, m), My, m,
+                                         outs(T, dim, off, m), 0.0, ptrs(T, dim, off, m));
+      k_bcombine<8><<<grid, 256, 0, s>>>(n2, m, ptrs(Vg, stride, off, m), My, m,
+                                         outs(W, dim, off, m), 0.0, ptrs(W, dim, off, m));
+      // W now holds V Y; T = T - W diag(lambda) are the residuals
+      k_bcombine<8><<<grid, 256, 0, s>>>(n2, m, ptrs(W, dim, off, m), Ml, m,
+                                         outs(T, dim, off, m), 1.0, ptrs(T, dim, off, m));
+      k_bdots<8><<<grid, kDotThreads, 0, s>>>(n2, ptrs(T, dim, off, m), ptrs(T, dim, off, m),
+                                              part, counter, res + 4 * K8);
+      double hr[2 * K8];
+      bool ok = cudaGetLastError() == cudaSuccess;
+      for (int e = 0; e < m && ok; e++)
+        ok = cudaMemcpyAsync(Vg + size_t(e) * stride + off, W + size_t(e) * dim + off,
+                             sizeof(double2) * n2, cudaMemcpyDeviceToDevice, s) == cudaSuccess;
+      if (!ok ||
+          cudaMemcpyAsync(hr, res + 4 * K8, sizeof(hr), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+          cudaStreamSynchronize(s) != cudaSuccess) {
+        rc = TBGPU_E_CUDA;
+        break;
+      }
+      for (int e = 0; e < m; e++) {
+        const int t = e * (e + 1) / 2 + e;  // diagonal entry (e, e)
+        const size_t at = size_t(q) * nvec + g0 + e;
+        if (resid) resid[at] = std::sqrt(std::max(hr[2 * t], 0.0));
+        if (delta) delta[at] = lam[e] - values[at];
+        values[at] = lam[e];
+      }
     }
   }
   cudaStreamSynchronize(s);

@@ -224,10 +224,9 @@ static int to_float(Ctx &c, long n, const double *in, float **out) {
 int assemble(Ctx &c) {
   const long na = c.natoms;
   if (c.recompute && c.ham_fp32) return set_error(TBGPU_E_UNSUPPORTED);
-  // the mixed-precision solve runs on the float store (10-orbital models) or
-  // on the recompute product (any model)
-  if (c.lanczos_f32 && !c.recompute && !(c.ham_fp32 && c.norb == 10))
-    return set_error(TBGPU_E_UNSUPPORTED);
+  // the mixed-precision solve runs on the float store or on the recompute
+  // product
+  if (c.lanczos_f32 && !c.recompute && !c.ham_fp32) return set_error(TBGPU_E_UNSUPPORTED);
   // recompute: the blocks are not stored; the assembly still runs the bond
   // kernel for the on-site strain corrections
   if (!c.recompute)

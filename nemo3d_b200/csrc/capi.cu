@@ -181,10 +181,7 @@ int tbgpu_hx_dev_f32(tbgpu_ctx *ctx, double shift, const float *x_dev, float *y_
   if (!ctx || !x_dev || !y_dev) return set_error(TBGPU_E_ARG);
   Ctx &c = *C(ctx);
   if (!c.built) return set_error(TBGPU_E_STATE);
-  if (c.bloch) return set_error(TBGPU_E_UNSUPPORTED);
-  if (c.recompute)
-    return launch_spmv_recompute_f32(c, x_dev, y_dev, shift, nullptr, 0, nullptr, 0, c.stream);
-  return launch_spmv_async_f32(c, x_dev, y_dev, shift, nullptr, 0, nullptr, 0, c.stream);
+  return launch_spmv_f32(c, x_dev, y_dev, shift, nullptr, 0, nullptr, 0, c.stream);
 }
 
 void tbgpu_matvect_mult(const int **argList, tbgpu_dcomplex *y, const tbgpu_dcomplex *x) {

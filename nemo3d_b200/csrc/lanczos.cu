@@ -25,8 +25,9 @@
 #include <cstring>
 #include <vector>
 
-#include "tbgpu_internal.cuh"
+#include "host_par.h"
 #include "reduce.cuh"
+#include "tbgpu_internal.cuh"
 
 namespace tbgpu {
 
@@ -189,24 +190,6 @@ static int sturm_below(int n, const double *d, const double *e2, double x) {
   return cnt;
 }
 
-// run f(i) for i in [0, n) on up to hardware_concurrency host threads
-template <class F>
-static void parallel_for(int n, F f) {
-  int nt = int(std::thread::hardware_concurrency());
-  nt = std::max(1, std::min({nt, 32, n}));
-  if (nt <= 1) {
-    for (int i = 0; i < n; i++) f(i);
-    return;
-  }
-  std::atomic<int> next{0};
-  std::vector<std::thread> th;
-  for (int t = 0; t < nt; t++)
-    th.emplace_back([&]() {
-      for (int i = next++; i < n; i = next++) f(i);
-    });
-  for (auto &x : th) x.join();
-}
-
 // eigenvalues of T (diag d, off-diagonal e) in (vl, vu], ascending
 static std::vector<double> tri_eigs(int n, const double *d, const double *e, double vl,
                                     double vu) {
@@ -235,17 +218,10 @@ static std::vector<double> tri_eigs(int n, const double *d, const double *e, dou
   return w;
 }
 
-struct Rng {  // uniform [0,1] starts for inverse iteration
-  unsigned long long s;
-  double next() {
-    s = s * 6364136223846793005ULL + 1442695040888963407ULL;
-    return double(s >> 11) * (1.0 / 9007199254740992.0);
-  }
-};
 
 // 20 solves with T - (lambda + 1e-8) on the leading m x m block; x out
-static bool inverse_iteration(int m, const double *d, const double *e, double lambda,
-                              Rng &rng, std::vector<double> &x) {
+bool inverse_iteration(int m, const double *d, const double *e, double lambda, Rng &rng,
+                       std::vector<double> &x) {
   std::vector<double> ds(m), g(m), y(m);
   x.assign(m, 0.0);
   for (int i = 0; i < m; i++) ds[i] = d[i] - (lambda + 1e-8);
@@ -279,9 +255,9 @@ static bool inverse_iteration(int m, const double *d, const double *e, double la
 // find_converged_eigval, method 2 (lanczos.c:764-996).  The inverse
 // iterations of the candidates run in parallel; the acceptance pass then
 // walks the candidates in ascending order exactly as the reference does.
-static void check_window(int it, const double *al, const double *be, double emin,
-                         double emax, double tol, double res, std::vector<double> &conv,
-                         std::vector<int> &conv_it, unsigned long long seed) {
+void check_window(int it, const double *al, const double *be, double emin, double emax,
+                  double tol, double res, std::vector<double> &conv, std::vector<int> &conv_it,
+                  unsigned long long seed) {
   const std::vector<double> ev = tri_eigs(it, al, be, emin, emax);
   const int ne = int(ev.size());
   std::vector<char> cand(ne, 0), ok(ne, 0);
@@ -325,10 +301,8 @@ static int spmv_step(Ctx &c, const double2 *x, double2 *y, const double *bet, in
 }
 static int spmv_step(Ctx &c, const float2 *x, float2 *y, const double *bet, int it,
                      double *alpha, cudaStream_t s) {
-  const float *X = reinterpret_cast<const float *>(x);
-  float *Y = reinterpret_cast<float *>(y);
-  if (c.recompute) return launch_spmv_recompute_f32(c, X, Y, 0.0, bet, it, alpha, it, s);
-  return launch_spmv_async_f32(c, X, Y, 0.0, bet, it, alpha, it, s);
+  return launch_spmv_f32(c, reinterpret_cast<const float *>(x), reinterpret_cast<float *>(y), 0.0,
+                         bet, it, alpha, it, s);
 }
 
 template <typename VT>
@@ -606,7 +580,11 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
     c.stats.vectors_ms = ms;
     if (kMixed) {  // double-precision Rayleigh-Ritz of the Ritz vectors
       cudaEventRecord(tm.t2, s);
-      SOLVE_RC(refine_ritz(c, V_dev, nvec, values, c.state_resid, c.state_delta, s));
+      c.state_resid.assign(nvec, 0.0);
+      c.state_delta.assign(nvec, 0.0);
+      const long off = 0;
+      SOLVE_RC(refine_ritz(c, V_dev, nvec, n2, 1, &off, &n2, values, c.state_resid.data(),
+                           c.state_delta.data(), s));
       cudaEventRecord(tm.t3, s);
       SOLVE_CUDA(cudaStreamSynchronize(s));
       cudaEventElapsedTime(&ms, tm.t2, tm.t3);

@@ -16,38 +16,55 @@
 
 namespace tbgpu {
 
-__device__ __forceinline__ double2 cmul_r(double v, double2 a) { return make_double2(v * a.x, v * a.y); }
-__device__ __forceinline__ void cfma_r(double2 &acc, double v, double2 a) {
+template <typename T, typename V>
+__device__ __forceinline__ V cmul_r(T v, V a) {
+  V r;
+  r.x = v * a.x;
+  r.y = v * a.y;
+  return r;
+}
+template <typename T, typename V>
+__device__ __forceinline__ void cfma_r(V &acc, T v, V a) {
   acc.x = fma(v, a.x, acc.x);
   acc.y = fma(v, a.y, acc.y);
 }
 // acc += (i*lambda) * a
-__device__ __forceinline__ void cfma_i(double2 &acc, double lam, double2 a) {
+template <typename T, typename V>
+__device__ __forceinline__ void cfma_i(V &acc, T lam, V a) {
   acc.x -= lam * a.y;
   acc.y += lam * a.x;
+}
+template <typename V> __device__ __forceinline__ V vzero() {
+  V r;
+  r.x = r.y = 0;
+  return r;
 }
 
 // PHASE: bonds carry the Bloch phase phase[a*4+n] of H[a][nbr] (periodic
 // structures away from the Gamma point).
 // HT: element type of the stored Hamiltonian (double, or float for the
-// single-precision store; the arithmetic stays double).
-template <int NORB, int NSPIN, int WPB, bool DOT, bool PHASE = false, typename HT = double>
+// single-precision store); VT: vector element, double2 (arithmetic in double)
+// or float2 (the mixed-precision solve: float arithmetic, alpha in double).
+template <int NORB, int NSPIN, int WPB, bool DOT, bool PHASE = false, typename HT = double,
+          typename VT = double2>
 __global__ void __launch_bounds__(WPB * 32)
     k_spmv(long natoms, const int4 *__restrict__ nbr, const unsigned char *__restrict__ site_m,
            const HT *__restrict__ onsite, const HT *__restrict__ blocks,
-           const double2 *__restrict__ x, double2 *__restrict__ y, double shift,
+           const VT *__restrict__ x, VT *__restrict__ y, double shift_d,
            const double *__restrict__ xnorm, int xnorm_idx, double *partial,
            unsigned int *counter, double *alpha_out, int alpha_idx,
            const double2 *__restrict__ phase = nullptr) {
+  using RT = decltype(VT::x);
   constexpr int NB = NORB * NSPIN;
   constexpr int APW = 32 / NORB;
   constexpr int ONS = onsite_len(NB);
-  __shared__ double2 xs[WPB][APW][5][NB];  // slots 0..3 neighbours, 4 own
+  __shared__ VT xs[WPB][APW][5][NB];  // slots 0..3 neighbours, 4 own
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int ai = lane / NORB, o = lane - ai * NORB;
   const long a = (long(blockIdx.x) * WPB + w) * APW + ai;
   const bool act = ai < APW && a < natoms;
-  const double scale = xnorm ? 1.0 / xnorm[xnorm_idx] : 1.0;
+  const RT scale = RT(xnorm ? 1.0 / xnorm[xnorm_idx] : 1.0);
+  const RT shift = RT(shift_d);
   int nb[4] = {-1, -1, -1, -1};
   int m = 0;
   if (act) {
@@ -60,21 +77,21 @@ __global__ void __launch_bounds__(WPB * 32)
       xs[w][ai][4][e] = cmul_r(scale, x[a * NB + e]);
 #pragma unroll
       for (int n = 0; n < 4; n++)
-        xs[w][ai][n][e] = nb[n] >= 0 ? cmul_r(scale, x[long(nb[n]) * NB + e]) : make_double2(0, 0);
+        xs[w][ai][n][e] = nb[n] >= 0 ? cmul_r(scale, x[long(nb[n]) * NB + e]) : vzero<VT>();
     }
   }
   __syncwarp();
   double dot = 0.0;
   if (act) {
     const HT *rec = onsite + a * ONS;
-    double2 acc[NSPIN];
+    VT acc[NSPIN];
 #pragma unroll
-    for (int s = 0; s < NSPIN; s++) acc[s] = cmul_r(double(rec[s * NORB + o]), xs[w][ai][4][s * NORB + o]);
+    for (int s = 0; s < NSPIN; s++) acc[s] = cmul_r(RT(rec[s * NORB + o]), xs[w][ai][4][s * NORB + o]);
     // dangling-bond sp3 couplings among s, px, py, pz (surface atoms only)
     if (o >= 1 && o <= 4 && rec[NB + 1] != HT(0)) {
-      const double sx = rec[NB + 2], sy = rec[NB + 3], sz = rec[NB + 4];
-      const double xy = rec[NB + 5], xz = rec[NB + 6], yz = rec[NB + 7];
-      double c1, c2, c3;
+      const RT sx = rec[NB + 2], sy = rec[NB + 3], sz = rec[NB + 4];
+      const RT xy = rec[NB + 5], xz = rec[NB + 6], yz = rec[NB + 7];
+      RT c1, c2, c3;
       int k1, k2, k3;
       if (o == 1) { c1 = sx; k1 = 2; c2 = sy; k2 = 3; c3 = sz; k3 = 4; }
       else if (o == 2) { c1 = sx; k1 = 1; c2 = xy; k2 = 3; c3 = xz; k3 = 4; }
@@ -89,8 +106,8 @@ __global__ void __launch_bounds__(WPB * 32)
     }
     // on-site spin-orbit (mb_ham_spds_so.h), p orbitals 2,3,4 of both spins
     if (NSPIN == 2 && o >= 2 && o <= 4) {
-      const double L = rec[NB];
-      const double2 *U = xs[w][ai][4], *D = xs[w][ai][4] + NORB;
+      const RT L = rec[NB];
+      const VT *U = xs[w][ai][4], *D = xs[w][ai][4] + NORB;
       if (o == 2) {
         cfma_i(acc[0], -L, U[3]); cfma_r(acc[0], L, D[4]);
         cfma_i(acc[1], L, D[3]);  cfma_r(acc[1], -L, U[4]);
@@ -107,18 +124,18 @@ __global__ void __launch_bounds__(WPB * 32)
 #pragma unroll
     for (int n = 0; n < 4; n++) {
       if (nb[n] < 0) continue;
-      const double2 *xn = xs[w][ai][n];
+      const VT *xn = xs[w][ai][n];
       // with phases, the bond's product is formed apart and then rotated
-      double2 part[NSPIN];
-      double2 *tgt = acc;
+      VT part[NSPIN];
+      VT *tgt = acc;
       if (PHASE) {
 #pragma unroll
-        for (int s = 0; s < NSPIN; s++) part[s] = make_double2(0.0, 0.0);
+        for (int s = 0; s < NSPIN; s++) part[s] = vzero<VT>();
         tgt = part;
       }
       if (cat) {
         const HT *M = blocks + (a * 4 + n) * (NORB * NORB) + o * NORB;
-        double r[NORB];
+        RT r[NORB];
         if constexpr (NORB % 2 == 0 && sizeof(HT) == 8) {
           // rows start on 16-byte boundaries when NORB is even (block = NORB^2
           // doubles, row = NORB doubles): 128-bit loads
@@ -140,7 +157,7 @@ __global__ void __launch_bounds__(WPB * 32)
         const HT *M = blocks + (long(nb[n]) * 4 + c_rev_slot[m][n]) * (NORB * NORB) + o;
 #pragma unroll
         for (int k = 0; k < NORB; k++) {
-          const double v = double(__ldg(M + k * NORB));
+          const RT v = RT(__ldg(M + k * NORB));
 #pragma unroll
           for (int s = 0; s < NSPIN; s++) cfma_r(tgt[s], v, xn[s * NORB + k]);
         }
@@ -149,17 +166,19 @@ __global__ void __launch_bounds__(WPB * 32)
         const double2 ph = __ldg(phase + a * 4 + n);
 #pragma unroll
         for (int s = 0; s < NSPIN; s++) {
-          acc[s].x += ph.x * part[s].x - ph.y * part[s].y;
-          acc[s].y += ph.x * part[s].y + ph.y * part[s].x;
+          acc[s].x += RT(ph.x) * part[s].x - RT(ph.y) * part[s].y;
+          acc[s].y += RT(ph.x) * part[s].y + RT(ph.y) * part[s].x;
         }
       }
     }
 #pragma unroll
     for (int s = 0; s < NSPIN; s++) {
-      const double2 xo = xs[w][ai][4][s * NORB + o];
-      double2 out = make_double2(acc[s].x - shift * xo.x, acc[s].y - shift * xo.y);
+      const VT xo = xs[w][ai][4][s * NORB + o];
+      VT out;
+      out.x = acc[s].x - shift * xo.x;
+      out.y = acc[s].y - shift * xo.y;
       y[a * NB + s * NORB + o] = out;
-      dot += xo.x * out.x + xo.y * out.y;
+      dot += double(xo.x) * double(out.x) + double(xo.y) * double(out.y);
     }
   }
   if (DOT) grid_reduce<WPB * 32>(dot, partial, counter, alpha_out, alpha_idx, false);
@@ -167,34 +186,34 @@ __global__ void __launch_bounds__(WPB * 32)
 
 constexpr int kWPB = 8;
 
-template <int NORB, int NSPIN, typename HT>
-static int launch_ht(Ctx &c, const double *x, double *y, double shift,
+template <int NORB, int NSPIN, typename HT, typename VT = double2>
+static int launch_ht(Ctx &c, const void *x, void *y, double shift,
                      const double *xnorm, int xidx, double *alpha_out, int aidx,
                      cudaStream_t s) {
   constexpr int APW = 32 / NORB;
   const long per_block = long(kWPB) * APW;
   const unsigned grid = unsigned((c.natoms + per_block - 1) / per_block);
-  const double2 *X = reinterpret_cast<const double2 *>(x);
-  double2 *Y = reinterpret_cast<double2 *>(y);
+  const VT *X = reinterpret_cast<const VT *>(x);
+  VT *Y = reinterpret_cast<VT *>(y);
   const HT *ons = ham_onsite<HT>(c), *blk = ham_blocks<HT>(c);
   if (alpha_out) {
     int rc = ensure_partials(c, int(grid));
     if (rc) return rc;
     if (c.bloch)
-      k_spmv<NORB, NSPIN, kWPB, true, true, HT><<<grid, kWPB * 32, 0, s>>>(
+      k_spmv<NORB, NSPIN, kWPB, true, true, HT, VT><<<grid, kWPB * 32, 0, s>>>(
           c.natoms, c.d_nbr, c.d_site_m, ons, blk, X, Y, shift, xnorm, xidx, c.d_partial,
           c.d_counter, alpha_out, aidx, c.d_phase);
     else
-      k_spmv<NORB, NSPIN, kWPB, true, false, HT><<<grid, kWPB * 32, 0, s>>>(
+      k_spmv<NORB, NSPIN, kWPB, true, false, HT, VT><<<grid, kWPB * 32, 0, s>>>(
           c.natoms, c.d_nbr, c.d_site_m, ons, blk, X, Y, shift, xnorm, xidx, c.d_partial,
           c.d_counter, alpha_out, aidx);
   } else {
     if (c.bloch)
-      k_spmv<NORB, NSPIN, kWPB, false, true, HT><<<grid, kWPB * 32, 0, s>>>(
+      k_spmv<NORB, NSPIN, kWPB, false, true, HT, VT><<<grid, kWPB * 32, 0, s>>>(
           c.natoms, c.d_nbr, c.d_site_m, ons, blk, X, Y, shift, xnorm, xidx, nullptr, nullptr,
           nullptr, 0, c.d_phase);
     else
-      k_spmv<NORB, NSPIN, kWPB, false, false, HT><<<grid, kWPB * 32, 0, s>>>(
+      k_spmv<NORB, NSPIN, kWPB, false, false, HT, VT><<<grid, kWPB * 32, 0, s>>>(
           c.natoms, c.d_nbr, c.d_site_m, ons, blk, X, Y, shift, xnorm, xidx, nullptr, nullptr,
           nullptr, 0);
   }
@@ -223,6 +242,21 @@ int launch_spmv(Ctx &c, const double *x, double *y, double shift, const double *
   if (c.norb == 5 && c.nspin == 2) return launch_t<5, 2>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
   if (c.norb == 5 && c.nspin == 1) return launch_t<5, 1>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
   return set_error(TBGPU_E_UNSUPPORTED);
+}
+
+// The mixed-precision product on complex-float vectors: recomputed in float,
+// or over the float store (the warp-staged kernel for 10 orbitals, the
+// lane-gather kernel for 5); at the Gamma point.
+int launch_spmv_f32(Ctx &c, const float *x, float *y, double shift, const double *xnorm,
+                    int xidx, double *alpha_out, int aidx, cudaStream_t s) {
+  if (c.bloch) return set_error(TBGPU_E_UNSUPPORTED);
+  if (c.recompute)
+    return launch_spmv_recompute_f32(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
+  if (!c.ham_fp32) return set_error(TBGPU_E_UNSUPPORTED);
+  if (c.norb == 10) return launch_spmv_async_f32(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
+  if (c.nspin == 2)
+    return launch_ht<5, 2, float, float2>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
+  return launch_ht<5, 1, float, float2>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
 }
 
 template <int NORB, int NSPIN, typename HT>

@@ -150,6 +150,8 @@ int launch_spmv_recompute(Ctx &c, const double *x, double *y, double shift,
 int launch_spmv(Ctx &c, const double *x, double *y, double shift,
                 const double *xscale_dev, int scale_index, double *alpha_out,
                 int alpha_index, cudaStream_t s);
+int launch_spmv_f32(Ctx &c, const float *x, float *y, double shift, const double *xscale_dev,
+                    int scale_index, double *alpha_out, int alpha_index, cudaStream_t s);
 // spmv_async.cu
 int launch_spmv_async(Ctx &c, const double *x, double *y, double shift,
                       const double *xscale_dev, int scale_index, double *alpha_out,
@@ -171,8 +173,24 @@ struct SolveArgs {
 };
 int solve(Ctx &c, const SolveArgs &A, const double *r0_dev, double *values, int *conv_iters,
           int *iterations, double *V_dev, int maxvec);
+// lanczos.cu host pieces shared with the batched solve
+struct Rng {  // uniform [0,1] starts for inverse iteration
+  unsigned long long s;
+  double next() {
+    s = s * 6364136223846793005ULL + 1442695040888963407ULL;
+    return double(s >> 11) * (1.0 / 9007199254740992.0);
+  }
+};
+bool inverse_iteration(int m, const double *d, const double *e, double lambda, Rng &rng,
+                       std::vector<double> &x);
+void check_window(int it, const double *al, const double *be, double emin, double emax,
+                  double tol, double res, std::vector<double> &conv, std::vector<int> &conv_it,
+                  unsigned long long seed);
 // blk_lanczos.cu: double-precision Rayleigh-Ritz of nvec eigenvectors
-int refine_ritz(Ctx &c, double *V_dev, int nvec, double *values, std::vector<double> &resid,
-                std::vector<double> &delta, cudaStream_t s);
+// (vector e at V_dev + 2*e*stride doubles) over nseg independent segments
+// [seg_off, seg_off + seg_len); values/resid/delta are [nseg][nvec]
+int refine_ritz(Ctx &c, double *V_dev, int nvec, long stride, int nseg, const long *seg_off,
+                const long *seg_len, double *values, double *resid, double *delta,
+                cudaStream_t s, const int *seg_nvec = nullptr);
 
 }  // namespace tbgpu

@@ -75,6 +75,8 @@ def _lib():
         L.tbgpu_get_state_errors.argtypes = [vp, ip, vp, vp]
         L.tbgpu_hx_dev_f32.argtypes = [vp, dp, vp, vp]
         L.tbgpu_momentum_matrix.argtypes = [vp, ip, vp, vp, vp, vp]
+        L.tbgpu_eigensolve_lanczos_batched.argtypes = [vp, ip, vp, ip, ip, ip, ip, ip, vp, vp,
+                                                       vp, vp, dp, vp, vp, ip, vp, vp, vp, ip]
         L.tbgpu_vff_energy.argtypes = [vp, vp, vp, vp]
         L.tbgpu_vff_relax.argtypes = [vp, vp, ip, ip, dp, ip, vp, vp, vp]
         L.tbgpu_write_eigenvalues.argtypes = [C.c_char_p, C.c_char, vp, ip, vp]
@@ -302,6 +304,44 @@ class Hamiltonian:
         if vectors:
             k = min(ne, vectors)
             v = V[:k].reshape(k, self.n, 2)
+            out["vectors"] = v[..., 0] + 1j * v[..., 1]
+        return out
+
+    def eigensolve_lanczos_batched(self, r_0, dot_cells, emin1, emax1, emin2, emax2,
+                                   ConvCheckStartIter=200, ConvCheckSkipRate=50, imax=2400,
+                                   requested1=1, requested2=1, tolerance=1e-7, vectors=0,
+                                   values_stride=None):
+        """Lanczos for the dots of a packed structure (``workloads.pack_dots``):
+        ``dot_cells`` the cell boundaries along x, windows per dot (arrays, or
+        scalars for all).  ``r_0``: host start vector (2*dimension doubles) or a
+        CUDA tensor.  Returns a dict with ``values`` (list per dot, ascending),
+        ``iterations`` per dot and, with ``vectors`` > 0, ``vectors``
+        ([vectors, dimension] complex, the packed layout)."""
+        import torch
+        nd = len(dot_cells) - 1
+        cells = np.ascontiguousarray(dot_cells, np.int32)
+        win = [np.ascontiguousarray(np.broadcast_to(np.asarray(v, np.float64), (nd,)))
+               for v in (emin1, emax1, emin2, emax2)]
+        if isinstance(r_0, torch.Tensor) and r_0.is_cuda:
+            r0 = r_0.contiguous()
+        else:
+            r0 = torch.from_numpy(np.ascontiguousarray(r_0, np.float64)).cuda()
+        vs = values_stride or (requested1 + requested2 + 16)
+        vals = np.zeros(nd * vs)
+        found = np.zeros(nd, np.int32)
+        its = np.zeros(nd, np.int32)
+        V = torch.zeros(vectors * 2 * self.n, dtype=torch.float64, device="cuda") if vectors else None
+        rc = _lib().tbgpu_eigensolve_lanczos_batched(
+            self._ctx, nd, _p(cells), ConvCheckStartIter, ConvCheckSkipRate, imax, requested1,
+            requested2, _p(win[0]), _p(win[1]), _p(win[2]), _p(win[3]), tolerance,
+            C.c_void_p(r0.data_ptr()), _p(vals), vs, _p(found), _p(its),
+            C.c_void_p(V.data_ptr()) if V is not None else None, int(vectors))
+        if rc < 0:
+            raise TbgpuError(rc, "tbgpu_eigensolve_lanczos_batched")
+        out = dict(values=[vals[d * vs:d * vs + found[d]].copy() for d in range(nd)],
+                   iterations=its.copy())
+        if vectors:
+            v = V.cpu().numpy().reshape(vectors, self.n, 2)
             out["vectors"] = v[..., 0] + 1j * v[..., 1]
         return out
 

@@ -114,3 +114,47 @@ def random_start(n_complex: int, seed: int = 0) -> np.ndarray:
     """Start vector with real and imaginary parts uniform in [-1, 1]."""
     rng = np.random.default_rng(seed)
     return rng.uniform(-1.0, 1.0, size=2 * n_complex)
+
+
+def alloy_dot(natoms: int, x_in: float, seed: int = 0, a: float = A_GAAS) -> Structure:
+    """Free-standing In(x)Ga(1-x)As nanocrystal of about ``natoms`` atoms: a
+    box of cells as close to a cube as the count allows, every cation site In
+    with probability ``x_in`` (independent per site, seeded), anions As; the
+    surface is passivated by the Hamiltonian's dangling-bond shift."""
+    ncell = max(1, int(round(natoms / 8)))
+    n = max(1, int(round(ncell ** (1.0 / 3.0))))
+    nz = max(1, int(round(ncell / (n * n))))
+    rng = np.random.default_rng(seed)
+    t = _binary(n, n, nz)
+    t[..., :4] = np.where(rng.random((n, n, nz, 4)) < x_in, SPECIES["In"], SPECIES["Ga"])
+    return Structure(n, n, nz, (a, a, a), (False, False, False), t, None,
+                     f"InGaAs_dot_{n}x{n}x{nz}", dict(x_in=x_in, seed=seed))
+
+
+def pack_dots(dots, gap: int = 1):
+    """Place dots side by side along x in one grid, ``gap`` empty cells apart,
+    so that no bond joins two of them (the Hamiltonian of the packed grid is
+    block diagonal).  All dots must share the lattice constants.  Returns the
+    packed structure and the cell boundaries along x ([ndots + 1]): dot d owns
+    cells [bounds[d], bounds[d + 1]), its trailing gap included."""
+    lat = dots[0].lattice
+    if any(tuple(d.lattice) != tuple(lat) for d in dots):
+        raise ValueError("packed dots must share the lattice constants")
+    ny = max(d.ny for d in dots)
+    nz = max(d.nz for d in dots)
+    nx = sum(d.nx + gap for d in dots)
+    t = np.zeros((nx, ny, nz, 8), np.uint8)
+    dsp = None
+    if any(d.dsp is not None for d in dots):
+        dsp = np.zeros((nx, ny, nz, 8, 3))
+    bounds = [0]
+    x0 = 0
+    for d in dots:
+        t[x0:x0 + d.nx, :d.ny, :d.nz] = d.types
+        if dsp is not None and d.dsp is not None:
+            dsp[x0:x0 + d.nx, :d.ny, :d.nz] = d.dsp
+        x0 += d.nx + gap
+        bounds.append(x0)
+    st = Structure(nx, ny, nz, tuple(lat), (False, False, False), t, dsp,
+                   f"packed_{len(dots)}_dots", dict(ndots=len(dots)))
+    return st, np.asarray(bounds, np.int32)

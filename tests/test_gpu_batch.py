@@ -1,0 +1,112 @@
+"""Batched Lanczos over packed dots (tbgpu_eigensolve_lanczos_batched).
+
+Bars: every dot of a packed batch gives the eigenvalues (within 1e-9 eV), the
+iteration count (to one check interval) and the eigenvectors
+(|<v_batch, v_alone>| within 1e-8 of 1) of the same dot solved alone with its
+segment of the start vector; the
+mixed-precision batch refines each dot's states to within 1e-6 eV of the
+FP64 batch, the error printed per state; packings whose dots touch, and
+boundaries outside the grid, are refused.
+"""
+import numpy as np
+import pytest
+
+from nemo3d_b200 import materials, workloads
+
+pytestmark = pytest.mark.gpu
+
+SPS = ["GaAs_sps", "InAs_sps"]
+SPDS = ["GaAs_spds", "InAs_spds"]
+KW = dict(ConvCheckStartIter=100, ConvCheckSkipRate=50, imax=4000, requested1=1,
+          requested2=2, tolerance=1e-7)
+
+
+def _dots():
+    sizes, xs = [300, 900, 500, 1500], [0.5, 0.9, 0.7, 0.6]
+    return [workloads.alloy_dot(n, x, seed=i) for i, (n, x) in enumerate(zip(sizes, xs))]
+
+
+def _windows(nd):
+    return dict(emin1=np.full(nd, -0.8), emax1=np.full(nd, 0.4), emin2=np.full(nd, 1.0),
+                emax2=np.full(nd, 3.5))
+
+
+@pytest.mark.parametrize("model,fam", [("sp3s*_so", SPS), ("sp3d5s*_so", SPDS)])
+def test_batch_matches_dots_alone(model, fam):
+    from nemo3d_b200.tbgpu import Hamiltonian
+    dots = _dots()
+    mats = [materials.MATERIALS[m] for m in fam]
+    packed, cells = workloads.pack_dots(dots)
+    gb = Hamiltonian(packed, model, mats)
+    singles = [Hamiltonian(d, model, mats) for d in dots]
+    starts = [workloads.random_start(g.n, seed=10 + i) for i, g in enumerate(singles)]
+    r0 = np.concatenate(starts)
+    assert r0.size == 2 * gb.n
+    win = _windows(len(dots))
+    res = gb.eigensolve_lanczos_batched(r0, cells, vectors=3, **win, **KW)
+    off = 0
+    for d, (g, st0) in enumerate(zip(singles, starts)):
+        alone = g.eigensolve_lanczos(st0, emin1=-0.8, emax1=0.4, emin2=1.0, emax2=3.5,
+                                     vectors=3, **KW)
+        vb, va = res["values"][d], alone["values"]
+        # alpha is formed from the unnormalised product here (<r, Hr>/beta^2),
+        # so T differs by rounding and a borderline check may pass one
+        # interval apart, accepting a value more or less
+        assert abs(res["iterations"][d] - alone["iterations"]) <= KW["ConvCheckSkipRate"]
+        if res["iterations"][d] == alone["iterations"]:
+            assert len(vb) == len(va) >= 3
+            assert np.abs(vb - va).max() < 1e-9, d
+        else:
+            short, long_ = (vb, va) if len(vb) <= len(va) else (va, vb)
+            assert len(short) >= 3 and len(long_) - len(short) <= 2
+            assert all(np.abs(long_ - v).min() < 1e-9 for v in short), d
+        for e in range(3):  # the states both runs hold (the lowest ones)
+            if abs(vb[e] - va[e]) > 1e-9:
+                continue
+            seg = res["vectors"][e][off:off + g.n]
+            ov = abs(np.vdot(seg, alone["vectors"][e]))
+            assert abs(ov - 1.0) < 1e-8, (d, e, ov)
+        off += g.n
+
+
+def test_mixed_batch_per_state():
+    from nemo3d_b200.tbgpu import Hamiltonian
+    dots = _dots()
+    mats = [materials.MATERIALS[m] for m in SPS]
+    packed, cells = workloads.pack_dots(dots)
+    r0 = workloads.random_start(Hamiltonian(packed, "sp3s*_so", mats).n, seed=3)
+    nd = len(dots)
+    ref = Hamiltonian(packed, "sp3s*_so", mats).eigensolve_lanczos_batched(
+        r0, cells, **_windows(nd), **KW)
+    # one window per dot around its lowest conduction state of the FP64 run
+    e1 = np.array([v[v > 1.0].min() for v in ref["values"]])
+    kw = dict(KW, requested1=0, requested2=1)
+    for opts in (dict(ham_bits=32), dict(recompute=True)):
+        gm = Hamiltonian(packed, "sp3s*_so", mats, lanczos_bits=32, **opts)
+        mix = gm.eigensolve_lanczos_batched(r0, cells, emin1=np.zeros(nd), emax1=np.zeros(nd),
+                                            emin2=e1 - 2e-3, emax2=e1 + 2e-3, vectors=1, **kw)
+        got = np.array([v[0] for v in mix["values"]])
+        resid, delta = gm.state_errors()
+        err = np.abs(got - e1)
+        print(opts, "mixed batch error per dot (eV):", err, "residual:", resid)
+        assert err.max() < 1e-6
+        assert resid.max() < 1e-3
+
+
+def test_batch_refusals():
+    from nemo3d_b200 import tbgpu
+    dots = _dots()[:2]
+    mats = [materials.MATERIALS[m] for m in SPS]
+    packed, cells = workloads.pack_dots(dots, gap=0)  # touching dots
+    g = tbgpu.Hamiltonian(packed, "sp3s*_so", mats)
+    r0 = workloads.random_start(g.n, seed=1)
+    with pytest.raises(tbgpu.TbgpuError) as e:
+        g.eigensolve_lanczos_batched(r0, cells, **_windows(2), **KW)
+    assert e.value.code == -1
+    packed, cells = workloads.pack_dots(dots)
+    g = tbgpu.Hamiltonian(packed, "sp3s*_so", mats)
+    bad = cells.copy()
+    bad[-1] = packed.nx + 3
+    with pytest.raises(tbgpu.TbgpuError) as e:
+        g.eigensolve_lanczos_batched(workloads.random_start(g.n, seed=1), bad, **_windows(2), **KW)
+    assert e.value.code == -1
