@@ -139,9 +139,9 @@ int tbgpu_set_ham_storage(tbgpu_ctx *ctx, int recompute);
 /* Precision of the Lanczos vectors, set before tbgpu_build_hamiltonian: 64
  * (default) or 32.  32 is the mixed-precision solve (no counterpart in the
  * reference): it runs on the 32-bit store, tbgpu_set_ham_precision(ctx, 32),
- * with a 10-orbital model, or on the recompute storage,
- * tbgpu_set_ham_storage(ctx, 1), with any model (float Slater-Koster
- * elements from double geometry), else TBGPU_E_UNSUPPORTED at build.  The
+ * or on the recompute storage, tbgpu_set_ham_storage(ctx, 1) (float
+ * Slater-Koster elements from double geometry), with any model; else
+ * TBGPU_E_UNSUPPORTED at build.  The
  * recurrence vectors are complex float and H*x accumulates in float, while
  * alpha, beta, their reductions, the tridiagonal eigenvalues, the
  * convergence test and the eigenvector accumulation stay double.  The
@@ -176,10 +176,9 @@ int tbgpu_hx_dev(tbgpu_ctx *ctx, double shift, const double *x_dev,
 
 /* The mixed-precision product: y = (H - shift) x on complex-float device
  * vectors ({float re, im} per entry), accumulated in float, over the 32-bit
- * store (10-orbital models) or recomputed in float (recompute storage, any
- * model): the H*x of a tbgpu_set_lanczos_precision(ctx, 32) solve; no
- * counterpart in the reference.  At the Gamma point only; else
- * TBGPU_E_UNSUPPORTED. */
+ * store or recomputed in float (recompute storage), any model: the H*x of
+ * a tbgpu_set_lanczos_precision(ctx, 32) solve; no counterpart in the
+ * reference.  At the Gamma point only; else TBGPU_E_UNSUPPORTED. */
 int tbgpu_hx_dev_f32(tbgpu_ctx *ctx, double shift, const float *x_dev, float *y_dev);
 
 /* Y_v = (H - shift) X_v for a block of p <= 8 device vectors stored one

@@ -23,6 +23,7 @@
 // deterministic: a block covers part of one dot, writes its partial, and the
 // last block of that dot sums the dot's partials in block order.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <numeric>
 #include <vector>
@@ -116,8 +117,9 @@ template <typename VT>
 __global__ void __launch_bounds__(kBT)
     k_balpha(Seg S, const VT *__restrict__ r, const VT *__restrict__ w, const double *bet,
              double *alpha, long sa, long sb, const int *itp, double *partial,
-             unsigned *counters) {
+             unsigned *counters, const unsigned char *__restrict__ done) {
   const int d = S.blk_dot[blockIdx.x];
+  if (done[d]) return;  // a converged dot: every block of it leaves
   const int it = *itp;
   double s = 0.0;
   for (long j = S.blk_lo[blockIdx.x] + threadIdx.x; j < S.blk_hi[blockIdx.x]; j += kBT) {
@@ -137,8 +139,10 @@ template <typename VT>
 __global__ void __launch_bounds__(kBT)
     k_bupdate(Seg S, const VT *__restrict__ w, const VT *__restrict__ rc,
               const VT *__restrict__ rp, VT *__restrict__ rout, const double *alpha, double *bet,
-              long sa, long sb, const int *itp, double *partial, unsigned *counters) {
+              long sa, long sb, const int *itp, double *partial, unsigned *counters,
+              const unsigned char *__restrict__ done) {
   const int d = S.blk_dot[blockIdx.x];
+  if (done[d]) return;
   const int it = *itp;
   const double al = alpha[d * sa + it], bprev = bet[d * sb + it];
   const double iq = 1.0 / bprev;
@@ -163,6 +167,14 @@ __global__ void __launch_bounds__(kBT)
 }
 
 __global__ void k_badvance(int *itp) { *itp += 1; }
+
+// leave dot d out of the products and updates from here on
+__global__ void k_bmark(long lo, long hi, int d, unsigned char *skip, unsigned char *done) {
+  for (long a = lo + blockIdx.x * (long)blockDim.x + threadIdx.x; a < hi;
+       a += (long)gridDim.x * blockDim.x)
+    skip[a] = 1;
+  if (blockIdx.x == 0 && threadIdx.x == 0) done[d] = 1;
+}
 
 template <typename VT>
 struct RingPtrs {
@@ -301,7 +313,8 @@ static int solve_batch_t(Ctx &c, int ndots, const int *dot_cells, const BatchArg
       S1 = k;
       break;
     }
-  const bool use_graph = A.conv_skip % S1 == 0;
+  // graphs need a stream that can be captured: not the legacy default stream
+  bool use_graph = A.conv_skip % S1 == 0 && s != nullptr;
   std::vector<VT *> ring(std::max(S1, kMaxK + 1), nullptr);
   VT *W = nullptr;
   int *d_blk_dot = nullptr, *d_dot_blk0 = nullptr, *d_it = nullptr;
@@ -309,10 +322,14 @@ static int solve_batch_t(Ctx &c, int ndots, const int *dot_cells, const BatchArg
   double *d_alpha = nullptr, *d_bet = nullptr, *d_tmp = nullptr, *d_part = nullptr;
   double *d_coef = nullptr, *h_alpha = nullptr, *h_bet = nullptr;
   unsigned *d_cnt = nullptr;
+  unsigned char *d_skip = nullptr, *d_done = nullptr;
   cudaGraphExec_t gexec = nullptr;
   cudaGraph_t graph = nullptr;
   auto cleanup = [&]() {
     cudaStreamSynchronize(s);
+    c.d_skip = nullptr;
+    cudaFree(d_skip);
+    cudaFree(d_done);
     if (gexec) cudaGraphExecDestroy(gexec);
     if (graph) cudaGraphDestroy(graph);
     for (auto p : ring) if (p) cudaFree(p);
@@ -350,8 +367,18 @@ static int solve_batch_t(Ctx &c, int ndots, const int *dot_cells, const BatchArg
   B_CUDA(cudaMalloc(&d_tmp, sizeof(double) * ndots));
   B_CUDA(cudaMalloc(&d_part, sizeof(double) * nblk));
   B_CUDA(cudaMalloc(&d_cnt, sizeof(unsigned) * ndots));
-  B_CUDA(cudaMallocHost(&h_alpha, sizeof(double) * SA * ndots));
-  B_CUDA(cudaMallocHost(&h_bet, sizeof(double) * SB * ndots));
+  // converged dots drop out of the products (per-atom mask) and of the
+  // segmented updates (per-dot flag)
+  B_CUDA(cudaMalloc(&d_skip, c.natoms));
+  B_CUDA(cudaMalloc(&d_done, ndots));
+  B_CUDA(cudaMemsetAsync(d_skip, 0, c.natoms, s));
+  B_CUDA(cudaMemsetAsync(d_done, 0, ndots, s));
+  c.d_skip = d_skip;
+  // pinned copies of alpha and beta, one slot per check in flight
+  constexpr int kAhead = 2;
+  constexpr int kSlots = kAhead + 1;
+  B_CUDA(cudaMallocHost(&h_alpha, sizeof(double) * SA * ndots * kSlots));
+  B_CUDA(cudaMallocHost(&h_bet, sizeof(double) * SB * ndots * kSlots));
   B_CUDA(cudaMemcpyAsync(d_blk_dot, bdot.data(), sizeof(int) * nblk, cudaMemcpyHostToDevice, s));
   B_CUDA(cudaMemcpyAsync(d_dot_blk0, dblk0.data(), sizeof(int) * (ndots + 1),
                          cudaMemcpyHostToDevice, s));
@@ -375,10 +402,18 @@ static int solve_batch_t(Ctx &c, int ndots, const int *dot_cells, const BatchArg
     VT *rc_ = ring[it % S], *rp_ = ring[(it + S - 1) % S], *ro = ring[(it + 1) % S];
     int r_ = hx_plain(c, rc_, W, s);
     if (r_) return r_;
-    k_balpha<VT><<<nblk, kBT, 0, s>>>(SG, rc_, W, d_bet, d_alpha, SA, SB, d_it, d_part, d_cnt);
+    k_balpha<VT><<<nblk, kBT, 0, s>>>(SG, rc_, W, d_bet, d_alpha, SA, SB, d_it, d_part, d_cnt,
+                                      d_done);
     k_bupdate<VT><<<nblk, kBT, 0, s>>>(SG, W, rc_, rp_, ro, d_alpha, d_bet, SA, SB, d_it, d_part,
-                                       d_cnt);
+                                       d_cnt, d_done);
     k_badvance<<<1, 1, 0, s>>>(d_it);
+    return cudaGetLastError() == cudaSuccess ? TBGPU_OK : set_error(TBGPU_E_CUDA);
+  };
+
+  auto mark = [&](int d) -> int {
+    const long n = a0[d + 1] - a0[d];
+    k_bmark<<<unsigned(std::max<long>(1, std::min<long>((n + 255) / 256, 1024))), 256, 0, s>>>(
+        a0[d], a0[d + 1], d, d_skip, d_done);
     return cudaGetLastError() == cudaSuccess ? TBGPU_OK : set_error(TBGPU_E_CUDA);
   };
 
@@ -400,8 +435,11 @@ static int solve_batch_t(Ctx &c, int ndots, const int *dot_cells, const BatchArg
       if (use_graph && launched > 0 && lim - launched >= A.conv_skip &&
           (launched % S1) == (checks.empty() ? 1 : checks[0] % S1)) {
         if (!gexec) {  // capture one check interval, starting on this ring slot
-          if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
-            return set_error(TBGPU_E_CUDA);
+          if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            cudaGetLastError();  // not capturable here: launch directly
+            use_graph = false;
+            continue;
+          }
           int r_ = TBGPU_OK;
           for (int k = 0; k < A.conv_skip && !r_; k++) r_ = step(launched + k, S1);
           if (cudaStreamEndCapture(s, &graph) != cudaSuccess || r_) return set_error(TBGPU_E_CUDA);
@@ -417,20 +455,68 @@ static int solve_batch_t(Ctx &c, int ndots, const int *dot_cells, const BatchArg
     }
     return TBGPU_OK;
   };
+  // The GPU runs up to kAhead check intervals ahead of the host's test; each
+  // check in flight copies alpha and beta into its own pinned slot.
+  struct Pending {
+    int at, slot;
+    cudaEvent_t ev;
+  };
+  std::vector<Pending> pend;
+  auto drop_pending = [&]() {
+    for (auto &p : pend) cudaEventDestroy(p.ev);
+    pend.clear();
+  };
+  size_t qi = 0;
+  auto fill = [&]() -> int {
+    while (qi < checks.size() && pend.size() < size_t(kAhead)) {
+      const int at = checks[qi];
+      int r_ = run_to(at);
+      if (r_) return r_;
+      const int sl = int(qi % kSlots);
+      double *ha = h_alpha + size_t(sl) * SA * ndots, *hb = h_bet + size_t(sl) * SB * ndots;
+      cudaEvent_t ev;
+      if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess ||
+          cudaMemcpy2DAsync(ha, sizeof(double) * SA, d_alpha, sizeof(double) * SA,
+                            sizeof(double) * at, ndots, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+          cudaMemcpy2DAsync(hb, sizeof(double) * SB, d_bet, sizeof(double) * SB,
+                            sizeof(double) * (at + 1), ndots, cudaMemcpyDeviceToHost,
+                            s) != cudaSuccess ||
+          cudaEventRecord(ev, s) != cudaSuccess)
+        return set_error(TBGPU_E_CUDA);
+      pend.push_back({at, sl, ev});
+      qi++;
+    }
+    return TBGPU_OK;
+  };
   int final_all = -1;
-  for (size_t qi = 0; qi < checks.size(); qi++) {
-    const int at = checks[qi];
-    B_RC(run_to(at));
-    B_CUDA(cudaMemcpy2DAsync(h_alpha, sizeof(double) * SA, d_alpha, sizeof(double) * SA,
-                             sizeof(double) * at, ndots, cudaMemcpyDeviceToHost, s));
-    B_CUDA(cudaMemcpy2DAsync(h_bet, sizeof(double) * SB, d_bet, sizeof(double) * SB,
-                             sizeof(double) * (at + 1), ndots, cudaMemcpyDeviceToHost, s));
-    B_CUDA(cudaStreamSynchronize(s));
-    bool bad = false;
+  {
+    int r_ = fill();
+    if (r_) {
+      drop_pending();
+      cleanup();
+      return r_;
+    }
+  }
+  while (!pend.empty()) {
+    const Pending p = pend.front();
+    pend.erase(pend.begin());
+    const int at = p.at;
+    if (cudaEventSynchronize(p.ev) != cudaSuccess) {
+      cudaEventDestroy(p.ev);
+      drop_pending();
+      cleanup();
+      return set_error(TBGPU_E_CUDA);
+    }
+    cudaEventDestroy(p.ev);
+    const double *sa_ = h_alpha + size_t(p.slot) * SA * ndots;
+    const double *sb_ = h_bet + size_t(p.slot) * SB * ndots;
+    std::atomic<bool> bad{false};
+    std::vector<char> was_done(ndots);
+    for (int d = 0; d < ndots; d++) was_done[d] = st[d].done;
     parallel_for(ndots, [&](int d) {
       DotState &D = st[d];
       if (D.done) return;
-      const double *ha = h_alpha + d * SA, *hb = h_bet + d * SB;
+      const double *ha = sa_ + d * SA, *hb = sb_ + d * SB;
       for (int i = 0; i < at; i++)
         if (!std::isfinite(ha[i])) bad = true;
       if (A.req1 > 0 && int(D.c1.size()) <= A.req1)
@@ -439,7 +525,8 @@ static int solve_batch_t(Ctx &c, int ndots, const int *dot_cells, const BatchArg
       if (A.req2 > 0 && int(D.c2.size()) <= A.req2)
         check_window(at, ha, hb + 1, A.emin2[d], A.emax2[d], A.tol, res, D.c2, D.i2,
                      0x51ED27ULL * at + 2);
-      const bool more = (at + 1 < A.imax) && (int(D.c1.size()) < A.req1 || int(D.c2.size()) < A.req2);
+      const bool more =
+          (at + 1 < A.imax) && (int(D.c1.size()) < A.req1 || int(D.c2.size()) < A.req2);
       if (!more) {
         D.done = true;
         D.final_it = at;
@@ -448,6 +535,7 @@ static int solve_batch_t(Ctx &c, int ndots, const int *dot_cells, const BatchArg
       }
     });
     if (bad) {
+      drop_pending();
       cleanup();
       return set_error(TBGPU_E_NUMERIC);
     }
@@ -455,7 +543,17 @@ static int solve_batch_t(Ctx &c, int ndots, const int *dot_cells, const BatchArg
       final_all = at;
       break;
     }
+    int r_ = TBGPU_OK;
+    for (int d = 0; d < ndots && !r_; d++)
+      if (st[d].done && !was_done[d]) r_ = mark(d);
+    if (!r_) r_ = fill();
+    if (r_) {
+      drop_pending();
+      cleanup();
+      return r_;
+    }
   }
+  drop_pending();
   if (final_all < 0) {  // iteration limit: the dots not done keep T up to there
     B_RC(run_to(A.imax));
     const int at = launched;
@@ -531,12 +629,23 @@ static int solve_batch_t(Ctx &c, int ndots, const int *dot_cells, const BatchArg
     for (int i = S1; i < S2; i++) B_CUDA(cudaMalloc(&ring[i], vbytes));
     B_CUDA(cudaMalloc(&d_coef, sizeof(double) * ndots * kMaxK * kMaxVec));
     B_CUDA(cudaMemsetAsync(V_dev, 0, sizeof(double2) * dim * nvec, s));
+    // each dot regenerates its recurrence up to its own last needed
+    // iteration and then drops out
+    std::vector<int> dot_maxit(ndots, 0);
+    for (int d = 0; d < ndots; d++)
+      for (int k = 0; k < nv_dot[d]; k++) dot_maxit[d] = std::max(dot_maxit[d], fd[d][k].second);
+    B_CUDA(cudaMemsetAsync(d_skip, 0, c.natoms, s));
+    B_CUDA(cudaMemsetAsync(d_done, 0, ndots, s));
     cudaEventRecord(t0, s);
     B_RC(start());
+    for (int d = 0; d < ndots; d++)
+      if (dot_maxit[d] == 0) B_RC(mark(d));
     std::vector<double> ch(size_t(ndots) * kMaxK * kMaxVec);
     int it0 = 0;
     for (int it = 0; it < maxit; it++) {
       B_RC(step(it, S2));
+      for (int d = 0; d < ndots; d++)
+        if (dot_maxit[d] == it + 1) B_RC(mark(d));
       if ((it + 1 - it0) == K || it == maxit - 1) {
         const int nk = it + 1 - it0;
         RingPtrs<VT> P{};
@@ -562,6 +671,7 @@ static int solve_batch_t(Ctx &c, int ndots, const int *dot_cells, const BatchArg
     B_CUDA(cudaStreamSynchronize(s));
     cudaEventElapsedTime(&ms, t0, t1);
     c.stats.vectors_ms = ms;
+    c.d_skip = nullptr;  // the refinement's products cover every dot
     if (kMixed) {  // double-precision Rayleigh-Ritz, dot by dot
       std::vector<double> vals(size_t(ndots) * nvec, 0.0);
       for (int d = 0; d < ndots; d++)

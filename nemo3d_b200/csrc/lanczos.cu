@@ -190,7 +190,34 @@ static int sturm_below(int n, const double *d, const double *e2, double x) {
   return cnt;
 }
 
-// eigenvalues of T (diag d, off-diagonal e) in (vl, vu], ascending
+// Sturm counts of kLanes shift points in one pass over T: the counts of
+// independent shifts are independent chains of divisions, which the core
+// overlaps (one chain alone waits on each division).  Each count is the
+// same arithmetic as sturm_below.
+constexpr int kLanes = 8;
+static void sturm_below_multi(int n, const double *d, const double *e2, const double *x,
+                              int *cnt) {
+  double q[kLanes];
+  int c[kLanes];
+  for (int k = 0; k < kLanes; k++) {
+    q[k] = d[0] - x[k];
+    c[k] = q[k] < 0;
+  }
+  for (int i = 1; i < n; i++) {
+    const double di = d[i], ei = e2[i - 1];
+    for (int k = 0; k < kLanes; k++) {
+      double qk = q[k];
+      if (std::fabs(qk) < 1e-300) qk = qk < 0 ? -1e-300 : 1e-300;
+      qk = di - x[k] - ei / qk;
+      c[k] += qk < 0;
+      q[k] = qk;
+    }
+  }
+  for (int k = 0; k < kLanes; k++) cnt[k] = c[k];
+}
+
+// eigenvalues of T (diag d, off-diagonal e) in (vl, vu], ascending: one
+// bisection per eigenvalue, kLanes eigenvalues advanced together
 static std::vector<double> tri_eigs(int n, const double *d, const double *e, double vl,
                                     double vu) {
   std::vector<double> e2(std::max(n - 1, 1));
@@ -202,22 +229,47 @@ static std::vector<double> tri_eigs(int n, const double *d, const double *e, dou
     hi = std::max(hi, d[i] + r);
   }
   const int c0 = sturm_below(n, d, e2.data(), vl), c1 = sturm_below(n, d, e2.data(), vu);
-  std::vector<double> w(std::max(c1 - c0, 0));
-  parallel_for(c1 - c0, [&](int k) {
-    const int idx = c0 + k;
-    double a = std::max(vl, lo), b = std::min(vu, hi);
-    for (int it = 0; it < 200; it++) {
-      const double tol = 1e-13 + 2.2e-16 * std::max(std::fabs(a), std::fabs(b));
-      if (b - a <= tol) break;
-      const double mid = 0.5 * (a + b);
-      if (sturm_below(n, d, e2.data(), mid) > idx) b = mid;
-      else a = mid;
+  const int ne = std::max(c1 - c0, 0);
+  std::vector<double> w(ne);
+  const int ngroups = (ne + kLanes - 1) / kLanes;
+  parallel_for(ngroups, [&](int gi) {
+    double a[kLanes], b[kLanes], mid[kLanes];
+    int idx[kLanes], cnt[kLanes], its[kLanes];
+    bool live[kLanes];
+    for (int k = 0; k < kLanes; k++) {
+      const int j = gi * kLanes + k;
+      live[k] = j < ne;
+      idx[k] = c0 + j;
+      a[k] = std::max(vl, lo);
+      b[k] = std::min(vu, hi);
+      its[k] = 0;
     }
-    w[k] = 0.5 * (a + b);
+    for (;;) {
+      bool any = false;
+      for (int k = 0; k < kLanes; k++) {
+        if (live[k]) {  // the same stopping rule as one bisection alone
+          const double tol = 1e-13 + 2.2e-16 * std::max(std::fabs(a[k]), std::fabs(b[k]));
+          if (its[k] >= 200 || b[k] - a[k] <= tol) live[k] = false;
+        }
+        mid[k] = live[k] ? 0.5 * (a[k] + b[k]) : a[k];
+        any = any || live[k];
+      }
+      if (!any) break;
+      sturm_below_multi(n, d, e2.data(), mid, cnt);
+      for (int k = 0; k < kLanes; k++) {
+        if (!live[k]) continue;
+        if (cnt[k] > idx[k]) b[k] = mid[k];
+        else a[k] = mid[k];
+        its[k]++;
+      }
+    }
+    for (int k = 0; k < kLanes; k++) {
+      const int j = gi * kLanes + k;
+      if (j < ne) w[j] = 0.5 * (a[k] + b[k]);
+    }
   });
   return w;
 }
-
 
 // 20 solves with T - (lambda + 1e-8) on the leading m x m block; x out
 bool inverse_iteration(int m, const double *d, const double *e, double lambda, Rng &rng,
@@ -252,6 +304,68 @@ bool inverse_iteration(int m, const double *d, const double *e, double lambda, R
   return true;
 }
 
+// inverse_iteration for up to kLanes eigenvalues at once, the solves of the
+// lanes interleaved (independent division chains) and each lane's arithmetic
+// that of inverse_iteration: x[k] (length m) and ok[k] per lane k < nl.
+static void inverse_iteration_multi(int m, const double *d, const double *e, const double *lam,
+                                    Rng *rng, int nl, std::vector<double> *x, bool *ok) {
+  std::vector<double> ds(size_t(m) * kLanes), g(size_t(m) * kLanes), y(size_t(m) * kLanes),
+      xv(size_t(m) * kLanes);
+  double nrm[kLanes];
+  for (int k = 0; k < kLanes; k++) {
+    ok[k] = k < nl;
+    nrm[k] = 0.0;
+  }
+  for (int k = 0; k < nl; k++) {
+    for (int i = 0; i < m; i++) {
+      ds[size_t(i) * kLanes + k] = d[i] - (lam[k] + 1e-8);
+      const double r = rng[k].next();
+      y[size_t(i) * kLanes + k] = r;
+      nrm[k] += r * r;
+    }
+    nrm[k] = std::sqrt(nrm[k]);
+    for (int i = 0; i < m; i++) y[size_t(i) * kLanes + k] /= nrm[k];
+  }
+  for (int it = 0; it < 20; it++) {
+    double piv[kLanes];
+    for (int k = 0; k < kLanes; k++) {
+      piv[k] = ds[k];
+      if (k < nl && piv[k] == 0.0) ok[k] = false;
+      xv[k] = ok[k] ? y[k] / piv[k] : 0.0;
+    }
+    for (int j = 1; j < m; j++) {
+      const double ej = e[j - 1];
+      const size_t o = size_t(j) * kLanes, op = size_t(j - 1) * kLanes;
+      for (int k = 0; k < kLanes; k++) {
+        if (!ok[k]) continue;
+        const double gj = ej / piv[k];
+        g[o + k] = gj;
+        piv[k] = ds[o + k] - ej * gj;
+        if (piv[k] == 0.0) {
+          ok[k] = false;
+          continue;
+        }
+        xv[o + k] = (y[o + k] - ej * xv[op + k]) / piv[k];
+      }
+    }
+    for (int j = m - 1; j > 0; j--)
+      for (int k = 0; k < kLanes; k++)
+        if (ok[k]) xv[size_t(j - 1) * kLanes + k] -= g[size_t(j) * kLanes + k] * xv[size_t(j) * kLanes + k];
+    for (int k = 0; k < kLanes; k++) nrm[k] = 0.0;
+    for (int i = 0; i < m; i++)
+      for (int k = 0; k < kLanes; k++) nrm[k] += xv[size_t(i) * kLanes + k] * xv[size_t(i) * kLanes + k];
+    for (int k = 0; k < kLanes; k++) nrm[k] = std::sqrt(nrm[k]);
+    for (int i = 0; i < m; i++)
+      for (int k = 0; k < kLanes; k++)
+        if (ok[k]) y[size_t(i) * kLanes + k] = xv[size_t(i) * kLanes + k] / nrm[k];
+  }
+  for (int k = 0; k < nl; k++) {
+    if (!ok[k]) continue;
+    x[k].resize(m);
+    for (int i = 0; i < m; i++) x[k][i] = y[size_t(i) * kLanes + k];
+  }
+}
+
 // find_converged_eigval, method 2 (lanczos.c:764-996).  The inverse
 // iterations of the candidates run in parallel; the acceptance pass then
 // walks the candidates in ascending order exactly as the reference does.
@@ -268,15 +382,29 @@ void check_window(int it, const double *al, const double *be, double emin, doubl
       if (std::fabs(c - ev[i]) < res) done = true;
     cand[i] = !done;
   }
-  parallel_for(ne, [&](int i) {
-    if (!cand[i]) return;
-    Rng rng{seed ^ (0x9E3779B97F4A7C15ULL * (unsigned long long)(i + 1))};
-    std::vector<double> x;
-    if (!inverse_iteration(it, al, be, ev[i], rng, x)) return;
-    bool flag = true;
-    for (int k = std::max(it - 2, 0); k < it; k++)
-      if (std::fabs(x[k]) > tol) flag = false;
-    ok[i] = flag;
+  std::vector<int> cl;  // the candidates, kLanes at a time
+  for (int i = 0; i < ne; i++)
+    if (cand[i]) cl.push_back(i);
+  parallel_for((int(cl.size()) + kLanes - 1) / kLanes, [&](int gi) {
+    const int nl = std::min(kLanes, int(cl.size()) - gi * kLanes);
+    double lam[kLanes];
+    Rng rng[kLanes];
+    std::vector<double> x[kLanes];
+    bool good[kLanes];
+    for (int k = 0; k < nl; k++) {
+      const int i = cl[gi * kLanes + k];
+      lam[k] = ev[i];
+      rng[k] = Rng{seed ^ (0x9E3779B97F4A7C15ULL * (unsigned long long)(i + 1))};
+    }
+    inverse_iteration_multi(it, al, be, lam, rng, nl, x, good);
+    for (int k = 0; k < nl; k++) {
+      const int i = cl[gi * kLanes + k];
+      if (!good[k]) continue;
+      bool flag = true;
+      for (int q = std::max(it - 2, 0); q < it; q++)
+        if (std::fabs(x[k][q]) > tol) flag = false;
+      ok[i] = flag;
+    }
   });
   for (int i = 0; i < ne; i++) {
     if (!cand[i] || !ok[i]) continue;

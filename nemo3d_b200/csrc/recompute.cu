@@ -131,7 +131,8 @@ __global__ void __launch_bounds__(WPB * 32, rc_min_blocks(NORB, NSPIN))
                      const double *__restrict__ onsite, const VT *__restrict__ x,
                      VT *__restrict__ y, double shift_d, const double *__restrict__ xnorm,
                      int xnorm_idx, double *partial, unsigned int *counter, double *alpha_out,
-                     int alpha_idx, const double2 *__restrict__ phase) {
+                     int alpha_idx, const double2 *__restrict__ phase,
+                     const unsigned char *__restrict__ skip) {
   constexpr int NB = NORB * NSPIN;
   constexpr int PS = NB + 1;  // padded row: conflict-free accesses
   constexpr int ONS = onsite_len(NB);
@@ -148,7 +149,7 @@ __global__ void __launch_bounds__(WPB * 32, rc_min_blocks(NORB, NSPIN))
     const int a = order[gw * kRcAtoms + ai];
     VT *out = part[w][ai][n];
     int b = -1;
-    if (a >= 0) {
+    if (a >= 0 && !(skip && __ldg(skip + a))) {
       const int4 v = nbr[a];
       b = n == 0 ? v.x : n == 1 ? v.y : n == 2 ? v.z : v.w;
     }
@@ -186,7 +187,7 @@ __global__ void __launch_bounds__(WPB * 32, rc_min_blocks(NORB, NSPIN))
     const int ai = base + ai2;
     if (!live || ai2 >= APW || ai >= kRcAtoms) continue;
     const int a = order[gw * kRcAtoms + ai];
-    if (a < 0) continue;
+    if (a < 0 || (skip && __ldg(skip + a))) continue;
     const double *rec = onsite + long(a) * ONS;
     const VT *X0 = x + long(a) * NB;
     auto xo = [&](int e) {
@@ -283,7 +284,7 @@ int launch_t(Ctx &c, const void *x, void *y, double shift, const double *xnorm, 
       c.rc_cat_warps, c.rc_warps, c.d_rc_order, c.d_nbr, c.d_site_m, c.d_atom_site, c.d_type, \
       c.d_dsp, c.d_par, c.nspecies, c.lattice[0], c.lattice[1], c.lattice[2],                 \
       c.include_strain, c.d_onsite, X, Y, shift, xnorm, xidx, DOT ? c.d_partial : nullptr,    \
-      DOT ? c.d_counter : nullptr, alpha_out, aidx, c.d_phase)
+      DOT ? c.d_counter : nullptr, alpha_out, aidx, c.d_phase, c.d_skip)
   if constexpr (sizeof(T) == sizeof(double)) {
     if (alpha_out && c.bloch) TBGPU_RECOMPUTE(true, true);
     else if (alpha_out) TBGPU_RECOMPUTE(true, false);

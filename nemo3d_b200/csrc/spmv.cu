@@ -53,7 +53,8 @@ __global__ void __launch_bounds__(WPB * 32)
            const VT *__restrict__ x, VT *__restrict__ y, double shift_d,
            const double *__restrict__ xnorm, int xnorm_idx, double *partial,
            unsigned int *counter, double *alpha_out, int alpha_idx,
-           const double2 *__restrict__ phase = nullptr) {
+           const double2 *__restrict__ phase = nullptr,
+           const unsigned char *__restrict__ skip = nullptr) {
   using RT = decltype(VT::x);
   constexpr int NB = NORB * NSPIN;
   constexpr int APW = 32 / NORB;
@@ -62,7 +63,8 @@ __global__ void __launch_bounds__(WPB * 32)
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int ai = lane / NORB, o = lane - ai * NORB;
   const long a = (long(blockIdx.x) * WPB + w) * APW + ai;
-  const bool act = ai < APW && a < natoms;
+  // skip: atoms left out of the product (a converged dot of a batched solve)
+  const bool act = ai < APW && a < natoms && !(skip && __ldg(skip + a));
   const RT scale = RT(xnorm ? 1.0 / xnorm[xnorm_idx] : 1.0);
   const RT shift = RT(shift_d);
   int nb[4] = {-1, -1, -1, -1};
@@ -202,20 +204,20 @@ static int launch_ht(Ctx &c, const void *x, void *y, double shift,
     if (c.bloch)
       k_spmv<NORB, NSPIN, kWPB, true, true, HT, VT><<<grid, kWPB * 32, 0, s>>>(
           c.natoms, c.d_nbr, c.d_site_m, ons, blk, X, Y, shift, xnorm, xidx, c.d_partial,
-          c.d_counter, alpha_out, aidx, c.d_phase);
+          c.d_counter, alpha_out, aidx, c.d_phase, c.d_skip);
     else
       k_spmv<NORB, NSPIN, kWPB, true, false, HT, VT><<<grid, kWPB * 32, 0, s>>>(
           c.natoms, c.d_nbr, c.d_site_m, ons, blk, X, Y, shift, xnorm, xidx, c.d_partial,
-          c.d_counter, alpha_out, aidx);
+          c.d_counter, alpha_out, aidx, nullptr, c.d_skip);
   } else {
     if (c.bloch)
       k_spmv<NORB, NSPIN, kWPB, false, true, HT, VT><<<grid, kWPB * 32, 0, s>>>(
           c.natoms, c.d_nbr, c.d_site_m, ons, blk, X, Y, shift, xnorm, xidx, nullptr, nullptr,
-          nullptr, 0, c.d_phase);
+          nullptr, 0, c.d_phase, c.d_skip);
     else
       k_spmv<NORB, NSPIN, kWPB, false, false, HT, VT><<<grid, kWPB * 32, 0, s>>>(
           c.natoms, c.d_nbr, c.d_site_m, ons, blk, X, Y, shift, xnorm, xidx, nullptr, nullptr,
-          nullptr, 0);
+          nullptr, 0, nullptr, c.d_skip);
   }
   TB_CUDA(cudaGetLastError());
   return TBGPU_OK;

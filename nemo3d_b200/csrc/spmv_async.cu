@@ -133,7 +133,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
                  const HT *__restrict__ blocks, const VT *__restrict__ x,
                  VT *__restrict__ y, double shift_d, const double *__restrict__ xnorm,
                  int xnorm_idx, double *partial, unsigned int *counter, double *alpha_out,
-                 int alpha_idx) {
+                 int alpha_idx, const unsigned char *__restrict__ skip) {
   using L = Layout<NSPIN, WARPS, STAGES, HT, VT>;
   using RT = typename L::RT;
   constexpr int NB = L::NB;
@@ -147,10 +147,10 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
   const long nw = long(gridDim.x) * WARPS;
   long g = long(blockIdx.x) * WARPS + warp;
   // prologue: copies of the first group in flight, metadata of the next
-  Meta cur = load_meta(g, ngroups, groups, nbr, site_m);
+  Meta cur = load_meta(g, ngroups, groups, nbr, site_m, skip);
   if (STAGES > 1 && g < ngroups) issue<L>(wbase, g, cur, lane, onsite, blocks, x);
   cp_commit();
-  Meta nxt = load_meta(g + nw, ngroups, groups, nbr, site_m);
+  Meta nxt = load_meta(g + nw, ngroups, groups, nbr, site_m, skip);
   int k = 0;
   for (; g < ngroups; g += nw, ++k) {
     const long gn = g + nw;
@@ -163,7 +163,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
       issue<L>(st, g, cur, lane, onsite, blocks, x);
       cp_commit();
     }
-    const Meta nn = load_meta(gn + nw, ngroups, groups, nbr, site_m);  // two groups ahead
+    const Meta nn = load_meta(gn + nw, ngroups, groups, nbr, site_m, skip);  // two groups ahead
     if (STAGES > 1) cp_wait<1>(); else cp_wait<0>();  // this lane's copies of g landed
     __syncwarp();   // ... and every lane's
     // this lane's atom, selected without indexing the metadata at run time
@@ -281,7 +281,7 @@ int launch_async_t(Ctx &c, const void *x, void *y, double shift, const double *x
   k_spmv_async<NSPIN, DOT, WARPS, STAGES, HT, VT><<<grid, WARPS * 32, L::SMEM, s>>>(
       c.ngroups, c.d_groups, c.d_nbr, c.d_site_m, ham_onsite<HT>(c), ham_blocks<HT>(c),
       reinterpret_cast<const VT *>(x), reinterpret_cast<VT *>(y), shift, xnorm, xidx,
-      DOT ? c.d_partial : nullptr, DOT ? c.d_counter : nullptr, alpha_out, aidx);
+      DOT ? c.d_partial : nullptr, DOT ? c.d_counter : nullptr, alpha_out, aidx, c.d_skip);
   TB_CUDA(cudaGetLastError());
   return TBGPU_OK;
 }
@@ -338,7 +338,7 @@ static int launch_scratch_async_t(Ctx &c, int sms, const double2 *X, double2 *Y,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM));
   k_spmv_async<NSPIN, true, WARPS, 1, HT><<<sms, WARPS * 32, L::SMEM, s>>>(
       c.ngroups, c.d_groups, c.d_nbr, c.d_site_m, ham_onsite<HT>(c), ham_blocks<HT>(c), X, Y,
-      shift, nullptr, 0, partial, counter, dot_out, 0);
+      shift, nullptr, 0, partial, counter, dot_out, 0, nullptr);
   TB_CUDA(cudaGetLastError());
   return TBGPU_OK;
 }

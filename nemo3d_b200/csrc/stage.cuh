@@ -40,12 +40,16 @@ struct Meta {
 };
 
 // Group g of the work order: up to three consecutive atoms of one pencil.
+// skip (or null): per atom, 1 for atoms left out of the product (the atoms of
+// a converged dot in a batched solve; a group lies in one dot).
 __device__ __forceinline__ Meta load_meta(long g, long ngroups, const int2 *__restrict__ groups,
                                           const int4 *__restrict__ nbr,
-                                          const unsigned char *__restrict__ site_m) {
+                                          const unsigned char *__restrict__ site_m,
+                                          const unsigned char *__restrict__ skip = nullptr) {
   Meta M;
   int2 e = make_int2(0, 0);
   if (g < ngroups) e = __ldg(groups + g);
+  if (skip && g < ngroups && __ldg(skip + e.x)) e.y = 0;
   M.a0 = e.x;
 #pragma unroll
   for (int i = 0; i < kAPW; i++) {

@@ -81,6 +81,9 @@ struct Ctx {
   // vectors through the recompute product (the double on-site records and
   // the recompute work order are kept for it)
   bool lanczos_f32 = false;
+  // per atom, 1 = left out of the products (set only while a batched solve
+  // runs, for the dots that have converged); null otherwise
+  const unsigned char *d_skip = nullptr;
   std::vector<double> state_resid, state_delta;  // per state of the last solve
   float *d_onsite32 = nullptr;
   float *d_blocks32 = nullptr;

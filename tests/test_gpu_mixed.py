@@ -33,6 +33,7 @@ def _rounded(o):
 
 
 @pytest.mark.parametrize("model,storage", [("sp3d5s*_so", "store"), ("sp3d5s*", "store"),
+                                           ("sp3s*_so", "store"), ("sp3s*", "store"),
                                            ("sp3d5s*_so", "recompute"),
                                            ("sp3d5s*", "recompute"),
                                            ("sp3s*_so", "recompute"), ("sp3s*", "recompute")])
@@ -109,10 +110,6 @@ def test_mixed_refusals():
     st = workloads.gaas_cube(2)
     with pytest.raises(tbgpu.TbgpuError) as e:  # needs the 32-bit store
         tbgpu.Hamiltonian(st, "sp3d5s*", [materials.MATERIALS["GaAs_spds"]], lanczos_bits=32)
-    assert e.value.code == -6
-    with pytest.raises(tbgpu.TbgpuError) as e:  # the float store: 10-orbital models only
-        tbgpu.Hamiltonian(st, "sp3s*", [materials.MATERIALS["GaAs_sps"]], ham_bits=32,
-                          lanczos_bits=32)
     assert e.value.code == -6
     with pytest.raises(tbgpu.TbgpuError) as e:
         tbgpu.Hamiltonian(st, "sp3d5s*", [materials.MATERIALS["GaAs_spds"]], lanczos_bits=16)
