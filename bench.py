@@ -316,6 +316,148 @@ def run_profile_case(args):
                       "iterations": res["iterations"], "stats": H.stats()}), flush=True)
 
 
+def _event_time(fn, reps, stream_ctx):
+    """Average device time (ms) of fn() over reps calls, CUDA events on the
+    context's stream (bound to torch's current stream)."""
+    import torch
+    for _ in range(3):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def run_extra(args):
+    """Measurements beside the headline (one JSON line each), on one GPU:
+    kernels   H*x of the 1.02M-atom dome: FP64 store, float store with float
+              vectors, recompute in FP64 and in float
+    mixed2M   the same dome at 72 x 72 x 48 cells (1,990,656 atoms): plain FP64
+              solve against the mixed-precision solve on the float store and on
+              the recompute product, eigenvalue error per state
+    batch256  256 In(x)Ga(1-x)As dots, 1k-50k atoms log-uniform, x uniform in
+              [0.4, 1.0], sp3s*+SO, 4 conduction states each with vectors:
+              batched FP64 and mixed solves, and 16 of the dots solved one at
+              a time (scaled by atoms)
+    vff1M     Keating relaxation of the 1.02M-atom dome (no Gaussian
+              displacements), AllFree"""
+    import torch
+    from nemo3d_b200 import tbgpu
+    torch.cuda.set_device(0)
+    w = args.workload
+    if w == "kernels":
+        st = make_structure()
+        for name, opts, f32 in (("fp64 store", {}, False),
+                                ("float store, float vectors", dict(ham_bits=32, lanczos_bits=32), True),
+                                ("recompute fp64", dict(recompute=True), False),
+                                ("recompute float", dict(recompute=True, lanczos_bits=32), True)):
+            H = tbgpu.Hamiltonian(st, "sp3d5s*_so", MATS, **opts)
+            stream = torch.cuda.Stream()
+            H.set_stream(stream.cuda_stream)
+            dt = torch.float32 if f32 else torch.float64
+            x = torch.from_numpy(workloads.random_start(H.n, seed=0)).to(dt).cuda()
+            y = torch.empty_like(x)
+            torch.cuda.synchronize()
+            with torch.cuda.stream(stream):
+                f = (lambda: H.hx_dev_f32(x.data_ptr(), y.data_ptr())) if f32 else \
+                    (lambda: H.hx_dev(x.data_ptr(), y.data_ptr()))
+                ms = _event_time(f, 20, stream)
+            print(json.dumps({"workload": "kernels", "metric": "H*x ms per launch", "variant": name,
+                              "natoms": H.natoms, "value": ms, "unit": "ms"}), flush=True)
+            H.close()
+    elif w == "mixed2M":
+        st = workloads.dome_in_box(cells=(72, 72, 48), base_nm=20.0, height_nm=5.0,
+                                   sigma_frac=0.005, seed=1)
+        ref = None
+        for name, opts in (("fp64", {}), ("mixed, float store", dict(ham_bits=32, lanczos_bits=32)),
+                           ("mixed, recompute", dict(recompute=True, lanczos_bits=32))):
+            H = tbgpu.Hamiltonian(st, "sp3d5s*_so", MATS, **opts)
+            r0 = torch.from_numpy(workloads.random_start(H.n, seed=0)).cuda()
+            V = torch.empty((NVEC, 2 * H.n), dtype=torch.float64, device="cuda")
+            torch.cuda.synchronize()
+            t = time.time()
+            res = H.eigensolve_lanczos_dev(r0.data_ptr(), V.data_ptr(), NVEC, **SOLVE)
+            torch.cuda.synchronize()
+            wall = time.time() - t
+            stt = H.stats()
+            line = {"workload": "mixed2M", "metric": "s to 8 band-edge eigenpairs", "variant": name,
+                    "natoms": H.natoms, "value": wall, "unit": "s",
+                    "first_pass_ms": stt["solve_ms"], "vectors_ms": stt["vectors_ms"],
+                    "refine_ms": stt["refine_ms"], "iterations": res["iterations"],
+                    "eigenvalues": [round(float(v), 12) for v in res["values"]]}
+            if ref is None:
+                ref = res["values"]
+            elif len(ref) == len(res["values"]):
+                line["error_per_state_ev"] = [float(abs(a - b)) for a, b in zip(ref, res["values"])]
+            if "lanczos_bits" in opts:
+                r, _ = H.state_errors()
+                line["residual_per_state_ev"] = [float(v) for v in r]
+            print(json.dumps(line), flush=True)
+            H.close()
+            del V, r0
+            torch.cuda.empty_cache()
+    elif w == "batch256":
+        nd = 256
+        rng = np.random.default_rng(2024)
+        sizes = np.exp(rng.uniform(np.log(1000), np.log(50000), nd)).astype(int)
+        xs = rng.uniform(0.4, 1.0, nd)
+        dots = [workloads.alloy_dot(int(n), float(x), seed=i) for i, (n, x) in enumerate(zip(sizes, xs))]
+        packed, cells = workloads.pack_dots(dots)
+        mats = [materials.MATERIALS["GaAs_sps"], materials.MATERIALS["InAs_sps"]]
+        kw = dict(ConvCheckStartIter=200, ConvCheckSkipRate=50, imax=12000, requested1=0,
+                  requested2=4, tolerance=1e-7)
+        win = dict(emin1=np.zeros(nd), emax1=np.zeros(nd), emin2=np.full(nd, 1.0),
+                   emax2=np.full(nd, 2.6))
+        for name, opts in (("fp64 batch", {}), ("mixed batch", dict(ham_bits=32, lanczos_bits=32))):
+            H = tbgpu.Hamiltonian(packed, "sp3s*_so", mats, **opts)
+            r0 = torch.from_numpy(workloads.random_start(H.n, seed=0)).cuda()
+            torch.cuda.synchronize()
+            t = time.time()
+            res = H.eigensolve_lanczos_batched(r0, cells, vectors=4, **win, **kw)
+            torch.cuda.synchronize()
+            wall = time.time() - t
+            stt = H.stats()
+            print(json.dumps({"workload": "batch256", "metric": "s to 4 conduction states of 256 dots",
+                              "variant": name, "natoms": H.natoms, "value": wall, "unit": "s",
+                              "first_pass_ms": stt["solve_ms"], "vectors_ms": stt["vectors_ms"],
+                              "refine_ms": stt["refine_ms"],
+                              "iterations_max": int(res["iterations"].max()),
+                              "iterations_median": float(np.median(res["iterations"])),
+                              "found_min": int(min(len(v) for v in res["values"]))}), flush=True)
+            H.close()
+        samp = list(range(0, nd, nd // 16))
+        t = time.time()
+        atoms = 0
+        for i in samp:
+            H = tbgpu.Hamiltonian(dots[i], "sp3s*_so", mats, ham_bits=32, lanczos_bits=32)
+            H.eigensolve_lanczos(workloads.random_start(H.n, seed=i), emin1=0.0, emax1=0.0,
+                                 emin2=1.0, emax2=2.6, vectors=4, **kw)
+            atoms += H.natoms
+            H.close()
+        wall = time.time() - t
+        print(json.dumps({"workload": "batch256", "metric": "s to 4 conduction states of 256 dots",
+                          "variant": "dots one at a time (mixed; 16-dot sample scaled by atoms)",
+                          "value": wall * sizes.sum() / atoms, "unit": "s",
+                          "sample_s": wall, "sample_atoms": atoms}), flush=True)
+    elif w == "vff1M":
+        st = workloads.dome_in_box(cells=(58, 58, 38), base_nm=20.0, height_nm=5.0,
+                                   sigma_frac=0.0, seed=1)
+        H = tbgpu.Hamiltonian(st, "sp3d5s*_so", MATS, build=False)
+        e0 = H.vff_energy()
+        torch.cuda.synchronize()
+        t = time.time()
+        _, e, its = H.vff_relax(bc=0, max_iter=20000, tol=1e-9)
+        torch.cuda.synchronize()
+        wall = time.time() - t
+        print(json.dumps({"workload": "vff1M", "metric": "s to relax (Keating, macopt)",
+                          "natoms": st.nsites, "value": wall, "unit": "s", "iterations": its,
+                          "energy_start": e0, "energy_end": e}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -330,6 +472,9 @@ def main():
     ap.add_argument("--profile-iterations", type=int, default=6)
     ap.add_argument("--profile-full", action="store_true",
                     help="with --profile-case: use the full-size workload")
+    ap.add_argument("--workload", default="dome1M",
+                    choices=["dome1M", "kernels", "mixed2M", "batch256", "vff1M"],
+                    help="dome1M: the headline bench; the others: measurements beside it")
     ap.add_argument("--ref-iterations", type=int, default=19002,
                     help="iterations of a full solve (both passes) the CPU sample is scaled to")
     args = ap.parse_args()
@@ -338,6 +483,9 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     if args.profile_case:
         run_profile_case(args)
+    elif args.workload != "dome1M":
+        if rank == 0:
+            run_extra(args)
     elif args.impl == "reference":
         run_reference(args, rank, world)
     else:
