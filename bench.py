@@ -298,7 +298,9 @@ def run_ours(args, rank, world, local_rank):
 def run_profile_case(args):
     """A smaller dot (40 x 40 x 30 cells, 384,000 atoms; H and vectors ~2 GB,
     larger than L2) running a few Lanczos iterations without convergence
-    checks: the k_spmv / k_update launches that ncu captures."""
+    checks: the k_spmv / k_update launches that ncu captures (stored or
+    recomputed blocks, FP64 or mixed precision), or a few Keating VFF
+    iterations of the same structure."""
     import torch
     from nemo3d_b200 import tbgpu
     torch.cuda.set_device(0)
@@ -307,7 +309,22 @@ def run_profile_case(args):
     else:
         st = workloads.dome_in_box(cells=(40, 40, 30), base_nm=14.0, height_nm=4.0,
                                    sigma_frac=0.005, seed=1)
-    H = tbgpu.Hamiltonian(st, "sp3d5s*_so", MATS)
+    if args.profile_vff:  # a few Keating iterations (k_vff_vertex / k_vff_gather)
+        st.dsp = None
+        H = tbgpu.Hamiltonian(st, "sp3d5s*_so", MATS, build=False)
+        _, e, its = H.vff_relax(max_iter=args.profile_iterations, tol=0.0)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_case": "vff", "natoms": st.nsites, "iterations": its,
+                          "energy": e}), flush=True)
+        return
+    opts = {}
+    if args.profile_storage == "recompute":
+        opts["recompute"] = True
+    elif args.profile_precision == 32:
+        opts["ham_bits"] = 32
+    if args.profile_precision == 32:
+        opts["lanczos_bits"] = 32
+    H = tbgpu.Hamiltonian(st, "sp3d5s*_so", MATS, **opts)
     r0 = workloads.random_start(H.n, seed=0)
     res = H.eigensolve_lanczos(r0, imax=args.profile_iterations + 1, requested1=1,
                                requested2=1, ConvCheckStartIter=10 ** 9)
@@ -472,6 +489,12 @@ def main():
     ap.add_argument("--profile-iterations", type=int, default=6)
     ap.add_argument("--profile-full", action="store_true",
                     help="with --profile-case: use the full-size workload")
+    ap.add_argument("--profile-storage", default="store", choices=["store", "recompute"],
+                    help="with --profile-case: stored blocks or blocks recomputed in H*x")
+    ap.add_argument("--profile-precision", type=int, default=64, choices=[64, 32],
+                    help="with --profile-case: FP64 or the mixed-precision Lanczos")
+    ap.add_argument("--profile-vff", action="store_true",
+                    help="with --profile-case: a few Keating VFF iterations instead")
     ap.add_argument("--workload", default="dome1M",
                     choices=["dome1M", "kernels", "mixed2M", "batch256", "vff1M"],
                     help="dome1M: the headline bench; the others: measurements beside it")
