@@ -206,6 +206,7 @@ def run_ours(args, rank, world, local_rank):
         H = tbgpu.Hamiltonian(st, "sp3d5s*_so", MATS, build=False,
                               device_inputs=(types_d.data_ptr(), dsp_d.data_ptr()))
         H.set_stream(stream.cuda_stream)
+        H.set_spmv_variant(args.spmv_variant)
         H.build()
         if profile:
             H.set_profiling(True)
@@ -245,6 +246,7 @@ def run_ours(args, rank, world, local_rank):
             barrier()
             t0 = time.perf_counter()
             H = tbgpu.Hamiltonian(st, "sp3d5s*_so", MATS)          # host geometry in
+            H.set_spmv_variant(args.spmv_variant)
             out = H.eigensolve_lanczos(r0_h, vectors=NVEC, **SOLVE)  # host r0 in, vectors out
             H.close()
             torch.cuda.synchronize()
@@ -325,6 +327,7 @@ def run_profile_case(args):
     if args.profile_precision == 32:
         opts["lanczos_bits"] = 32
     H = tbgpu.Hamiltonian(st, "sp3d5s*_so", MATS, **opts)
+    H.set_spmv_variant(args.spmv_variant)
     r0 = workloads.random_start(H.n, seed=0)
     res = H.eigensolve_lanczos(r0, imax=args.profile_iterations + 1, requested1=1,
                                requested2=1, ConvCheckStartIter=10 ** 9)
@@ -351,7 +354,8 @@ def _event_time(fn, reps, stream_ctx):
 
 def run_extra(args):
     """Measurements beside the headline (one JSON line each), on one GPU:
-    kernels   H*x of the 1.02M-atom dome: FP64 store, float store with float
+    kernels   H*x of the 1.02M-atom dome: FP64 store (warp-staged and two-cell unit
+              kernels), float store with float
               vectors, recompute in FP64 and in float
     mixed2M   the same dome at 72 x 72 x 48 cells (1,990,656 atoms): plain FP64
               solve against the mixed-precision solve on the float store and on
@@ -368,11 +372,14 @@ def run_extra(args):
     w = args.workload
     if w == "kernels":
         st = make_structure()
-        for name, opts, f32 in (("fp64 store", {}, False),
-                                ("float store, float vectors", dict(ham_bits=32, lanczos_bits=32), True),
-                                ("recompute fp64", dict(recompute=True), False),
-                                ("recompute float", dict(recompute=True, lanczos_bits=32), True)):
+        for name, opts, f32, var in (
+                ("fp64 store", {}, False, 0),
+                ("fp64 store, two-cell units (variant 3)", {}, False, 3),
+                ("float store, float vectors", dict(ham_bits=32, lanczos_bits=32), True, 0),
+                ("recompute fp64", dict(recompute=True), False, 0),
+                ("recompute float", dict(recompute=True, lanczos_bits=32), True, 0)):
             H = tbgpu.Hamiltonian(st, "sp3d5s*_so", MATS, **opts)
+            H.set_spmv_variant(var)
             stream = torch.cuda.Stream()
             H.set_stream(stream.cuda_stream)
             dt = torch.float32 if f32 else torch.float64
@@ -495,6 +502,8 @@ def main():
                     help="with --profile-case: FP64 or the mixed-precision Lanczos")
     ap.add_argument("--profile-vff", action="store_true",
                     help="with --profile-case: a few Keating VFF iterations instead")
+    ap.add_argument("--spmv-variant", type=int, default=0, choices=[0, 1, 2, 3],
+                    help="H*x kernel of the solve (tbgpu_set_spmv_variant)")
     ap.add_argument("--workload", default="dome1M",
                     choices=["dome1M", "kernels", "mixed2M", "batch256", "vff1M"],
                     help="dome1M: the headline bench; the others: measurements beside it")

@@ -16,7 +16,8 @@
  *                       -> tbgpu_eigensolve_lanczos
  *
  * All pointers are plain host pointers unless the name ends in _dev (device
- * pointers on the context's CUDA device).  Complex vectors are interleaved
+ * pointers on the context's CUDA device; device vectors must start on a
+ * 16-byte boundary, as cudaMalloc's do, else TBGPU_E_ARG).  Complex vectors are interleaved
  * (re, im) doubles, layout-compatible with nml_dcscalar {double r, i}, in the
  * reference's order: index = atom * NBasisStates + orbital, spin-up orbitals
  * first (nemo3d/src/base/ham3d_final.c:547-620).
@@ -303,7 +304,9 @@ int tbgpu_hx_dot_noalloc(tbgpu_ctx *ctx, double shift, const double *x_dev,
 /* H*x kernel: 0 = default (warp-staged cp.async kernel, 14 warps x 1 stage
  * per SM, for the 10-orbital models; lane-gather kernel otherwise),
  * 1 = lane-gather kernel for every model, 2 = warp-staged kernel with
- * 7 warps x 2 stages. */
+ * 7 warps x 2 stages, 3 = two-cell unit kernel (bulk copies of each unit's
+ * contiguous pieces; 10-orbital models with the 64-bit store at the Gamma
+ * point, else as 0).  Every variant gives the same y bit for bit. */
 int tbgpu_set_spmv_variant(tbgpu_ctx *ctx, int variant);
 
 /* Lanczos for many independent dots at once (no counterpart in the

@@ -732,7 +732,7 @@ extern "C" int tbgpu_eigensolve_lanczos_batched(
     const double *emax1, const double *emin2, const double *emax2, double tolerance,
     const double *r0_dev, double *values, int values_stride, int *found, int *iterations,
     double *vectors_dev, int max_vectors) {
-  if (!ctx) return set_error(TBGPU_E_ARG);
+  if (!ctx || misaligned16(r0_dev) || misaligned16(vectors_dev)) return set_error(TBGPU_E_ARG);
   BatchArgs A{ConvCheckStartIter, ConvCheckSkipRate, imax, requested1, requested2, tolerance,
               emin1, emax1, emin2, emax2};
   return solve_batch(*reinterpret_cast<Ctx *>(ctx), ndots, dot_cells, A, r0_dev, values,

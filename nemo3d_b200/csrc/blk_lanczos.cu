@@ -860,7 +860,8 @@ extern "C" int tbgpu_eigensolve_blk_lanczos_dev(
     int p, int max_no_success, const double *r0_dev, double *values, int *found_vb,
     int *found_cb, int *iterations, double *vectors_dev, int max_vectors) {
   if (!ctx || !r0_dev || !values || p < 1 || p > kMaxP || imax < 2 || ConvCheckSkipRate < 1 ||
-      requested1 < 0 || requested2 < 0 || tolerance <= 0.0 || max_vectors < 0)
+      requested1 < 0 || requested2 < 0 || tolerance <= 0.0 || max_vectors < 0 ||
+      misaligned16(r0_dev) || misaligned16(vectors_dev))
     return set_error(TBGPU_E_ARG);
   Ctx &c = *reinterpret_cast<Ctx *>(ctx);
   if (!c.built) return set_error(TBGPU_E_STATE);

@@ -32,7 +32,7 @@ static void free_ctx(Ctx *c) {
   void *ptrs[] = {c->d_type, c->d_dsp, c->d_par, c->d_par_ok, c->d_site_index, c->d_atom_site,
                   c->d_nbr, c->d_site_m, c->d_surface, c->d_onsite, c->d_blocks, c->d_partial,
                   c->d_counter, c->d_status, c->d_x, c->d_y, c->d_phase, c->d_groups,
-                  c->d_blocks32, c->d_onsite32, c->d_rc_order};
+                  c->d_blocks32, c->d_onsite32, c->d_rc_order, c->d_units};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -171,14 +171,16 @@ long tbgpu_dimension(const tbgpu_ctx *ctx) {
 }
 
 int tbgpu_hx_dev(tbgpu_ctx *ctx, double shift, const double *x_dev, double *y_dev) {
-  if (!ctx || !x_dev || !y_dev) return set_error(TBGPU_E_ARG);
+  if (!ctx || !x_dev || !y_dev || misaligned16(x_dev) || misaligned16(y_dev))
+    return set_error(TBGPU_E_ARG);
   Ctx &c = *C(ctx);
   if (!c.built) return set_error(TBGPU_E_STATE);
   return launch_spmv(c, x_dev, y_dev, shift, nullptr, 0, nullptr, 0, c.stream);
 }
 
 int tbgpu_hx_dev_f32(tbgpu_ctx *ctx, double shift, const float *x_dev, float *y_dev) {
-  if (!ctx || !x_dev || !y_dev) return set_error(TBGPU_E_ARG);
+  if (!ctx || !x_dev || !y_dev || misaligned16(x_dev) || misaligned16(y_dev))
+    return set_error(TBGPU_E_ARG);
   Ctx &c = *C(ctx);
   if (!c.built) return set_error(TBGPU_E_STATE);
   return launch_spmv_f32(c, x_dev, y_dev, shift, nullptr, 0, nullptr, 0, c.stream);
@@ -218,7 +220,7 @@ int tbgpu_eigensolve_lanczos_dev(tbgpu_ctx *ctx, int ConvCheckStartIter, int Con
                                  double emax1, double emin2, double emax2, double tolerance,
                                  const double *r0_dev, double *values, int *conv_iterations,
                                  int *iterations, double *vectors_dev, int max_vectors) {
-  if (!ctx) return set_error(TBGPU_E_ARG);
+  if (!ctx || misaligned16(r0_dev) || misaligned16(vectors_dev)) return set_error(TBGPU_E_ARG);
   SolveArgs A{ConvCheckStartIter, ConvCheckSkipRate, imax, requested1, requested2,
               emin1, emax1, emin2, emax2, tolerance};
   return solve(*C(ctx), A, r0_dev, values, conv_iterations, iterations, vectors_dev,
@@ -346,7 +348,7 @@ int tbgpu_export_hamiltonian(const tbgpu_ctx *ctx, double *onsite, double *block
 }
 
 int tbgpu_set_spmv_variant(tbgpu_ctx *ctx, int variant) {
-  if (!ctx || variant < 0 || variant > 2) return set_error(TBGPU_E_ARG);
+  if (!ctx || variant < 0 || variant > 3) return set_error(TBGPU_E_ARG);
   C(ctx)->spmv_variant = variant;
   return TBGPU_OK;
 }

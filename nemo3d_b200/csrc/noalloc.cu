@@ -61,7 +61,8 @@ using namespace tbgpu;
 
 extern "C" int tbgpu_hx_dot_noalloc(tbgpu_ctx *ctx, double shift, const double *x_dev,
                                     double *y_dev, double *dot_dev) {
-  if (!ctx || !x_dev || !y_dev || !dot_dev) return set_error(TBGPU_E_ARG);
+  if (!ctx || !x_dev || !y_dev || !dot_dev || misaligned16(x_dev) || misaligned16(y_dev))
+    return set_error(TBGPU_E_ARG);
   Ctx &c = *reinterpret_cast<Ctx *>(ctx);
   if (!c.built) return set_error(TBGPU_E_STATE);
   int cur = -1;

@@ -281,6 +281,6 @@ using namespace tbgpu;
 
 extern "C" int tbgpu_momentum_matrix(tbgpu_ctx *ctx, int n, const double *psi_dev,
                                      const double *E, double *P, double *trans) {
-  if (!ctx) return set_error(TBGPU_E_ARG);
+  if (!ctx || misaligned16(psi_dev)) return set_error(TBGPU_E_ARG);
   return momentum_matrix(*reinterpret_cast<Ctx *>(ctx), n, psi_dev, E, P, trans);
 }

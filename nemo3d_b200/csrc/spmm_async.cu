@@ -272,7 +272,8 @@ int launch_spmm(Ctx &c, int p, const double *x, long xstride, double *y, long ys
 extern "C" int tbgpu_hx_block_dev(tbgpu_ctx *ctx, int p, double shift, const double *x_dev,
                                   double *y_dev) {
   using namespace tbgpu;
-  if (!ctx || !x_dev || !y_dev || p < 1 || p > 8) return set_error(TBGPU_E_ARG);
+  if (!ctx || !x_dev || !y_dev || p < 1 || p > 8 || misaligned16(x_dev) || misaligned16(y_dev))
+    return set_error(TBGPU_E_ARG);
   Ctx &c = *reinterpret_cast<Ctx *>(ctx);
   if (!c.built) return set_error(TBGPU_E_STATE);
   set_error(TBGPU_OK);

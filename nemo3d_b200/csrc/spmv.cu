@@ -237,6 +237,8 @@ int launch_spmv(Ctx &c, const double *x, double *y, double shift, const double *
   if (c.recompute) return launch_spmv_recompute(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
   // the warp-staged kernel has no phase support: periodic structures away
   // from Gamma take the lane-gather kernel
+  if (c.norb == 10 && c.spmv_variant == 3 && !c.bloch)
+    return launch_spmv_tile(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
   if (c.norb == 10 && c.spmv_variant != 1 && !c.bloch)
     return launch_spmv_async(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
   if (c.norb == 10 && c.nspin == 2) return launch_t<10, 2>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);

@@ -91,6 +91,11 @@ struct Ctx {
   // cells, pencils visited in j-blocks (first atom, atom count)
   int2 *d_groups = nullptr;
   long ngroups = 0;
+  // unit table of H*x variant 3 (units of two cells of one pencil; built on
+  // first use): nunits descriptors of unit_stride ints, stage capacities
+  int *d_units = nullptr;
+  long nunits = 0;
+  int unit_stride = 0, unit_cap_nb = 0, unit_cap_nx = 0;
   // reduction scratch (per-block partials + completion counter)
   double *d_partial = nullptr;
   unsigned int *d_counter = nullptr;
@@ -120,6 +125,9 @@ template <> inline const float *ham_onsite<float>(const Ctx &c) { return c.d_ons
 
 // error helpers
 int set_error(int code);
+// device vectors must start on a 16-byte boundary (the kernels move them in
+// 16-byte pieces); null passes
+inline bool misaligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15) != 0; }
 #define TB_CUDA(call)                                              \
   do {                                                             \
     cudaError_t e_ = (call);                                       \
@@ -162,6 +170,10 @@ int launch_spmv_async(Ctx &c, const double *x, double *y, double shift,
 int launch_spmv_async_f32(Ctx &c, const float *x, float *y, double shift,
                           const double *xscale_dev, int scale_index, double *alpha_out,
                           int alpha_index, cudaStream_t s);
+// spmv_tile.cu: variant 3 (falls back to launch_spmv_async where it does not apply)
+int launch_spmv_tile(Ctx &c, const double *x, double *y, double shift,
+                     const double *xscale_dev, int scale_index, double *alpha_out,
+                     int alpha_index, cudaStream_t s);
 // caller-provided reduction scratch (noalloc.cu)
 int launch_spmv_scratch(Ctx &c, const double *x, double *y, double shift, double *partial,
                         unsigned int *counter, int cap, double *dot_out, cudaStream_t s);

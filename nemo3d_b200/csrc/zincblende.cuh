@@ -27,8 +27,11 @@ static __constant__ int8_t c_nnmap[8][4][4] = {
 // neighbour's list that points back across the same bond (derived from the
 // map above).  Every bond is stored once, in the cation's slot; an anion
 // reads that block, transposed, through this table.
-static __constant__ int8_t c_rev_slot[8][4] = {
-    {0, 3, 3, 3}, {0, 1, 2, 2}, {2, 0, 2, 1}, {3, 0, 1, 1},
-    {0, 1, 0, 0}, {0, 2, 2, 3}, {1, 3, 2, 2}, {1, 3, 3, 1}};
+#define TBGPU_REV_SLOT_TABLE                                 \
+  {{0, 3, 3, 3}, {0, 1, 2, 2}, {2, 0, 2, 1}, {3, 0, 1, 1}, \
+   {0, 1, 0, 0}, {0, 2, 2, 3}, {1, 3, 2, 2}, {1, 3, 3, 1}}
+static __constant__ int8_t c_rev_slot[8][4] = TBGPU_REV_SLOT_TABLE;
+// the same table for host code
+constexpr int8_t kRevSlot[8][4] = TBGPU_REV_SLOT_TABLE;
 
 }  // namespace tbgpu

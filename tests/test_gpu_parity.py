@@ -210,14 +210,14 @@ def test_full_size_hermitian_and_linear():
 
 @pytest.mark.parametrize("model", ["sp3d5s*", "sp3d5s*_so"])
 def test_spmv_variants_match_oracle(model):
-    """The TMA-staged kernel (default for 10 orbitals) and the lane-gather
-    kernel both reproduce the oracle's H*x."""
+    """Every H*x variant (warp-staged default, lane-gather, two-stage
+    warp-staged, two-cell units) reproduces the oracle's H*x."""
     st = small_dome(seed=11)
     g, o = pair(st, model)
     x = np.random.default_rng(3).uniform(-1, 1, 2 * g.n)
     scale = max(np.abs(o.onsite).max(), np.abs(o.blocks).max())
     yo = o.hx(x, 0.7)
-    for variant in (0, 1, 2):
+    for variant in (0, 1, 2, 3):
         g.set_spmv_variant(variant)
         assert np.abs(g.matvect_mult(x, 0.7) - yo).max() <= 1e-12 * scale * 45, variant
 
