@@ -365,7 +365,12 @@ def run_extra(args):
               batched FP64 and mixed solves, and 16 of the dots solved one at
               a time (scaled by atoms)
     vff1M     Keating relaxation of the 1.02M-atom dome (no Gaussian
-              displacements), AllFree"""
+              displacements), AllFree
+    warm      learned warm start: plain solves of --warm-train randomized
+              In(x)Ga(1-x)As lens dots (20 x 20 x 14 cells, 44,800 sites,
+              sp3d5s*+SO, 4 h + 4 e levels with vectors) as training data,
+              the network trained on them, then --warm-test held-out seeds
+              solved cold and warm: iterations and wall time of each"""
     import torch
     from nemo3d_b200 import tbgpu
     torch.cuda.set_device(0)
@@ -480,6 +485,63 @@ def run_extra(args):
         print(json.dumps({"workload": "vff1M", "metric": "s to relax (Keating, macopt)",
                           "natoms": st.nsites, "value": wall, "unit": "s", "iterations": its,
                           "energy_start": e0, "energy_end": e}), flush=True)
+    elif w == "warm":
+        from nemo3d_b200 import warmstart as ws
+        G, cells = 16, (20, 20, 14)
+        t = time.time()
+        train = [ws.solve_sample(workloads.random_lens(s, cells), G)
+                 for s in range(args.warm_train)]
+        train = [x for x in train if x is not None]
+        t_data = time.time() - t
+        net = ws.WarmStartNet(G=G, seed=0)
+        torch.cuda.synchronize()
+        t = time.time()
+        hist = net.fit(train, epochs=args.warm_epochs, batch=8)
+        torch.cuda.synchronize()
+        t_fit = time.time() - t
+        # one untimed solve first, so that neither arm pays the first-call costs
+        H = tbgpu.Hamiltonian(workloads.random_lens(99_999, cells), ws.MODEL, ws._mats())
+        ws.warm_solve(H, net)
+        H.close()
+        rows = []
+        for s in range(args.warm_test):
+            st = workloads.random_lens(100_000 + s, cells)
+            H = tbgpu.Hamiltonian(st, ws.MODEL, ws._mats())
+            out = {}
+            for name, model in (("cold", None), ("warm", net)):
+                torch.cuda.synchronize()
+                t0 = time.time()
+                res = ws.warm_solve(H, model)
+                out[name] = (res, time.time() - t0)
+            c, wv = out["cold"][0], out["warm"][0]
+            ok = c["edges"] is not None and wv["edges"] is not None
+            rows.append(dict(
+                iters_cold=c["iterations"], iters_warm=wv["iterations"],
+                wall_cold=out["cold"][1], wall_warm=out["warm"][1], warm_used=wv["warm"],
+                dE=float(np.abs(c["edges"] - wv["edges"]).max()) if ok else None,
+                sigma_err=abs(wv["sigma"] - 0.5 * (c["edges"][3] + c["edges"][4]))
+                if c["edges"] is not None else None,
+                edges_cold=None if c["edges"] is None else [float(e) for e in c["edges"]],
+                edges_warm=None if wv["edges"] is None else [float(e) for e in wv["edges"]]))
+            H.close()
+        ic = np.array([r["iters_cold"] for r in rows], float)
+        iw = np.array([r["iters_warm"] for r in rows], float)
+        print(json.dumps({
+            "workload": "warm", "metric": "Lanczos iterations to 4 h + 4 e levels, warm / cold",
+            "value": float(iw.sum() / ic.sum()), "unit": "ratio",
+            "iterations_cold_mean": float(ic.mean()), "iterations_warm_mean": float(iw.mean()),
+            "wall_cold_mean_s": float(np.mean([r["wall_cold"] for r in rows])),
+            "wall_warm_mean_s": float(np.mean([r["wall_warm"] for r in rows])),
+            "iterations_cold_median": float(np.median(ic)),
+            "iterations_warm_median": float(np.median(iw)),
+            "warm_used": int(sum(r["warm_used"] for r in rows)), "test_dots": len(rows),
+            "max_dE_eV": max([r["dE"] for r in rows if r["dE"] is not None], default=None),
+            "sigma_err_mean_eV": float(np.mean([r["sigma_err"] for r in rows
+                                                if r["sigma_err"] is not None])),
+            "train_dots": len(train), "train_iterations_mean": float(np.mean(
+                [x["iterations"] for x in train])), "data_s": t_data, "fit_s": t_fit,
+            "loss_first": hist[0], "loss_last": hist[-1], "grid": G, "cells": list(cells),
+            "per_dot": rows}), flush=True)
 
 
 def main():
@@ -504,8 +566,12 @@ def main():
                     help="with --profile-case: a few Keating VFF iterations instead")
     ap.add_argument("--spmv-variant", type=int, default=0, choices=[0, 1, 2, 3],
                     help="H*x kernel of the solve (tbgpu_set_spmv_variant)")
+    ap.add_argument("--warm-train", type=int, default=64,
+                    help="--workload warm: training dots")
+    ap.add_argument("--warm-test", type=int, default=16, help="--workload warm: held-out dots")
+    ap.add_argument("--warm-epochs", type=int, default=300, help="--workload warm: epochs")
     ap.add_argument("--workload", default="dome1M",
-                    choices=["dome1M", "kernels", "mixed2M", "batch256", "vff1M"],
+                    choices=["dome1M", "kernels", "mixed2M", "batch256", "vff1M", "warm"],
                     help="dome1M: the headline bench; the others: measurements beside it")
     ap.add_argument("--ref-iterations", type=int, default=19002,
                     help="iterations of a full solve (both passes) the CPU sample is scaled to")

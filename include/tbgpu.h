@@ -33,6 +33,8 @@
 #ifndef TBGPU_H
 #define TBGPU_H
 
+#include <stdint.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -388,6 +390,45 @@ int tbgpu_momentum_matrix(tbgpu_ctx *ctx, int n, const double *psi_dev, const do
                           double *P, double *trans);
 
 /* Timing of the last solve / build (ms, CUDA events on the context stream). */
+/* ---- Learned warm start (no counterpart in the reference) -------------
+ * A 3-D convolutional network on a G^3 grid over the structure's cells
+ * predicts the in-gap shift sigma and K band-edge envelopes, which shape the
+ * Lanczos start vector (the r_0 seam of tbgpu_eigensolve_lanczos, where the
+ * reference uses rand() or a file).  These are its kernels; the network,
+ * its training loop and the cold-start fallback are host code
+ * (nemo3d_b200/warmstart.py).  Device pointers; activations float
+ * [n][c][G^3] (voxel index (x*G + y)*G + z, cell i in voxel i*G/nx),
+ * weights bf16 [cout][cin][27] (tap (dx+1)*9 + (dy+1)*3 + dz+1), float
+ * accumulation; channels 1..32, G 1..64, else TBGPU_E_ARG.  The
+ * context-free kernels run on the legacy default stream. */
+/* features [3][G^3]: In fraction of the cation sites (species in_species),
+ * site occupancy, mean displacement length (pm); synchronous */
+int tbgpu_ws_features(tbgpu_ctx *ctx, int G, int in_species, float *feat_dev);
+/* out = conv(in) + bias, ReLU on the output when relu != 0 */
+int tbgpu_ws_conv3d_fwd(const float *in_dev, const uint16_t *w_dev, const float *bias_dev,
+                        float *out_dev, int n, int cin, int cout, int G, int relu);
+/* din = conv^T(g), g = dout masked by act > 0 (act = the layer's stored
+ * ReLU output, or NULL for a linear layer) */
+int tbgpu_ws_conv3d_bwd_data(const float *dout_dev, const float *act_dev, const uint16_t *w_dev,
+                             float *din_dev, int n, int cin, int cout, int G);
+/* dw [cout][cin][27] and db [cout] from the layer input and g as above */
+int tbgpu_ws_conv3d_bwd_weight(const float *in_dev, const float *dout_dev, const float *act_dev,
+                               float *dw_dev, float *db_dev, int n, int cin, int cout, int G);
+/* out [n][k+1][G^3]: sigma_pred[n] = grid mean of channel k.  With targets
+ * env [n][k][G^3] and sigma [n]: loss = mean (out - env)^2 over the first k
+ * channels + w_sigma * mean_n (sigma_pred - sigma)^2, dout its gradient;
+ * env = NULL computes sigma_pred alone */
+int tbgpu_ws_loss(const float *out_dev, const float *env_dev, const float *sigma_dev, int n, int k,
+                  int G, float w_sigma, float *dout_dev, float *sigma_pred_dev, float *loss_dev);
+/* Adam step (bias-corrected, step >= 1) on float w; wbf = bf16(w) */
+int tbgpu_ws_adam(float *w_dev, uint16_t *wbf_dev, const float *g_dev, float *m_dev,
+                  float *v_dev, long n, float lr, float b1, float b2, float eps, int step);
+/* r0[a][o] = u[a][o] * sqrt(sum_q env[q][voxel(a)]^2 prof[q][sub(a)][o] +
+ * floor_w), sub = 0 for cation sites, 1 for anion sites; u and r0 complex
+ * [dimension] (each part scaled); synchronous */
+int tbgpu_ws_start_vector(tbgpu_ctx *ctx, const float *env_dev, const float *prof_dev, int k,
+                          int G, float floor_w, const double *u_dev, double *r0_dev);
+
 typedef struct {
   double build_ms;            /* topology + assembly                          */
   double solve_ms;            /* eigensolve_lanczos, first pass               */

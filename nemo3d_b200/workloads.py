@@ -158,3 +158,49 @@ def pack_dots(dots, gap: int = 1):
     st = Structure(nx, ny, nz, tuple(lat), (False, False, False), t, dsp,
                    f"packed_{len(dots)}_dots", dict(ndots=len(dots)))
     return st, np.asarray(bounds, np.int32)
+
+
+def lens_dot(cells=(20, 20, 14), base_nm: float = 6.0, height_nm: float = 2.0,
+             x_in: float = 0.8, center=(0.5, 0.5), wl_z_frac: float = 0.3,
+             sigma_frac: float = 0.005, seed: int = 0, a: float = A_GAAS) -> Structure:
+    """In(x)Ga(1-x)As lens on a one-monolayer wetting layer of the same alloy
+    in a GaAs box: the half-ellipsoid of ``dome_in_box`` with its axis at the
+    fractional position ``center`` of the box in x, y, every cation site of
+    the lens and the layer In with probability ``x_in`` (independent per
+    site), Gaussian displacements as in ``dome_in_box``; all draws from
+    ``seed``.  The randomized dots the learned warm start is trained on."""
+    nx, ny, nz = cells
+    rng = np.random.default_rng(seed)
+    t = _binary(nx, ny, nz)
+    st = Structure(nx, ny, nz, (a, a, a), (False, False, False), t, None,
+                   f"InGaAs_lens_{nx}x{ny}x{nz}_s{seed}")
+    pos = st.site_positions()
+    z0 = wl_z_frac * nz * a
+    cx, cy = center[0] * nx * a - 0.5 * a, center[1] * ny * a - 0.5 * a
+    cat = pos[..., :4, :]
+    wl = (cat[..., 2] >= z0 - 0.5 * a) & (cat[..., 2] < z0)
+    rb, h = 0.5 * base_nm, height_nm
+    lens = (cat[..., 2] >= z0) & (((cat[..., 0] - cx) / rb) ** 2 +
+                                  ((cat[..., 1] - cy) / rb) ** 2 +
+                                  ((cat[..., 2] - z0) / h) ** 2 <= 1.0)
+    sub = t[..., :4]
+    alloy = rng.random(sub.shape) < x_in
+    sub[(wl | lens) & alloy] = SPECIES["In"]
+    if sigma_frac > 0:
+        sigma = sigma_frac * np.sqrt(3.0) / 4.0 * a
+        st.dsp = rng.normal(0.0, sigma, size=(nx, ny, nz, 8, 3))
+    st.info = dict(base_nm=base_nm, height_nm=height_nm, x_in=x_in, center=tuple(center),
+                   seed=seed, n_in=int((sub == SPECIES["In"]).sum()))
+    return st
+
+
+def random_lens(seed: int, cells=(20, 20, 14)) -> Structure:
+    """One draw of the warm start's training distribution: base 4-7 nm,
+    height 1.5-3 nm, x_in uniform in [0.4, 1.0], lens axis uniform in the
+    middle half of the box (all from ``seed``)."""
+    rng = np.random.default_rng(10_000 + seed)
+    base = rng.uniform(4.0, 7.0)
+    height = rng.uniform(1.5, 3.0)
+    x_in = rng.uniform(0.4, 1.0)
+    center = tuple(rng.uniform(0.25, 0.75, 2))
+    return lens_dot(cells, base, height, x_in, center, seed=seed)
