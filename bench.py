@@ -380,6 +380,7 @@ def run_extra(args):
         for name, opts, f32, var in (
                 ("fp64 store", {}, False, 0),
                 ("fp64 store, two-cell units (variant 3)", {}, False, 3),
+                ("fp64 store, cation block runs by bulk copy (variant 4)", {}, False, 4),
                 ("float store, float vectors", dict(ham_bits=32, lanczos_bits=32), True, 0),
                 ("recompute fp64", dict(recompute=True), False, 0),
                 ("recompute float", dict(recompute=True, lanczos_bits=32), True, 0)):
@@ -564,7 +565,7 @@ def main():
                     help="with --profile-case: FP64 or the mixed-precision Lanczos")
     ap.add_argument("--profile-vff", action="store_true",
                     help="with --profile-case: a few Keating VFF iterations instead")
-    ap.add_argument("--spmv-variant", type=int, default=0, choices=[0, 1, 2, 3],
+    ap.add_argument("--spmv-variant", type=int, default=0, choices=[0, 1, 2, 3, 4],
                     help="H*x kernel of the solve (tbgpu_set_spmv_variant)")
     ap.add_argument("--warm-train", type=int, default=64,
                     help="--workload warm: training dots")

@@ -308,7 +308,9 @@ int tbgpu_hx_dot_noalloc(tbgpu_ctx *ctx, double shift, const double *x_dev,
  * 1 = lane-gather kernel for every model, 2 = warp-staged kernel with
  * 7 warps x 2 stages, 3 = two-cell unit kernel (bulk copies of each unit's
  * contiguous pieces; 10-orbital models with the 64-bit store at the Gamma
- * point, else as 0).  Every variant gives the same y bit for bit. */
+ * point, else as 0), 4 = the default kernel with each cation's block run
+ * staged by one bulk copy (TMA) instead of 16-byte copies.  Every variant
+ * gives the same y bit for bit. */
 int tbgpu_set_spmv_variant(tbgpu_ctx *ctx, int variant);
 
 /* Lanczos for many independent dots at once (no counterpart in the

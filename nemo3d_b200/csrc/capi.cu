@@ -348,7 +348,7 @@ int tbgpu_export_hamiltonian(const tbgpu_ctx *ctx, double *onsite, double *block
 }
 
 int tbgpu_set_spmv_variant(tbgpu_ctx *ctx, int variant) {
-  if (!ctx || variant < 0 || variant > 3) return set_error(TBGPU_E_ARG);
+  if (!ctx || variant < 0 || variant > 4) return set_error(TBGPU_E_ARG);
   C(ctx)->spmv_variant = variant;
   return TBGPU_OK;
 }

@@ -20,6 +20,14 @@
 // (A variant that gathered the same bytes with one 1-D TMA bulk copy per
 // 300-800-byte segment took 2.4 ms per launch on the 1.02M-atom dot: that
 // many small requests are limited by the TMA request rate, not by HBM.)
+//
+// BULK (H*x variant 4): a cation's four blocks, one contiguous 3200-byte
+// run, arrive by one 1-D bulk copy (cp.async.bulk, no multicast) issued by
+// lane 0 on an mbarrier of the warp's stage instead of 200 16-byte cp.async
+// copies, which takes about a third of the staging writes off the
+// load/store unit.  The wait on the mbarrier is bounded: a warp whose copy
+// does not arrive reports TBGPU_E_TIMEOUT in the status word, waits once
+// more for its copies in flight and leaves its loop.
 #include <cstdint>
 
 #include "tbgpu_internal.cuh"
@@ -76,13 +84,28 @@ struct Layout {
   static __device__ __forceinline__ int ons(int i) { return i * ATOM + 4 * BLK * HS + 5 * NB * VS; }
 };
 
-// Issue the copies of group g into one stage (all lanes; no wait).
-template <class L>
+// Issue the copies of group g into one stage (all lanes; no wait).  BULK:
+// the cations' block runs as bulk copies on the stage's mbarrier mb (lane 0
+// always arrives once, with the byte count, even for a group without
+// cations).
+template <class L, bool BULK = false>
 __device__ __forceinline__ void issue(unsigned char *st, long g, const Meta &M, int lane,
                                       const typename L::HT *__restrict__ onsite,
                                       const typename L::HT *__restrict__ blocks,
-                                      const typename L::VT *__restrict__ x) {
+                                      const typename L::VT *__restrict__ x, uint32_t mb = 0) {
   constexpr int NB = L::NB;
+  if (BULK && lane == 0) {
+    uint32_t ncat = 0;
+#pragma unroll
+    for (int i = 0; i < kAPW; i++) ncat += M.m[i] >= 0 && M.m[i] < 4;
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(mb, ncat * uint32_t(4 * L::BLK * L::HS));
+#pragma unroll
+    for (int i = 0; i < kAPW; i++)
+      if (M.m[i] >= 0 && M.m[i] < 4)
+        bulk_g2s(smem_addr(st + L::blk(i)), blocks + (long(M.a0) + i) * 4 * L::BLK,
+                 uint32_t(4 * L::BLK * L::HS), mb);
+  }
 #pragma unroll
   for (int i = 0; i < kAPW; i++) {
     const int m = M.m[i];
@@ -91,9 +114,12 @@ __device__ __forceinline__ void issue(unsigned char *st, long g, const Meta &M, 
     const bool cat = m < 4;
     unsigned char *bk = st + L::blk(i);
     if (cat) {  // the cation's four blocks are one contiguous run
-      const unsigned char *src = reinterpret_cast<const unsigned char *>(blocks + a * 4 * L::BLK);
+      if (!BULK) {
+        const unsigned char *src =
+            reinterpret_cast<const unsigned char *>(blocks + a * 4 * L::BLK);
 #pragma unroll
-      for (int c = lane; c < 4 * L::BLK_CH; c += 32) cp16(bk + c * 16, src + c * 16);
+        for (int c = lane; c < 4 * L::BLK_CH; c += 32) cp16(bk + c * 16, src + c * 16);
+      }
     } else {
       // a missing neighbour (surface) is zero-filled, not skipped
 #pragma unroll
@@ -126,20 +152,31 @@ __device__ __forceinline__ void issue(unsigned char *st, long g, const Meta &M, 
 }
 
 template <int NSPIN, bool DOT, int WARPS, int STAGES, typename HT = double,
-          typename VT = double2>
+          typename VT = double2, bool BULK = false>
 __global__ void __launch_bounds__(WARPS * 32, 1)
     k_spmv_async(long ngroups, const int2 *__restrict__ groups, const int4 *__restrict__ nbr,
                  const unsigned char *__restrict__ site_m, const HT *__restrict__ onsite,
                  const HT *__restrict__ blocks, const VT *__restrict__ x,
                  VT *__restrict__ y, double shift_d, const double *__restrict__ xnorm,
                  int xnorm_idx, double *partial, unsigned int *counter, double *alpha_out,
-                 int alpha_idx, const unsigned char *__restrict__ skip) {
+                 int alpha_idx, const unsigned char *__restrict__ skip, int *status = nullptr) {
   using L = Layout<NSPIN, WARPS, STAGES, HT, VT>;
   using RT = typename L::RT;
   constexpr int NB = L::NB;
   extern __shared__ __align__(128) unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   unsigned char *wbase = smem + warp * L::WARP;
+  // BULK: one mbarrier per stage of this warp, after the stages
+  const uint32_t mb0 = smem_addr(smem + L::SMEM) + uint32_t(warp * STAGES * 8);
+  uint32_t phase = 0;  // bit s: parity of stage s's next completion
+  if (BULK) {
+    if (lane == 0) {
+#pragma unroll
+      for (int s = 0; s < STAGES; s++) mbar_init(mb0 + 8 * s, 1);
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();
+  }
   const int ai = lane / kNorb, o = lane - ai * kNorb;
   const RT scale = RT(xnorm ? 1.0 / xnorm[xnorm_idx] : 1.0);
   const RT shift = RT(shift_d);
@@ -148,7 +185,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
   long g = long(blockIdx.x) * WARPS + warp;
   // prologue: copies of the first group in flight, metadata of the next
   Meta cur = load_meta(g, ngroups, groups, nbr, site_m, skip);
-  if (STAGES > 1 && g < ngroups) issue<L>(wbase, g, cur, lane, onsite, blocks, x);
+  if (STAGES > 1 && g < ngroups) issue<L, BULK>(wbase, g, cur, lane, onsite, blocks, x, mb0);
   cp_commit();
   Meta nxt = load_meta(g + nw, ngroups, groups, nbr, site_m, skip);
   int k = 0;
@@ -156,15 +193,27 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
     const long gn = g + nw;
     unsigned char *st = wbase + (k % STAGES) * L::STAGE;
     if (STAGES > 1) {  // next group's copies overlap this group's compute
-      if (gn < ngroups) issue<L>(wbase + ((k + 1) % STAGES) * L::STAGE, gn, nxt, lane, onsite,
-                                 blocks, x);
+      if (gn < ngroups)
+        issue<L, BULK>(wbase + ((k + 1) % STAGES) * L::STAGE, gn, nxt, lane, onsite, blocks, x,
+                       mb0 + 8 * ((k + 1) % STAGES));
       cp_commit();
     } else {           // single stage: other warps overlap this one's wait
-      issue<L>(st, g, cur, lane, onsite, blocks, x);
+      issue<L, BULK>(st, g, cur, lane, onsite, blocks, x, mb0);
       cp_commit();
     }
     const Meta nn = load_meta(gn + nw, ngroups, groups, nbr, site_m, skip);  // two groups ahead
     if (STAGES > 1) cp_wait<1>(); else cp_wait<0>();  // this lane's copies of g landed
+    if (BULK) {  // and the stage's bulk copies (warp-uniform decision)
+      const int s = k % STAGES;
+      const uint32_t par = (phase >> s) & 1u;
+      const bool late = !mbar_wait(mb0 + 8 * s, par);
+      if (__any_sync(0xffffffffu, late)) {
+        if (lane == 0 && status) atomicExch(status, TBGPU_E_TIMEOUT);
+        mbar_wait(mb0 + 8 * s, par);
+        break;
+      }
+      phase ^= 1u << s;
+    }
     __syncwarp();   // ... and every lane's
     // this lane's atom, selected without indexing the metadata at run time
     const int m = ai == 0 ? cur.m[0] : ai == 1 ? cur.m[1] : ai == 2 ? cur.m[2] : -1;
@@ -262,15 +311,17 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
   if (DOT) grid_reduce<WARPS * 32>(dot, partial, counter, alpha_out, alpha_idx, false);
 }
 
-template <int NSPIN, bool DOT, int WARPS, int STAGES, typename HT, typename VT = double2>
+template <int NSPIN, bool DOT, int WARPS, int STAGES, typename HT, typename VT = double2,
+          bool BULK = false>
 int launch_async_t(Ctx &c, const void *x, void *y, double shift, const double *xnorm,
                    int xidx, double *alpha_out, int aidx, cudaStream_t s) {
   using L = Layout<NSPIN, WARPS, STAGES, HT, VT>;
+  constexpr int smem = L::SMEM + (BULK ? WARPS * STAGES * 8 : 0);
   static int sms = 0;
   if (!sms) {
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device);
-    if (cudaFuncSetAttribute(k_spmv_async<NSPIN, DOT, WARPS, STAGES, HT, VT>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM) != cudaSuccess)
+    if (cudaFuncSetAttribute(k_spmv_async<NSPIN, DOT, WARPS, STAGES, HT, VT, BULK>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
       return set_error(TBGPU_E_CUDA);
   }
   const unsigned grid = unsigned(sms);
@@ -278,26 +329,28 @@ int launch_async_t(Ctx &c, const void *x, void *y, double shift, const double *x
     int rc = ensure_partials(c, int(grid));
     if (rc) return rc;
   }
-  k_spmv_async<NSPIN, DOT, WARPS, STAGES, HT, VT><<<grid, WARPS * 32, L::SMEM, s>>>(
+  k_spmv_async<NSPIN, DOT, WARPS, STAGES, HT, VT, BULK><<<grid, WARPS * 32, smem, s>>>(
       c.ngroups, c.d_groups, c.d_nbr, c.d_site_m, ham_onsite<HT>(c), ham_blocks<HT>(c),
       reinterpret_cast<const VT *>(x), reinterpret_cast<VT *>(y), shift, xnorm, xidx,
-      DOT ? c.d_partial : nullptr, DOT ? c.d_counter : nullptr, alpha_out, aidx, c.d_skip);
+      DOT ? c.d_partial : nullptr, DOT ? c.d_counter : nullptr, alpha_out, aidx, c.d_skip,
+      c.d_status);
   TB_CUDA(cudaGetLastError());
   return TBGPU_OK;
 }
 
 }  // namespace
 
-template <int WARPS, int STAGES, typename HT>
+template <int WARPS, int STAGES, typename HT, bool BULK = false>
 int launch_cfg(Ctx &c, const double *x, double *y, double shift, const double *xnorm, int xidx,
                double *alpha_out, int aidx, cudaStream_t s) {
+  using V = double2;
   if (c.nspin == 2)
     return alpha_out
-               ? launch_async_t<2, true, WARPS, STAGES, HT>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s)
-               : launch_async_t<2, false, WARPS, STAGES, HT>(c, x, y, shift, xnorm, xidx, nullptr, 0, s);
+               ? launch_async_t<2, true, WARPS, STAGES, HT, V, BULK>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s)
+               : launch_async_t<2, false, WARPS, STAGES, HT, V, BULK>(c, x, y, shift, xnorm, xidx, nullptr, 0, s);
   return alpha_out
-             ? launch_async_t<1, true, WARPS, STAGES, HT>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s)
-             : launch_async_t<1, false, WARPS, STAGES, HT>(c, x, y, shift, xnorm, xidx, nullptr, 0, s);
+             ? launch_async_t<1, true, WARPS, STAGES, HT, V, BULK>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s)
+             : launch_async_t<1, false, WARPS, STAGES, HT, V, BULK>(c, x, y, shift, xnorm, xidx, nullptr, 0, s);
 }
 
 // complex-float vectors over the single-precision store, float accumulation
@@ -326,6 +379,8 @@ int launch_spmv_async(Ctx &c, const double *x, double *y, double shift, const do
     return launch_cfg<16, 1, float>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
   if (c.spmv_variant == 2)
     return launch_cfg<7, 2, double>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
+  if (c.spmv_variant == 4)
+    return launch_cfg<14, 1, double, true>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
   return launch_cfg<14, 1, double>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
 }
 

@@ -45,41 +45,6 @@ constexpr int kCatRun = 4 * 4 * kBlkBytes;         // a cell's four cations' blo
 constexpr int kHdr = 8;
 constexpr int kOffM = kHdr, kOffX = kOffM + kUnitAtoms, kOffB = kOffX + 4 * kUnitAtoms;
 constexpr int kOffItems = kOffB + 4 * kUnitAtoms;
-constexpr long kWaitLimit = 1L << 20;  // mbarrier polls before giving up
-
-__device__ __forceinline__ void mbar_init(uint32_t mb, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mb), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint32_t mb, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint32_t mb, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-      " selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(ok)
-      : "r"(mb), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// bounded wait for the phase of the given parity; false when it ran out
-__device__ __forceinline__ bool mbar_wait(uint32_t mb, uint32_t parity) {
-  for (long polls = 0; polls < kWaitLimit; polls++)
-    if (mbar_try_wait(mb, parity)) return true;
-  return false;
-}
-// 1-D bulk copy global -> shared with completion on mbarrier mb (addresses
-// and size multiples of 16 bytes)
-__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes,
-                                         uint32_t mb) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-          dst),
-      "l"(src), "r"(bytes), "r"(mb)
-      : "memory");
-}
 
 // the arithmetic helpers of k_spmv_async, so both kernels round alike
 __device__ __forceinline__ void cfma_r(double2 &acc, double v, double2 a) {

@@ -33,6 +33,44 @@ __device__ __forceinline__ void cp_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
+// 1-D bulk copies (cp.async.bulk, no multicast) complete on an mbarrier in
+// the copying CTA's shared memory; waits on it are bounded.
+constexpr long kWaitLimit = 1L << 20;  // mbarrier polls before giving up
+
+__device__ __forceinline__ void mbar_init(uint32_t mb, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mb), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t mb, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t mb, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(mb), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait for the phase of the given parity; false when it ran out
+__device__ __forceinline__ bool mbar_wait(uint32_t mb, uint32_t parity) {
+  for (long polls = 0; polls < kWaitLimit; polls++)
+    if (mbar_try_wait(mb, parity)) return true;
+  return false;
+}
+// 1-D bulk copy global -> shared with completion on mbarrier mb (addresses
+// and size multiples of 16 bytes)
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes,
+                                         uint32_t mb) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          dst),
+      "l"(src), "r"(bytes), "r"(mb)
+      : "memory");
+}
+
 struct Meta {
   int nb[kAPW][4];
   int m[kAPW];  // -1: no atom

@@ -217,7 +217,7 @@ def test_spmv_variants_match_oracle(model):
     x = np.random.default_rng(3).uniform(-1, 1, 2 * g.n)
     scale = max(np.abs(o.onsite).max(), np.abs(o.blocks).max())
     yo = o.hx(x, 0.7)
-    for variant in (0, 1, 2, 3):
+    for variant in (0, 1, 2, 3, 4):
         g.set_spmv_variant(variant)
         assert np.abs(g.matvect_mult(x, 0.7) - yo).max() <= 1e-12 * scale * 45, variant
 

@@ -102,11 +102,40 @@ def test_tile_other_models_fall_back():
     np.testing.assert_array_equal(g.matvect_mult(x, 0.2), y0)
 
 
+@pytest.mark.parametrize("name", list(STRUCTURES))
+@pytest.mark.parametrize("model", ["sp3d5s*", "sp3d5s*_so"])
+def test_bulk_block_runs_bit_identical(name, model):
+    """Variant 4 (cation block runs by bulk copy) stages the same bytes for
+    the same arithmetic as variant 0."""
+    g, _ = _ham(STRUCTURES[name](), model)
+    x = np.random.default_rng(23).uniform(-1, 1, 2 * g.n)
+    for shift in (0.0, 0.6):
+        g.set_spmv_variant(0)
+        y0 = g.matvect_mult(x, shift)
+        g.set_spmv_variant(4)
+        np.testing.assert_array_equal(g.matvect_mult(x, shift), y0)
+
+
+def test_bulk_lanczos_matches_default():
+    st = workloads.dome_in_box(cells=(8, 8, 6), base_nm=3.0, height_nm=1.2, wl_z_nm=1.2,
+                               sigma_frac=0.01, seed=2)
+    g, _ = _ham(st, "sp3d5s*_so")
+    r0 = workloads.random_start(g.n, seed=0)
+    kw = dict(imax=3000, requested1=3, requested2=3, emin1=-0.6, emax1=0.3, emin2=0.8,
+              emax2=2.4, tolerance=1e-7)
+    g.set_spmv_variant(0)
+    ref = g.eigensolve_lanczos(r0, **kw)
+    g.set_spmv_variant(4)
+    res = g.eigensolve_lanczos(r0, **kw)
+    assert res["iterations"] == ref["iterations"]
+    np.testing.assert_array_equal(res["values"], ref["values"])
+
+
 def test_tile_variant_range():
     from nemo3d_b200.tbgpu import TbgpuError
     g, _ = _ham(STRUCTURES["dome_7x6x5"](), "sp3d5s*")
     with pytest.raises(TbgpuError):
-        g.set_spmv_variant(4)
+        g.set_spmv_variant(5)
 
 
 def test_tile_lanczos_matches_default():
