@@ -380,7 +380,7 @@ def run_extra(args):
         for name, opts, f32, var in (
                 ("fp64 store", {}, False, 0),
                 ("fp64 store, two-cell units (variant 3)", {}, False, 3),
-                ("fp64 store, cation block runs by bulk copy (variant 4)", {}, False, 4),
+                ("fp64 store, every piece by cp.async (variant 4)", {}, False, 4),
                 ("float store, float vectors", dict(ham_bits=32, lanczos_bits=32), True, 0),
                 ("recompute fp64", dict(recompute=True), False, 0),
                 ("recompute float", dict(recompute=True, lanczos_bits=32), True, 0)):

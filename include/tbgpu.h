@@ -303,14 +303,16 @@ int tbgpu_export_hamiltonian(const tbgpu_ctx *ctx, double *onsite,
 int tbgpu_hx_dot_noalloc(tbgpu_ctx *ctx, double shift, const double *x_dev,
                          double *y_dev, double *dot_dev);
 
-/* H*x kernel: 0 = default (warp-staged cp.async kernel, 14 warps x 1 stage
- * per SM, for the 10-orbital models; lane-gather kernel otherwise),
+/* H*x kernel: 0 = default (warp-staged kernel, 14 warps x 1 stage per SM,
+ * each cation's block run by one bulk copy (TMA), the other pieces by
+ * 16-byte cp.async, for the 10-orbital models; lane-gather kernel
+ * otherwise),
  * 1 = lane-gather kernel for every model, 2 = warp-staged kernel with
  * 7 warps x 2 stages, 3 = two-cell unit kernel (bulk copies of each unit's
  * contiguous pieces; 10-orbital models with the 64-bit store at the Gamma
- * point, else as 0), 4 = the default kernel with each cation's block run
- * staged by one bulk copy (TMA) instead of 16-byte copies.  Every variant
- * gives the same y bit for bit. */
+ * point, else as 0), 4 = the default kernel with every piece, the cation
+ * block runs included, by 16-byte cp.async.  Every variant gives the same
+ * y bit for bit. */
 int tbgpu_set_spmv_variant(tbgpu_ctx *ctx, int variant);
 
 /* Lanczos for many independent dots at once (no counterpart in the

@@ -21,11 +21,12 @@
 // 300-800-byte segment took 2.4 ms per launch on the 1.02M-atom dot: that
 // many small requests are limited by the TMA request rate, not by HBM.)
 //
-// BULK (H*x variant 4): a cation's four blocks, one contiguous 3200-byte
-// run, arrive by one 1-D bulk copy (cp.async.bulk, no multicast) issued by
-// lane 0 on an mbarrier of the warp's stage instead of 200 16-byte cp.async
-// copies, which takes about a third of the staging writes off the
-// load/store unit.  The wait on the mbarrier is bounded: a warp whose copy
+// BULK (the default; variant 4 turns it off): a cation's four blocks, one
+// contiguous 3200-byte run, arrive by one 1-D bulk copy (cp.async.bulk, no
+// multicast) issued by lane 0 on an mbarrier of the warp's stage instead of
+// 200 16-byte cp.async copies, which takes about a third of the staging
+// copies off the load/store unit (the bytes written to shared memory stay
+// the same, and so does most of the time: 0.668 against 0.674 ms).  The wait on the mbarrier is bounded: a warp whose copy
 // does not arrive reports TBGPU_E_TIMEOUT in the status word, waits once
 // more for its copies in flight and leaves its loop.
 #include <cstdint>
@@ -371,17 +372,18 @@ int launch_spmv_async_f32(Ctx &c, const float *x, float *y, double shift, const 
 int launch_spmv_async(Ctx &c, const double *x, double *y, double shift, const double *xnorm,
                       int xidx, double *alpha_out, int aidx, cudaStream_t s) {
   if (c.norb != kNorb) return set_error(TBGPU_E_UNSUPPORTED);
-  // variant 0: 14 warps x 1 stage per SM (other warps cover a warp's wait;
-  // 0.82 ms per launch on the 1.02M-atom dot); variant 2: 7 warps x 2
-  // stages (each warp overlaps its own next copies; 0.91 ms)
-  // single-precision store: half the block bytes, 16 warps fit
+  // variant 0: 14 warps x 1 stage per SM (other warps cover a warp's wait),
+  // cation block runs by bulk copy (0.668 ms per launch on the 1.02M-atom
+  // dot); variant 4: the same with every piece by cp.async (0.674 ms);
+  // variant 2: 7 warps x 2 stages (each warp overlaps its own next copies;
+  // 0.91 ms).  Single-precision store: half the block bytes, 16 warps fit.
   if (c.ham_fp32)
     return launch_cfg<16, 1, float>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
   if (c.spmv_variant == 2)
     return launch_cfg<7, 2, double>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
   if (c.spmv_variant == 4)
-    return launch_cfg<14, 1, double, true>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
-  return launch_cfg<14, 1, double>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
+    return launch_cfg<14, 1, double>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
+  return launch_cfg<14, 1, double, true>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
 }
 
 template <int NSPIN, int WARPS, typename HT>

@@ -105,8 +105,8 @@ def test_tile_other_models_fall_back():
 @pytest.mark.parametrize("name", list(STRUCTURES))
 @pytest.mark.parametrize("model", ["sp3d5s*", "sp3d5s*_so"])
 def test_bulk_block_runs_bit_identical(name, model):
-    """Variant 4 (cation block runs by bulk copy) stages the same bytes for
-    the same arithmetic as variant 0."""
+    """Variant 0 (cation block runs by bulk copy) and variant 4 (by cp.async)
+    stage the same bytes for the same arithmetic."""
     g, _ = _ham(STRUCTURES[name](), model)
     x = np.random.default_rng(23).uniform(-1, 1, 2 * g.n)
     for shift in (0.0, 0.6):
