@@ -311,9 +311,18 @@ int tbgpu_hx_dot_noalloc(tbgpu_ctx *ctx, double shift, const double *x_dev,
  * 7 warps x 2 stages, 3 = two-cell unit kernel (bulk copies of each unit's
  * contiguous pieces; 10-orbital models with the 64-bit store at the Gamma
  * point, else as 0), 4 = the default kernel with every piece, the cation
- * block runs included, by 16-byte cp.async.  Every variant gives the same
- * y bit for bit. */
+ * block runs included, by 16-byte cp.async.  Variants 0, 2, 3 and 4 give
+ * the same y bit for bit; 1 sums in its own order (equal to rounding). */
 int tbgpu_set_spmv_variant(tbgpu_ctx *ctx, int variant);
+
+/* Autotuner: times the H*x variants that are distinct kernels for the built
+ * context (all five for the 10-orbital models with the 64-bit store at the
+ * Gamma point, 0 and 1 with the 32-bit store, only 0 for 5-orbital models,
+ * Bloch phases and recompute storage), reps launches each with the fused
+ * Lanczos dot after two untimed ones (CUDA events on the context stream;
+ * two temporary device vectors), selects the fastest (ties: the lower
+ * number) and returns it with its time per launch.  Synchronous. */
+int tbgpu_autotune_spmv(tbgpu_ctx *ctx, int reps, int *variant_out, double *ms_out);
 
 /* Lanczos for many independent dots at once (no counterpart in the
  * reference, which solves one structure per run): the context's grid holds

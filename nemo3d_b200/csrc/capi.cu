@@ -353,6 +353,84 @@ int tbgpu_set_spmv_variant(tbgpu_ctx *ctx, int variant) {
   return TBGPU_OK;
 }
 
+// The variants that launch distinct kernels for this context: all five for
+// the 10-orbital models with the double store at the Gamma point; the
+// warp-staged and the lane-gather kernel with the float store; one kernel
+// otherwise (5-orbital models, Bloch phases, recompute storage).
+static int distinct_variants(const Ctx &c, int *v) {
+  if (c.norb != 10 || c.bloch || c.recompute) {
+    v[0] = 0;
+    return 1;
+  }
+  if (c.ham_fp32) {
+    v[0] = 0;
+    v[1] = 1;
+    return 2;
+  }
+  for (int i = 0; i < 5; i++) v[i] = i;
+  return 5;
+}
+
+// Times the context's distinct H*x variants (the product with the fused
+// alpha dot, as the Lanczos recurrence launches it; CUDA events on the
+// context stream, two untimed launches first) and keeps the fastest (ties:
+// the lower number).
+int tbgpu_autotune_spmv(tbgpu_ctx *ctx, int reps, int *variant_out, double *ms_out) {
+  if (!ctx || reps < 1 || reps > 1000) return set_error(TBGPU_E_ARG);
+  Ctx &c = *C(ctx);
+  if (!c.built) return set_error(TBGPU_E_STATE);
+  set_error(TBGPU_OK);
+  const size_t bytes = sizeof(double) * 2 * size_t(c.natoms) * c.nb;
+  double *x = nullptr, *y = nullptr, *dot = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int rc = TBGPU_OK;
+  const int keep = c.spmv_variant;
+  int best = keep;
+  float best_ms = 0.0f;
+  if (cudaMalloc(&x, bytes) != cudaSuccess || cudaMalloc(&y, bytes) != cudaSuccess ||
+      cudaMalloc(&dot, sizeof(double)) != cudaSuccess) {
+    rc = TBGPU_E_NOMEM;
+  } else if (cudaMemsetAsync(x, 0, bytes, c.stream) != cudaSuccess ||
+             cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    rc = TBGPU_E_CUDA;
+  }
+  int cand[5];
+  const int ncand = distinct_variants(c, cand);
+  for (int ci = 0; ci < ncand && rc == TBGPU_OK; ci++) {
+    const int v = cand[ci];
+    c.spmv_variant = v;
+    for (int r = 0; r < reps + 2 && rc == TBGPU_OK; r++) {
+      if (r == 2 && cudaEventRecord(e0, c.stream) != cudaSuccess) rc = TBGPU_E_CUDA;
+      if (rc == TBGPU_OK) rc = launch_spmv(c, x, y, 0.0, nullptr, 0, dot, 0, c.stream);
+    }
+    float ms = 0.0f;
+    if (rc == TBGPU_OK && (cudaEventRecord(e1, c.stream) != cudaSuccess ||
+                           cudaEventSynchronize(e1) != cudaSuccess ||
+                           cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
+      rc = TBGPU_E_CUDA;
+    ms /= float(reps);
+    if (rc == TBGPU_OK && (ci == 0 || ms < best_ms)) {
+      best = v;
+      best_ms = ms;
+    }
+  }
+  c.spmv_variant = rc == TBGPU_OK ? best : keep;
+  if (c.spmv_variant != 3 && c.d_units) {  // the unit table only serves variant 3
+    cudaFree(c.d_units);
+    c.d_units = nullptr;
+    c.nunits = 0;
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFree(x);
+  cudaFree(y);
+  cudaFree(dot);
+  if (rc) return set_error(rc);
+  if (variant_out) *variant_out = best;
+  if (ms_out) *ms_out = double(best_ms);
+  return TBGPU_OK;
+}
+
 int tbgpu_set_ham_precision(tbgpu_ctx *ctx, int bits) {
   if (!ctx || (bits != 32 && bits != 64)) return set_error(TBGPU_E_ARG);
   Ctx &c = *C(ctx);

@@ -105,6 +105,7 @@ def _lib():
         L.tbgpu_export_hamiltonian.argtypes = [vp, vp, vp]
         L.tbgpu_set_profiling.argtypes = [vp, ip]
         L.tbgpu_set_spmv_variant.argtypes = [vp, ip]
+        L.tbgpu_autotune_spmv.argtypes = [vp, ip, vp, vp]
         L.tbgpu_get_stats.argtypes = [vp, C.POINTER(Stats)]
         _LIB = L
     return _LIB
@@ -441,6 +442,16 @@ class Hamiltonian:
         rc = _lib().tbgpu_set_spmv_variant(self._ctx, int(variant))
         if rc:
             raise TbgpuError(rc, "tbgpu_set_spmv_variant")
+
+    def autotune_spmv(self, reps: int = 10):
+        """Time every H*x variant on this structure and keep the fastest
+        (tbgpu_autotune_spmv); returns (variant, ms per launch)."""
+        v = C.c_int(-1)
+        ms = C.c_double(0.0)
+        rc = _lib().tbgpu_autotune_spmv(self._ctx, int(reps), C.byref(v), C.byref(ms))
+        if rc:
+            raise TbgpuError(rc, "tbgpu_autotune_spmv")
+        return v.value, ms.value
 
     def set_profiling(self, on=True):
         _lib().tbgpu_set_profiling(self._ctx, int(bool(on)))

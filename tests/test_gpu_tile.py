@@ -131,6 +131,25 @@ def test_bulk_lanczos_matches_default():
     np.testing.assert_array_equal(res["values"], ref["values"])
 
 
+def test_autotune_selects_a_variant_with_the_same_product():
+    g, _ = _ham(STRUCTURES["dome_20x18x13"](), "sp3d5s*_so")
+    x = np.random.default_rng(31).uniform(-1, 1, 2 * g.n)
+    g.set_spmv_variant(0)
+    y0 = g.matvect_mult(x, 0.3)
+    v, ms = g.autotune_spmv(reps=5)
+    assert v in range(5) and ms > 0.0
+    y = g.matvect_mult(x, 0.3)
+    if v == 1:  # the lane-gather kernel sums in its own order
+        ons, blk = g.export_hamiltonian()
+        assert np.abs(y - y0).max() <= 1e-13 * max(np.abs(ons).max(), np.abs(blk).max())
+    else:
+        np.testing.assert_array_equal(y, y0)
+    # a model with one H*x kernel: nothing to choose
+    h, _ = _ham(STRUCTURES["dome_7x6x5"](), "sp3s*_so", fam="sps")
+    v, ms = h.autotune_spmv(reps=3)
+    assert v == 0 and ms > 0.0
+
+
 def test_tile_variant_range():
     from nemo3d_b200.tbgpu import TbgpuError
     g, _ = _ham(STRUCTURES["dome_7x6x5"](), "sp3d5s*")
