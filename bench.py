@@ -532,6 +532,34 @@ def run_extra(args):
                 edges_cold=None if c["edges"] is None else [float(e) for e in c["edges"]],
                 edges_warm=None if wv["edges"] is None else [float(e) for e in wv["edges"]]))
             H.close()
+        # the bound on any start vector: the cold solve's own band-edge
+        # eigenvectors (random phases) plus a random part of relative weight
+        # eps, on the first held-out dots
+        ideal = []
+        for s in range(min(4, args.warm_test)):
+            st = workloads.random_lens(100_000 + s, cells)
+            H = tbgpu.Hamiltonian(st, ws.MODEL, ws._mats())
+            c = ws.warm_solve(H, None, vectors=ws.MAXVEC)
+            idx = ws.band_edges(c["values"], ws.SIGMA0)
+            if idx is None or idx[-1] >= len(c["vectors"]):
+                H.close()
+                continue
+            rng = np.random.default_rng(s)
+            u = workloads.random_start(H.n, seed=0)
+            uc = u[0::2] + 1j * u[1::2]
+            for eps in (1.0, 0.1):
+                v = sum(c["vectors"][i] * np.exp(2j * np.pi * rng.random()) for i in idx)
+                v = v / np.linalg.norm(v) + eps * uc / np.linalg.norm(uc)
+                r0 = np.empty(2 * H.n)
+                r0[0::2], r0[1::2] = v.real, v.imag
+                res = H.eigensolve_lanczos(r0, **ws.solve_kw(ws.SIGMA0))
+                e = ws.band_edges(res["values"], ws.SIGMA0)
+                ideal.append(dict(dot=s, eps=eps, iters_cold=c["iterations"],
+                                  iters_ideal=res["iterations"],
+                                  same_levels=e is not None and bool(np.abs(
+                                      np.asarray(res["values"])[e] - np.asarray(c["values"])[idx]
+                                  ).max() < 1e-6)))
+            H.close()
         ic = np.array([r["iters_cold"] for r in rows], float)
         iw = np.array([r["iters_warm"] for r in rows], float)
         print(json.dumps({
@@ -549,6 +577,7 @@ def run_extra(args):
             "train_dots": len(train), "train_iterations_mean": float(np.mean(
                 [x["iterations"] for x in train])), "data_s": t_data, "fit_s": t_fit,
             "loss_first": hist[0], "loss_last": hist[-1], "grid": G, "cells": list(cells),
+            "ideal_start": ideal,
             "per_dot": rows}), flush=True)
 
 
