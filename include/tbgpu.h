@@ -118,6 +118,10 @@ long tbgpu_dimension(const tbgpu_ctx *ctx); /* complex length n_atoms * nb */
  * unspecified and tbgpu_last_error() is set. */
 void tbgpu_matvect_mult(const int **argList, tbgpu_dcomplex *y,
                         const tbgpu_dcomplex *x);
+/* The same with device vectors (complex, interleaved doubles, 16-byte
+ * aligned): argList as above; asynchronous on the context stream; failures
+ * through tbgpu_last_error(). */
+void tbgpu_matvect_mult_dev(const int **argList, double *y_dev, const double *x_dev);
 
 /* Precision of the stored Hamiltonian: 64 (default) or 32 bits, set before
  * tbgpu_build_hamiltonian.  32 is the reference's HamMemorySave build
@@ -173,6 +177,14 @@ int tbgpu_get_state_errors(const tbgpu_ctx *ctx, int cap, double *residual, doub
  * Gamma, H*x runs the lane-gather kernel. */
 int tbgpu_set_bloch_k(tbgpu_ctx *ctx, const double *k);
 
+/* Start vector for the solves (the reference's lanczos_initialize /
+ * initStartVect with ReadFile, nemo3d/src/base/eigsys3d_par.c:113-215,
+ * nemo3d/src/io/i_3dout_files.c:2292): a host vector of tbgpu_dimension(ctx)
+ * complex entries, copied to the device and used by tbgpu_eigensolve_lanczos
+ * and tbgpu_eigensolve_lanczos_dev whenever they are called with a NULL
+ * start; NULL clears it.  After the build (TBGPU_E_STATE before). */
+int tbgpu_set_start_vector(tbgpu_ctx *ctx, const tbgpu_dcomplex *r_0);
+
 /* y = (H - shift) x on device vectors (asynchronous on the context stream). */
 int tbgpu_hx_dev(tbgpu_ctx *ctx, double shift, const double *x_dev,
                  double *y_dev);
@@ -198,7 +210,8 @@ int tbgpu_hx_block_dev(tbgpu_ctx *ctx, int p, double shift, const double *x_dev,
  * ConvCheckSkipRate iterations after ConvCheckStartIter on the last two
  * components of the tridiagonal eigenvector (lanczos.c:764-996), degenerate
  * and ghost values dropped at resolution 100*tolerance, windows
- * (emin1,emax1] and (emin2,emax2].  r_0: host start vector (normalised here,
+ * (emin1,emax1] and (emin2,emax2].  r_0: host start vector, or NULL for
+ * the one set by tbgpu_set_start_vector (normalised here,
  * as lanczos_initialize does, eigsys3d_par.c:113-215).  values[>= imax]
  * receives the eigenvalues ascending; conv_iterations (optional) the
  * iteration at which each converged; *iterations the iteration count.  If

@@ -32,7 +32,7 @@ static void free_ctx(Ctx *c) {
   void *ptrs[] = {c->d_type, c->d_dsp, c->d_par, c->d_par_ok, c->d_site_index, c->d_atom_site,
                   c->d_nbr, c->d_site_m, c->d_surface, c->d_onsite, c->d_blocks, c->d_partial,
                   c->d_counter, c->d_status, c->d_x, c->d_y, c->d_phase, c->d_groups,
-                  c->d_blocks32, c->d_onsite32, c->d_rc_order, c->d_units};
+                  c->d_blocks32, c->d_onsite32, c->d_rc_order, c->d_units, c->d_start};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -178,6 +178,32 @@ int tbgpu_hx_dev(tbgpu_ctx *ctx, double shift, const double *x_dev, double *y_de
   return launch_spmv(c, x_dev, y_dev, shift, nullptr, 0, nullptr, 0, c.stream);
 }
 
+void tbgpu_matvect_mult_dev(const int **argList, double *y_dev, const double *x_dev) {
+  set_error(TBGPU_OK);  // void entry point: status is read back via tbgpu_last_error
+  if (!argList || !argList[0]) {
+    set_error(TBGPU_E_ARG);
+    return;
+  }
+  const double shift = argList[1] ? *reinterpret_cast<const double *>(argList[1]) : 0.0;
+  tbgpu_hx_dev(reinterpret_cast<tbgpu_ctx *>(const_cast<int *>(argList[0])), shift, x_dev, y_dev);
+}
+
+int tbgpu_set_start_vector(tbgpu_ctx *ctx, const tbgpu_dcomplex *r_0) {
+  if (!ctx) return set_error(TBGPU_E_ARG);
+  Ctx &c = *C(ctx);
+  if (!r_0) {
+    if (c.d_start) cudaFree(c.d_start);
+    c.d_start = nullptr;
+    return TBGPU_OK;
+  }
+  if (!c.topo_built) return set_error(TBGPU_E_STATE);  // the dimension is known after the build
+  const size_t bytes = sizeof(double) * 2 * size_t(c.natoms) * c.nb;
+  if (!c.d_start && cudaMalloc(&c.d_start, bytes) != cudaSuccess) return set_error(TBGPU_E_NOMEM);
+  TB_CUDA(cudaMemcpyAsync(c.d_start, r_0, bytes, cudaMemcpyHostToDevice, c.stream));
+  TB_CUDA(cudaStreamSynchronize(c.stream));
+  return TBGPU_OK;
+}
+
 int tbgpu_hx_dev_f32(tbgpu_ctx *ctx, double shift, const float *x_dev, float *y_dev) {
   if (!ctx || !x_dev || !y_dev || misaligned16(x_dev) || misaligned16(y_dev))
     return set_error(TBGPU_E_ARG);
@@ -221,6 +247,8 @@ int tbgpu_eigensolve_lanczos_dev(tbgpu_ctx *ctx, int ConvCheckStartIter, int Con
                                  const double *r0_dev, double *values, int *conv_iterations,
                                  int *iterations, double *vectors_dev, int max_vectors) {
   if (!ctx || misaligned16(r0_dev) || misaligned16(vectors_dev)) return set_error(TBGPU_E_ARG);
+  if (!r0_dev) r0_dev = C(ctx)->d_start;  // the vector set by tbgpu_set_start_vector
+  if (!r0_dev) return set_error(TBGPU_E_ARG);
   SolveArgs A{ConvCheckStartIter, ConvCheckSkipRate, imax, requested1, requested2,
               emin1, emax1, emin2, emax2, tolerance};
   return solve(*C(ctx), A, r0_dev, values, conv_iterations, iterations, vectors_dev,
@@ -232,11 +260,27 @@ int tbgpu_eigensolve_lanczos(tbgpu_ctx *ctx, int ConvCheckStartIter, int ConvChe
                              double emax1, double emin2, double emax2, double tolerance,
                              const tbgpu_dcomplex *r_0, double *values, int *conv_iterations,
                              int *iterations, tbgpu_dcomplex *vectors, int max_vectors) {
-  if (!ctx || !r_0) return set_error(TBGPU_E_ARG);
+  if (!ctx || (!r_0 && !C(ctx)->d_start)) return set_error(TBGPU_E_ARG);
   Ctx &c = *C(ctx);
   if (!c.built) return set_error(TBGPU_E_STATE);
   const size_t bytes = sizeof(double) * 2 * size_t(c.natoms) * c.nb;
   double *r0 = nullptr, *V = nullptr;
+  if (!r_0) {  // the vector set by tbgpu_set_start_vector
+    int nv = (vectors && max_vectors > 0) ? max_vectors : 0;
+    if (nv && cudaMalloc(&V, bytes * nv) != cudaSuccess) return set_error(TBGPU_E_NOMEM);
+    int ne = tbgpu_eigensolve_lanczos_dev(ctx, ConvCheckStartIter, ConvCheckSkipRate, imax,
+                                          requested1, requested2, emin1, emax1, emin2, emax2,
+                                          tolerance, nullptr, values, conv_iterations, iterations,
+                                          V, nv);
+    if (ne > 0 && nv) {
+      const int got = ne < nv ? ne : nv;
+      if (cudaMemcpyAsync(vectors, V, bytes * got, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
+          cudaStreamSynchronize(c.stream) != cudaSuccess)
+        ne = set_error(TBGPU_E_CUDA);
+    }
+    if (V) cudaFree(V);
+    return ne;
+  }
   if (cudaMalloc(&r0, bytes) != cudaSuccess) return set_error(TBGPU_E_NOMEM);
   int nv = (vectors && max_vectors > 0) ? max_vectors : 0;
   if (nv && cudaMalloc(&V, bytes * nv) != cudaSuccess) {

@@ -113,6 +113,8 @@ struct Ctx {
   double2 *d_phase = nullptr;       // [natoms*4] phase of H[a][nbr], or null
   // scratch for the host-pointer matvec
   double *d_x = nullptr, *d_y = nullptr;
+  // start vector set by tbgpu_set_start_vector (used when a solve gets none)
+  double *d_start = nullptr;
 };
 
 // the stored Hamiltonian in its element type

@@ -106,6 +106,9 @@ def _lib():
         L.tbgpu_set_profiling.argtypes = [vp, ip]
         L.tbgpu_set_spmv_variant.argtypes = [vp, ip]
         L.tbgpu_autotune_spmv.argtypes = [vp, ip, vp, vp]
+        L.tbgpu_set_start_vector.argtypes = [vp, vp]
+        L.tbgpu_matvect_mult_dev.restype = None
+        L.tbgpu_matvect_mult_dev.argtypes = [C.POINTER(vp), vp, vp]
         L.tbgpu_get_stats.argtypes = [vp, C.POINTER(Stats)]
         _LIB = L
     return _LIB
@@ -287,8 +290,8 @@ class Hamiltonian:
         r_0: host start vector (2*dimension doubles).  Returns a dict with
         ``values`` (ascending), ``conv_iterations``, ``iterations`` and, when
         ``vectors`` > 0, ``vectors`` (complex, [k, dimension])."""
-        r0 = np.ascontiguousarray(r_0, np.float64)
-        if r0.size != 2 * self.n:
+        r0 = None if r_0 is None else np.ascontiguousarray(r_0, np.float64)
+        if r0 is not None and r0.size != 2 * self.n:
             raise ValueError("r_0 must hold 2*dimension doubles")
         vals = np.zeros(imax)
         cit = np.zeros(imax, np.int32)
@@ -442,6 +445,19 @@ class Hamiltonian:
         rc = _lib().tbgpu_set_spmv_variant(self._ctx, int(variant))
         if rc:
             raise TbgpuError(rc, "tbgpu_set_spmv_variant")
+
+    def set_start_vector(self, r_0):
+        """Keep a start vector in the context (tbgpu_set_start_vector); solves
+        called with ``r_0=None`` use it.  None clears it."""
+        if r_0 is None:
+            rc = _lib().tbgpu_set_start_vector(self._ctx, None)
+        else:
+            self._start = np.ascontiguousarray(r_0, np.float64)
+            if self._start.size != 2 * self.n:
+                raise ValueError("r_0 must hold 2*dimension doubles")
+            rc = _lib().tbgpu_set_start_vector(self._ctx, _p(self._start))
+        if rc:
+            raise TbgpuError(rc, "tbgpu_set_start_vector")
 
     def autotune_spmv(self, reps: int = 10):
         """Time every H*x variant on this structure and keep the fastest

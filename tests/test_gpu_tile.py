@@ -170,3 +170,35 @@ def test_tile_lanczos_matches_default():
     res = g.eigensolve_lanczos(r0, **kw)
     assert len(res["values"]) == len(ref["values"]) >= 2
     assert np.abs(np.sort(res["values"]) - np.sort(ref["values"])).max() < 1e-9
+
+
+def test_start_vector_seam_and_device_matvec():
+    """tbgpu_set_start_vector: a solve without r_0 uses the stored vector
+    (same result as passing it); tbgpu_matvect_mult_dev equals hx_dev."""
+    import ctypes as C
+    import torch
+    from nemo3d_b200 import tbgpu
+    st = workloads.dome_in_box(cells=(8, 8, 6), base_nm=3.0, height_nm=1.2, wl_z_nm=1.2,
+                               sigma_frac=0.01, seed=2)
+    g, _ = _ham(st, "sp3d5s*_so")
+    r0 = workloads.random_start(g.n, seed=4)
+    kw = dict(imax=3000, requested1=2, requested2=2, emin1=-0.6, emax1=0.3, emin2=0.8,
+              emax2=2.4, tolerance=1e-7)
+    ref = g.eigensolve_lanczos(r0, **kw)
+    g.set_start_vector(r0)
+    res = g.eigensolve_lanczos(None, **kw)
+    assert res["iterations"] == ref["iterations"]
+    np.testing.assert_array_equal(res["values"], ref["values"])
+    g.set_start_vector(None)
+    with pytest.raises(tbgpu.TbgpuError):
+        g.eigensolve_lanczos(None, **kw)
+    x = torch.rand(2 * g.n, dtype=torch.float64, device="cuda") - 0.5
+    y1, y2 = torch.empty_like(x), torch.empty_like(x)
+    g.hx_dev(x.data_ptr(), y1.data_ptr(), 0.25)
+    shift = C.c_double(0.25)
+    args = (C.c_void_p * 3)(g._ctx.value, C.cast(C.pointer(shift), C.c_void_p).value, None)
+    tbgpu._lib().tbgpu_matvect_mult_dev(args, C.c_void_p(y2.data_ptr()),
+                                        C.c_void_p(x.data_ptr()))
+    torch.cuda.synchronize()
+    assert tbgpu._lib().tbgpu_last_error() == 0
+    assert torch.equal(y1, y2)
