@@ -468,6 +468,15 @@ typedef struct {
 int tbgpu_set_profiling(tbgpu_ctx *ctx, int on);
 int tbgpu_get_stats(const tbgpu_ctx *ctx, tbgpu_stats *out);
 
+/* Failure-detection self-test: one warp waits, with the bounded poll loop
+ * (at most polls, 1..2^24) that every device-side wait of the library uses,
+ * on an mbarrier that is never completed.  Returns TBGPU_E_TIMEOUT when the
+ * wait ran out and reported itself as designed; the context stays usable.
+ * The solves and tbgpu_matvect_mult report the same status word (a kernel's
+ * wait that ran out) after their stream drains; asynchronous calls leave it
+ * for the next synchronous one. */
+int tbgpu_selftest_bounded_wait(tbgpu_ctx *ctx, long polls);
+
 int tbgpu_last_error(void);
 const char *tbgpu_error_string(int code);
 

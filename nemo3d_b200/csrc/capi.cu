@@ -5,6 +5,7 @@
 #include <new>
 #include <vector>
 
+#include "stage.cuh"
 #include "tbgpu_internal.cuh"
 
 namespace tbgpu {
@@ -212,6 +213,18 @@ int tbgpu_hx_dev_f32(tbgpu_ctx *ctx, double shift, const float *x_dev, float *y_
   return launch_spmv_f32(c, x_dev, y_dev, shift, nullptr, 0, nullptr, 0, c.stream);
 }
 
+// The status word of the context's kernels (a device-side wait that ran
+// out, a bad species id): read after the stream drained, cleared, returned.
+static int take_status(Ctx &c) {
+  if (cudaStreamSynchronize(c.stream) != cudaSuccess) return set_error(TBGPU_E_CUDA);
+  int st = 0;
+  if (cudaMemcpy(&st, c.d_status, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return set_error(TBGPU_E_CUDA);
+  if (!st) return TBGPU_OK;
+  if (cudaMemset(c.d_status, 0, sizeof(int)) != cudaSuccess) return set_error(TBGPU_E_CUDA);
+  return set_error(st);
+}
+
 void tbgpu_matvect_mult(const int **argList, tbgpu_dcomplex *y, const tbgpu_dcomplex *x) {
   set_error(TBGPU_OK);  // void entry point: status is read back via tbgpu_last_error
   if (!argList || !argList[0] || !x || !y) {
@@ -237,8 +250,40 @@ void tbgpu_matvect_mult(const int **argList, tbgpu_dcomplex *y, const tbgpu_dcom
   }
   if (launch_spmv(c, c.d_x, c.d_y, shift, nullptr, 0, nullptr, 0, c.stream)) return;
   if (cudaMemcpyAsync(y, c.d_y, bytes, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
-      cudaStreamSynchronize(c.stream) != cudaSuccess)
+      cudaStreamSynchronize(c.stream) != cudaSuccess) {
     set_error(TBGPU_E_CUDA);
+    return;
+  }
+  take_status(c);
+}
+
+namespace tbgpu {
+namespace {
+// One warp waits, with the bounded poll loop of the library's device-side
+// waits, on an mbarrier that expects two arrivals and gets one: the wait
+// runs out and the status word says so.
+__global__ void k_selftest_wait(long polls, int *status) {
+  __shared__ unsigned long long bar;
+  const uint32_t mb = stage::smem_addr(&bar);
+  if (threadIdx.x == 0) {
+    stage::mbar_init(mb, 2);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncwarp();
+  if (threadIdx.x == 0) stage::mbar_arrive(mb);
+  bool done = false;
+  for (long p = 0; p < polls && !done; p++) done = stage::mbar_try_wait(mb, 0);
+  if (!__any_sync(0xffffffffu, done) && threadIdx.x == 0) atomicExch(status, TBGPU_E_TIMEOUT);
+}
+}  // namespace
+}  // namespace tbgpu
+
+int tbgpu_selftest_bounded_wait(tbgpu_ctx *ctx, long polls) {
+  if (!ctx || polls < 1 || polls > (1L << 24)) return set_error(TBGPU_E_ARG);
+  Ctx &c = *C(ctx);
+  k_selftest_wait<<<1, 32, 0, c.stream>>>(polls, c.d_status);
+  TB_CUDA(cudaGetLastError());
+  return take_status(c);
 }
 
 int tbgpu_eigensolve_lanczos_dev(tbgpu_ctx *ctx, int ConvCheckStartIter, int ConvCheckSkipRate,
@@ -251,8 +296,11 @@ int tbgpu_eigensolve_lanczos_dev(tbgpu_ctx *ctx, int ConvCheckStartIter, int Con
   if (!r0_dev) return set_error(TBGPU_E_ARG);
   SolveArgs A{ConvCheckStartIter, ConvCheckSkipRate, imax, requested1, requested2,
               emin1, emax1, emin2, emax2, tolerance};
-  return solve(*C(ctx), A, r0_dev, values, conv_iterations, iterations, vectors_dev,
-               max_vectors);
+  const int ne = solve(*C(ctx), A, r0_dev, values, conv_iterations, iterations, vectors_dev,
+                       max_vectors);
+  if (ne < 0) return ne;
+  const int st = take_status(*C(ctx));
+  return st ? st : ne;
 }
 
 int tbgpu_eigensolve_lanczos(tbgpu_ctx *ctx, int ConvCheckStartIter, int ConvCheckSkipRate,

@@ -40,6 +40,9 @@ constexpr long kWaitLimit = 1L << 20;  // mbarrier polls before giving up
 __device__ __forceinline__ void mbar_init(uint32_t mb, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mb), "r"(count) : "memory");
 }
+__device__ __forceinline__ void mbar_arrive(uint32_t mb) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(mb) : "memory");
+}
 __device__ __forceinline__ void mbar_expect_tx(uint32_t mb, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(bytes)
                : "memory");
