@@ -472,9 +472,15 @@ int tbgpu_get_stats(const tbgpu_ctx *ctx, tbgpu_stats *out);
  * (at most polls, 1..2^24) that every device-side wait of the library uses,
  * on an mbarrier that is never completed.  Returns TBGPU_E_TIMEOUT when the
  * wait ran out and reported itself as designed; the context stays usable.
- * The solves and tbgpu_matvect_mult report the same status word (a kernel's
- * wait that ran out) after their stream drains; asynchronous calls leave it
- * for the next synchronous one. */
+ * These synchronous entry points read the same status word (a kernel's wait
+ * that ran out) after their stream drains, clear it and return its code:
+ * tbgpu_eigensolve_lanczos(_dev), tbgpu_eigensolve_lanczos_batched,
+ * tbgpu_eigensolve_blk_lanczos(_dev), tbgpu_momentum_matrix,
+ * tbgpu_matvect_mult (through tbgpu_last_error), tbgpu_vff_energy,
+ * tbgpu_vff_relax and tbgpu_build_hamiltonian.  The asynchronous device
+ * entry points (tbgpu_hx_dev, tbgpu_hx_dev_f32, tbgpu_hx_block_dev,
+ * tbgpu_matvect_mult_dev, tbgpu_hx_dot_noalloc) leave it for the next
+ * synchronous call on the context. */
 int tbgpu_selftest_bounded_wait(tbgpu_ctx *ctx, long polls);
 
 int tbgpu_last_error(void);

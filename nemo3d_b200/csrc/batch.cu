@@ -735,6 +735,11 @@ extern "C" int tbgpu_eigensolve_lanczos_batched(
   if (!ctx || misaligned16(r0_dev) || misaligned16(vectors_dev)) return set_error(TBGPU_E_ARG);
   BatchArgs A{ConvCheckStartIter, ConvCheckSkipRate, imax, requested1, requested2, tolerance,
               emin1, emax1, emin2, emax2};
-  return solve_batch(*reinterpret_cast<Ctx *>(ctx), ndots, dot_cells, A, r0_dev, values,
-                     values_stride, found, iterations, vectors_dev, max_vectors);
+  Ctx &c = *reinterpret_cast<Ctx *>(ctx);
+  const int rc = solve_batch(c, ndots, dot_cells, A, r0_dev, values, values_stride, found,
+                             iterations, vectors_dev, max_vectors);
+  if (rc < 0) return rc;
+  // a bounded device-side wait that ran out in any product of the solve
+  const int st = take_status(c);
+  return st ? st : rc;
 }

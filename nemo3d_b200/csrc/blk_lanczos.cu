@@ -873,6 +873,8 @@ extern "C" int tbgpu_eigensolve_blk_lanczos_dev(
   int f1 = 0, f2 = 0, it = 0;
   int rc = solve_block(c, A, r0_dev, vals, f1, f2, it, vectors_dev, max_vectors);
   if (rc) return rc;
+  rc = take_status(c);  // a bounded device-side wait that ran out in a product
+  if (rc) return rc;
   for (size_t k = 0; k < vals.size(); k++) values[k] = vals[k];
   if (found_vb) *found_vb = f1;
   if (found_cb) *found_cb = f2;

@@ -17,6 +17,16 @@ int set_error(int code) {
   return code;
 }
 
+int take_status(Ctx &c) {
+  if (cudaStreamSynchronize(c.stream) != cudaSuccess) return set_error(TBGPU_E_CUDA);
+  int st = 0;
+  if (cudaMemcpy(&st, c.d_status, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return set_error(TBGPU_E_CUDA);
+  if (!st) return TBGPU_OK;
+  if (cudaMemset(c.d_status, 0, sizeof(int)) != cudaSuccess) return set_error(TBGPU_E_CUDA);
+  return set_error(st);
+}
+
 
 static int model_dims(int bm, int *norb, int *nspin) {
   switch (bm) {
@@ -65,6 +75,11 @@ static int create(const tbgpu_geom *g, const tbgpu_model *m, bool dev, tbgpu_ctx
   }
   c->nsites = long(g->nx) * g->ny * g->nz * 8;
   cudaGetDevice(&c->device);
+  if (cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->device) != cudaSuccess ||
+      c->sms < 1) {
+    delete c;
+    return set_error(TBGPU_E_CUDA);
+  }
   auto fail = [&](int code) {
     free_ctx(c);
     return set_error(code);
@@ -211,18 +226,6 @@ int tbgpu_hx_dev_f32(tbgpu_ctx *ctx, double shift, const float *x_dev, float *y_
   Ctx &c = *C(ctx);
   if (!c.built) return set_error(TBGPU_E_STATE);
   return launch_spmv_f32(c, x_dev, y_dev, shift, nullptr, 0, nullptr, 0, c.stream);
-}
-
-// The status word of the context's kernels (a device-side wait that ran
-// out, a bad species id): read after the stream drained, cleared, returned.
-static int take_status(Ctx &c) {
-  if (cudaStreamSynchronize(c.stream) != cudaSuccess) return set_error(TBGPU_E_CUDA);
-  int st = 0;
-  if (cudaMemcpy(&st, c.d_status, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
-    return set_error(TBGPU_E_CUDA);
-  if (!st) return TBGPU_OK;
-  if (cudaMemset(c.d_status, 0, sizeof(int)) != cudaSuccess) return set_error(TBGPU_E_CUDA);
-  return set_error(st);
 }
 
 void tbgpu_matvect_mult(const int **argList, tbgpu_dcomplex *y, const tbgpu_dcomplex *x) {

@@ -144,13 +144,8 @@ template <int NB>
 int launch_momentum(Ctx &c, int grid, int na, const VecSet &A, int nbv, const VecSet &B,
                     double *partial, double *out, cudaStream_t s) {
   const size_t smem = sizeof(double2) * 4 * kTile * NB * kRow;
-  static bool attr = false;
-  if (!attr) {
-    if (cudaFuncSetAttribute(k_momentum<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(smem)) != cudaSuccess)
-      return set_error(TBGPU_E_CUDA);
-    attr = true;
-  }
+  static std::atomic<unsigned long long> attr_done{0};
+  if (ensure_smem_attr(attr_done, c.device, k_momentum<NB>, int(smem))) return TBGPU_E_CUDA;
   k_momentum<NB><<<grid, kThreads, smem, s>>>(c.natoms, na, A, nbv, B, c.d_atom_site, c.d_dsp,
                                               c.ny, c.nz, c.lattice[0], c.lattice[1],
                                               c.lattice[2], partial);
@@ -282,5 +277,8 @@ using namespace tbgpu;
 extern "C" int tbgpu_momentum_matrix(tbgpu_ctx *ctx, int n, const double *psi_dev,
                                      const double *E, double *P, double *trans) {
   if (!ctx || misaligned16(psi_dev)) return set_error(TBGPU_E_ARG);
-  return momentum_matrix(*reinterpret_cast<Ctx *>(ctx), n, psi_dev, E, P, trans);
+  Ctx &c = *reinterpret_cast<Ctx *>(ctx);
+  const int rc = momentum_matrix(c, n, psi_dev, E, P, trans);
+  if (rc) return rc;
+  return take_status(c);  // a bounded device-side wait that ran out in a product
 }

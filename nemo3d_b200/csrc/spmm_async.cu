@@ -217,14 +217,9 @@ int launch_mt(Ctx &c, const double *x, long xstride, double *y, long ystride, do
               cudaStream_t s) {
   using L = MLayout<NSPIN, P>;
   static_assert(L::WARPS >= 1, "block too large for shared memory");
-  static int sms = 0;
-  if (!sms) {
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device);
-    if (cudaFuncSetAttribute(k_spmm_async<NSPIN, P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             L::SMEM) != cudaSuccess)
-      return set_error(TBGPU_E_CUDA);
-  }
-  k_spmm_async<NSPIN, P><<<unsigned(sms), L::WARPS * 32, L::SMEM, s>>>(
+  static std::atomic<unsigned long long> attr_done{0};
+  if (ensure_smem_attr(attr_done, c.device, k_spmm_async<NSPIN, P>, L::SMEM)) return TBGPU_E_CUDA;
+  k_spmm_async<NSPIN, P><<<unsigned(c.sms), L::WARPS * 32, L::SMEM, s>>>(
       c.ngroups, c.d_groups, c.d_nbr, c.d_site_m, c.d_onsite, c.d_blocks,
       reinterpret_cast<const double2 *>(x), xstride / 2, reinterpret_cast<double2 *>(y),
       ystride / 2, shift);

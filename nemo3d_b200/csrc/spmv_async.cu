@@ -26,9 +26,12 @@
 // multicast) issued by lane 0 on an mbarrier of the warp's stage instead of
 // 200 16-byte cp.async copies, which takes about a third of the staging
 // copies off the load/store unit (the bytes written to shared memory stay
-// the same, and so does most of the time: 0.668 against 0.674 ms).  The wait on the mbarrier is bounded: a warp whose copy
-// does not arrive reports TBGPU_E_TIMEOUT in the status word, waits once
-// more for its copies in flight and leaves its loop.
+// // the same, and so does most of the time: 0.668 against 0.674 ms).  The
+// wait on the mbarrier is bounded: a warp whose copy does not arrive reports
+// TBGPU_E_TIMEOUT in the status word, waits once more (bounded) for its
+// copies in flight and leaves its loop; if that second wait also runs out,
+// every warp of the CTA stops issuing copies, and the CTA may end with that
+// one copy outstanding.
 #include <cstdint>
 
 #include "tbgpu_internal.cuh"
@@ -170,13 +173,17 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
   // BULK: one mbarrier per stage of this warp, after the stages
   const uint32_t mb0 = smem_addr(smem + L::SMEM) + uint32_t(warp * STAGES * 8);
   uint32_t phase = 0;  // bit s: parity of stage s's next completion
+  // set when a warp's copies did not land within two bounded waits: every
+  // warp of the CTA then stops issuing copies (BULK only)
+  __shared__ int s_stop;
   if (BULK) {
     if (lane == 0) {
 #pragma unroll
       for (int s = 0; s < STAGES; s++) mbar_init(mb0 + 8 * s, 1);
       asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    __syncwarp();
+    if (threadIdx.x == 0) s_stop = 0;
+    __syncthreads();
   }
   const int ai = lane / kNorb, o = lane - ai * kNorb;
   const RT scale = RT(xnorm ? 1.0 / xnorm[xnorm_idx] : 1.0);
@@ -191,6 +198,8 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
   Meta nxt = load_meta(g + nw, ngroups, groups, nbr, site_m, skip);
   int k = 0;
   for (; g < ngroups; g += nw, ++k) {
+    if (BULK && __any_sync(0xffffffffu, *reinterpret_cast<volatile int *>(&s_stop) != 0))
+      break;  // another warp's copies never landed: issue nothing more
     const long gn = g + nw;
     unsigned char *st = wbase + (k % STAGES) * L::STAGE;
     if (STAGES > 1) {  // next group's copies overlap this group's compute
@@ -210,7 +219,12 @@ __global__ void __launch_bounds__(WARPS * 32, 1)
       const bool late = !mbar_wait(mb0 + 8 * s, par);
       if (__any_sync(0xffffffffu, late)) {
         if (lane == 0 && status) atomicExch(status, TBGPU_E_TIMEOUT);
-        mbar_wait(mb0 + 8 * s, par);
+        // one more bounded wait for the copies in flight; if they still did
+        // not land, the CTA stops issuing copies and may exit with that copy
+        // outstanding (the one exit whose shared-memory state is not
+        // guaranteed; the status word reports it)
+        const bool drained = mbar_wait(mb0 + 8 * s, par);
+        if (!drained && lane == 0) *reinterpret_cast<volatile int *>(&s_stop) = 1;
         break;
       }
       phase ^= 1u << s;
@@ -318,14 +332,11 @@ int launch_async_t(Ctx &c, const void *x, void *y, double shift, const double *x
                    int xidx, double *alpha_out, int aidx, cudaStream_t s) {
   using L = Layout<NSPIN, WARPS, STAGES, HT, VT>;
   constexpr int smem = L::SMEM + (BULK ? WARPS * STAGES * 8 : 0);
-  static int sms = 0;
-  if (!sms) {
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device);
-    if (cudaFuncSetAttribute(k_spmv_async<NSPIN, DOT, WARPS, STAGES, HT, VT, BULK>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
-      return set_error(TBGPU_E_CUDA);
-  }
-  const unsigned grid = unsigned(sms);
+  static std::atomic<unsigned long long> attr_done{0};
+  if (ensure_smem_attr(attr_done, c.device, k_spmv_async<NSPIN, DOT, WARPS, STAGES, HT, VT, BULK>,
+                       smem))
+    return TBGPU_E_CUDA;
+  const unsigned grid = unsigned(c.sms);
   if (DOT) {
     int rc = ensure_partials(c, int(grid));
     if (rc) return rc;

@@ -137,7 +137,9 @@ __global__ void __launch_bounds__(kTileThreads, 3)
     const bool late = !mbar_wait(mb, parity);
     if (__syncthreads_or(late)) {
       // a bulk copy that did not complete: report it, give the copies in
-      // flight one more bounded wait, and stop (the decision is block-wide)
+      // flight one more bounded wait, and stop (the decision is block-wide,
+      // so no thread issues another copy; if the second wait also runs out
+      // the CTA ends with that copy outstanding, reported by the status word)
       if (t == 0) atomicExch(status, TBGPU_E_TIMEOUT);
       mbar_wait(mb, parity);
       break;
@@ -358,14 +360,11 @@ static int launch_tile_t(Ctx &c, const double *x, double *y, double shift, const
                          int xidx, double *alpha_out, int aidx, cudaStream_t s) {
   using L = TileLayout<NSPIN>;
   const int smem = desc_bytes(c.unit_stride) + 128 + L::bytes(c.unit_cap_nb, c.unit_cap_nx);
-  static int attr = 0, sms = 0;
-  if (attr < smem) {
-    if (cudaFuncSetAttribute(k_spmv_tile<NSPIN, DOT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             smem) != cudaSuccess)
-      return set_error(TBGPU_E_UNSUPPORTED);
-    attr = smem;
-  }
-  if (!sms) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device);
+  // the stage size depends on the context's unit table: set on every launch
+  if (cudaFuncSetAttribute(k_spmv_tile<NSPIN, DOT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           smem) != cudaSuccess)
+    return set_error(TBGPU_E_UNSUPPORTED);
+  const int sms = c.sms;
   int per_sm = 0;
   TB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spmv_tile<NSPIN, DOT>,
                                                         kTileThreads, smem));

@@ -34,7 +34,11 @@ __device__ __forceinline__ void cp_wait() {
 }
 
 // 1-D bulk copies (cp.async.bulk, no multicast) complete on an mbarrier in
-// the copying CTA's shared memory; waits on it are bounded.
+// the copying CTA's shared memory; waits on it are bounded.  A kernel whose
+// wait runs out reports TBGPU_E_TIMEOUT, waits once more (bounded) and stops
+// issuing copies; if the second wait also runs out, the CTA may end with
+// that copy still in flight into its shared memory -- the one exit whose
+// state is not guaranteed, and the status word says it happened.
 constexpr long kWaitLimit = 1L << 20;  // mbarrier polls before giving up
 
 __device__ __forceinline__ void mbar_init(uint32_t mb, uint32_t count) {

@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <complex>
 #include <cstdint>
 #include <vector>
@@ -53,6 +54,7 @@ struct Ctx {
   bool built = false;
   bool topo_built = false;  // topology done (by the build or a strain relaxation)
   int device = 0;
+  int sms = 0;                      // multiprocessors of the context's device
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   // device arrays
@@ -127,6 +129,26 @@ template <> inline const float *ham_onsite<float>(const Ctx &c) { return c.d_ons
 
 // error helpers
 int set_error(int code);
+// The status word of the context's kernels (a device-side wait that ran
+// out, a bad species id): read after the context's stream drained, cleared,
+// and returned as the call's status (TBGPU_OK when clear).
+int take_status(Ctx &c);
+
+// Dynamic shared memory above 48 KB is allowed per kernel and per device
+// context.  `done` (one per kernel instance) records the devices already
+// set; devices past 63 set it on every launch.  Setting it twice from two
+// host threads is harmless.
+template <typename K>
+inline int ensure_smem_attr(std::atomic<unsigned long long> &done, int device, K *func,
+                            int bytes) {
+  const unsigned long long bit = (device >= 0 && device < 64) ? 1ull << device : 0ull;
+  if (bit && (done.load(std::memory_order_acquire) & bit)) return TBGPU_OK;
+  if (cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) !=
+      cudaSuccess)
+    return set_error(TBGPU_E_CUDA);
+  done.fetch_or(bit, std::memory_order_acq_rel);
+  return TBGPU_OK;
+}
 // device vectors must start on a 16-byte boundary (the kernels move them in
 // 16-byte pieces); null passes
 inline bool misaligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15) != 0; }

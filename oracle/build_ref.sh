@@ -2,17 +2,24 @@
 # build_ref.sh -- TEST INFRASTRUCTURE ONLY.
 #
 # Compiles the reference's Slater-Koster routines
-# (nemo3d/src/ham/mb_ham_spds_micro.c) from the NEMO-3D source tree, where
-# they lie, together with oracle/ref_sk_driver.cc into oracle/_ref/ref_sk.
-# The tests use it to check the oracle's restatement of the bond blocks, the
-# strain diagonal correction, the on-site/spin-orbit block and the sp3s*
-# parameter conversion.  Outputs go to oracle/_ref/ only.
+# (nemo3d/src/ham/mb_ham_spds_micro.c) and its zincblende cell
+# (nemo3d/src/base/Cell.c) from the NEMO-3D source tree, where they lie,
+# together with oracle/ref_sk_driver.cc into oracle/_ref/ref_sk.  The tests
+# use it to check the oracle's restatement of the bond blocks, the strain
+# diagonal correction, the on-site/spin-orbit block, the sp3s* parameter
+# conversion and the dangling-bond passivation.  Outputs go to oracle/_ref/
+# only.
 #
-# Usage: oracle/build_ref.sh [path to the NEMO_3D directory of the reference]
+# Usage: oracle/build_ref.sh <path to the NEMO_3D directory of the reference>
+#        (or set NEMO3D_SRC to it)
 set -e
 HERE=$(cd "$(dirname "$0")" && pwd)
-R=${1:-${NEMO3D_SRC:-/root/reference/NEMO_3D}}
+R=${1:-${NEMO3D_SRC:-}}
 OUT="$HERE/_ref"
+if [ -z "$R" ]; then
+  echo "build_ref.sh: give the reference's NEMO_3D directory (argument or NEMO3D_SRC); skipped" >&2
+  exit 0
+fi
 if [ ! -f "$R/nemo3d/src/ham/mb_ham_spds_micro.c" ]; then
   # machines without the reference tree use the prebuilt binary, if any
   echo "build_ref.sh: reference sources not found under $R; skipped" >&2
@@ -27,8 +34,11 @@ INC="-I$R/nemo3d/src/base -I$R/nemo3d/src/ham -I$R/nemo3d/src/math -I$R/nemo3d/s
 DEFS="-DFAKE_MPI -DLINUX"
 FLAGS="-O2 -ffp-contract=off -fpermissive -w -ffunction-sections -fdata-sections"
 g++ -x c++ $FLAGS $DEFS $INC -c "$R/nemo3d/src/ham/mb_ham_spds_micro.c" -o "$OUT/mb_ham_spds_micro.o"
+# the zincblende cell (neighbour map, positions) for the passivation check
+g++ -x c++ $FLAGS $DEFS $INC -c "$R/nemo3d/src/base/Cell.c" -o "$OUT/Cell.o"
 g++ $FLAGS $DEFS $INC -c "$HERE/ref_sk_driver.cc" -o "$OUT/ref_sk_driver.o"
 # routines the driver never reaches (geometry, dense eigensolvers) are
 # dropped by --gc-sections together with their unresolved references
-g++ -Wl,--gc-sections -o "$OUT/ref_sk" "$OUT/ref_sk_driver.o" "$OUT/mb_ham_spds_micro.o" -lm
+g++ -Wl,--gc-sections -o "$OUT/ref_sk" "$OUT/ref_sk_driver.o" "$OUT/mb_ham_spds_micro.o" \
+  "$OUT/Cell.o" -lm
 echo "$OUT/ref_sk"

@@ -22,6 +22,19 @@
 //     -> double h[nbasis][nbasis][2]
 //   int32 cmd = 3  param_sp3s_2_sp3d5s (mb_ham_spds_micro.c:2984)
 //       double param_in[15], a0 -> double param_out[35]
+//   int32 cmd = 4  dangling-bond passivation,
+//                  h3d_diag_dangling_bond_shift_zincblende
+//                  (mb_ham_spds_micro.c:1910-2150), on a closed box
+//       int32 nbasis (10: sp3s* with spin, 20: sp3d5s* with spin), nx, ny, nz
+//       double DanglingBondEnergyShift
+//       uint8 occupied[nx][ny][nz][8] (the reference's AtomType != 0)
+//       int32 count, then count pairs (cell index, atom in cell) with cell
+//             index (i * ny + j) * nz + k
+//     -> per pair double h[nbasis][nbasis][2], the routine's additions to a
+//        zero on-site block
+//     The cell's neighbour map, positions and neighbour counts come from the
+//     reference's own Cell::Initialize (nemo3d/src/base/Cell.c, compiled where
+//     it lies) for the zincblende crystal.
 // The basis and spin arrays are the ones basis_init builds
 // (nemo3d/src/base/ham3d_final.c:597-619).
 #include <stdint.h>
@@ -30,6 +43,7 @@
 #include <string.h>
 
 #include "mb_ham_spds_micro.h"
+#include "mb_ham_spds_micro2.h"
 
 // ---------------------------------------------------------------- nml helpers
 namespace {
@@ -90,6 +104,31 @@ void rm_cmatrix(cmatrix *p) {
     *p = NULL;
   }
 }
+// 3-D tensors with lower bounds (the nml i3tensor/r3tensor interface):
+// t[i][j][k] for lb3 <= i <= ub3, lb2 <= j <= ub2, lb1 <= k <= ub1
+template <typename T>
+T ***tensor3(int lb3, int ub3, int lb2, int ub2, int lb1, int ub1) {
+  const int n3 = ub3 - lb3 + 1, n2 = ub2 - lb2 + 1, n1 = ub1 - lb1 + 1;
+  T ***p = static_cast<T ***>(calloc(n3, sizeof(T **)));
+  T **rows = static_cast<T **>(calloc(size_t(n3) * n2, sizeof(T *)));
+  T *data = static_cast<T *>(calloc(size_t(n3) * n2 * n1, sizeof(T)));
+  if (!p || !rows || !data) {
+    fprintf(stderr, "ref_sk_driver: out of memory\n");
+    exit(2);
+  }
+  for (int a = 0; a < n3; ++a) {
+    p[a] = rows + size_t(a) * n2 - lb2;
+    for (int b = 0; b < n2; ++b) rows[size_t(a) * n2 + b] = data + (size_t(a) * n2 + b) * n1 - lb1;
+  }
+  return p - lb3;
+}
+i3tensor I3tensor(int a, int b, int c, int d, int e, int f) { return tensor3<int>(a, b, c, d, e, f); }
+r3tensor R3tensor(int a, int b, int c, int d, int e, int f) {
+  return tensor3<double>(a, b, c, d, e, f);
+}
+void rm_i3tensor(i3tensor *p, int) { if (p) *p = NULL; }  // the driver's tensors live until exit
+void rm_r3tensor(r3tensor *p, int) { if (p) *p = NULL; }
+
 complex Complex(double r, double i) {
   complex z;
   z.r = r;
@@ -101,6 +140,13 @@ complex cmul(complex a, complex b) {
   return Complex(a.r * b.r - a.i * b.i, a.r * b.i + a.i * b.r);
 }
 complex cconj(complex a) { return Complex(a.r, -a.i); }
+// the master-rank output stream Cell::Initialize writes its notices to
+ostream_N3D cout_master;
+// only reached for tilted periodic crystals, which the driver never builds
+int geo_struct::get_cindx_tilted(int, int, int) {
+  fprintf(stderr, "ref_sk_driver: tilted crystals are not supported\n");
+  exit(7);
+}
 void die(char *s, ...) {
   fprintf(stderr, "reference die(): %s\n", s);
   exit(3);
@@ -195,6 +241,55 @@ int main() {
       fwrite(pout, sizeof(double), sp3d5s_nparam, stdout);
       rm_rvectr(&pout);
       rm_rvectr(&pin);
+    } else if (cmd == 4) {
+      int32_t h[4];
+      double shift;
+      if (!rd(h, sizeof(h)) || !rd(&shift, 8)) return 4;
+      const int nb = h[0], nx = h[1], ny = h[2], nz = h[3];
+      if ((nb != 10 && nb != 20) || nx < 1 || ny < 1 || nz < 1) return 5;
+      const long ncell = long(nx) * ny * nz;
+      unsigned char *occ = static_cast<unsigned char *>(malloc(ncell * 8));
+      if (!occ || !rd(occ, ncell * 8)) return 4;
+      // the routine reads opt, hd, geo and BandModel of the structure; the
+      // rest of it stays zero (no constructors run)
+      QD_struct *d = static_cast<QD_struct *>(calloc(1, sizeof(QD_struct)));
+      top_struct *opt = new top_struct();
+      opt->Dev.StructFile = "NULL";
+      opt->Dev.CrystalStruct = Dev_struct::Zincblende;
+      Cell *cell = new Cell();
+      cell->Initialize(*opt);
+      memcpy(static_cast<void *>(&d->geo.cellgeom), static_cast<void *>(cell), sizeof(Cell));
+      d->opt.ExecParam.Phys.DanglingBondEnergyShift = shift;
+      d->BandModel = nb == 10 ? BM_10_sp3ss_spin : BM_20_sp3d5ss_spin;
+      d->geo.N_Cell = int(ncell);
+      d->geo.ijk__cell = I3tensor(-1, nx, -1, ny, -1, nz);
+      for (int i = -1; i <= nx; ++i)
+        for (int j = -1; j <= ny; ++j)
+          for (int k = -1; k <= nz; ++k)
+            d->geo.ijk__cell[i][j][k] =
+                (i < 0 || j < 0 || k < 0 || i >= nx || j >= ny || k >= nz) ? -1
+                                                                           : (i * ny + j) * nz + k;
+      d->geo.cell__ijk = static_cast<int **>(calloc(ncell, sizeof(int *)));
+      d->geo.AtomType = static_cast<nml_bscalar **>(calloc(ncell, sizeof(nml_bscalar *)));
+      for (long l = 0; l < ncell; ++l) {
+        d->geo.cell__ijk[l] = static_cast<int *>(calloc(3, sizeof(int)));
+        d->geo.cell__ijk[l][0] = int(l / (long(ny) * nz));
+        d->geo.cell__ijk[l][1] = int((l / nz) % ny);
+        d->geo.cell__ijk[l][2] = int(l % nz);
+        d->geo.AtomType[l] = static_cast<nml_bscalar *>(calloc(8, sizeof(nml_bscalar)));
+        for (int m = 0; m < 8; ++m) d->geo.AtomType[l][m] = occ[l * 8 + m] != 0;
+      }
+      int32_t count;
+      if (!rd(&count, 4)) return 4;
+      for (int q = 0; q < count; ++q) {
+        int32_t ca[2];
+        if (!rd(ca, sizeof(ca)) || ca[0] < 0 || ca[0] >= ncell || ca[1] < 0 || ca[1] > 7) return 4;
+        d->hd = cmat(nb);
+        h3d_diag_dangling_bond_shift_zincblende(d, ca[0], ca[1]);
+        wr_cmat(d->hd, nb);
+        rm_cmatrix(&d->hd);
+      }
+      free(occ);
     } else {
       return 6;
     }

@@ -1,6 +1,7 @@
 """Extract the reference's golden data for the hot path into a small fixture.
 
-Reads, from a NEMO-3D source tree (default /root/reference/NEMO_3D):
+Reads, from a NEMO-3D source tree (its NEMO_3D directory, given as the
+argument or in NEMO3D_SRC):
   nemo3d/example/TestRun/GaAs_bulk.old_nd_Ek_ascii  (6400 eigenvalues, 40 k)
   nemo3d/example/TestRun/Si_Bulk.old_nd_Ek_ascii    (358 Lanczos eigenvalues)
   nemo3d/bin/Si_Bulk.nd_nbrIndx                      (8x4 neighbour table)
@@ -15,7 +16,9 @@ import sys
 
 import numpy as np
 
-ROOT = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/NEMO_3D"
+ROOT = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("NEMO3D_SRC", "")
+if not ROOT:
+    sys.exit("usage: make_golden.py <NEMO_3D directory of the reference> (or set NEMO3D_SRC)")
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 

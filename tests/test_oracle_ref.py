@@ -137,3 +137,52 @@ def test_sp3s_parameter_conversion(ref_sk):
         O.lib().orc_prepare_params(1, 0, O._p(np.ascontiguousarray(pv)),
                                    O._p(np.zeros(O.NSTR)), 0.0, float(mat["a0"]), O._p(ours))
         assert np.array_equal(ours[:35], ref), name
+
+
+@pytest.mark.parametrize("model,nbasis,norb", [("sp3d5s*_so", 20, 10), ("sp3s*_so", 10, 5)])
+def test_dangling_bond_passivation(ref_sk, model, nbasis, norb):
+    """The oracle's passivation of surface atoms against the reference's
+    h3d_diag_dangling_bond_shift_zincblende (mb_ham_spds_micro.c:1910-2150),
+    with the reference's own zincblende cell (Cell.c): a closed 3x3x3-cell
+    GaAs box with random vacancies, so that faces, edges, corners and
+    vacancy neighbours give every pattern of lost bonds and both signs of
+    the last bond's direction.  The oracle's addition is its on-site block
+    built with the passivation minus the block built without it (no strain
+    shift, so the difference is the term alone up to one rounding of the
+    diagonal)."""
+    from nemo3d_b200 import workloads as W
+    fam = ["GaAs_spds", "InAs_spds"] if norb == 10 else ["GaAs_sps", "InAs_sps"]
+    mats = [M.MATERIALS[m] for m in fam]
+    rng = np.random.default_rng(11)
+    st = W.gaas_cube(3)
+    t = st.types.reshape(-1).copy()
+    t[rng.random(t.size) < 0.08] = 0  # vacancies
+    st.types = t.reshape(st.types.shape)
+    shift = 30.0
+    on = O.OracleHamiltonian(st, norb, 2, mats, include_strain=False, passivate=True,
+                             dangling_shift=shift)
+    off = O.OracleHamiltonian(st, norb, 2, mats, include_strain=False, passivate=False)
+    nb = 2 * norb
+    dh = (on.onsite - off.onsite).reshape(on.natoms, nb, nb, 2)
+    occ = np.zeros(st.nsites, np.uint8)
+    occ[on.atom_slot] = 1  # the sites that hold an atom after the unbonded ones left
+    pairs = np.stack([on.atom_slot // 8, on.atom_slot % 8], -1).astype(np.int32)
+    payload = struct.pack("<5i", 4, nbasis, st.nx, st.ny, st.nz) + struct.pack("<d", shift)
+    payload += occ.tobytes() + struct.pack("<i", len(pairs)) + pairs.tobytes()
+    out = _run(ref_sk, payload)
+    step = nbasis * nbasis * 16
+    assert len(out) == step * len(pairs)
+    patterns = set()
+    nsurf = 0
+    for a in range(on.natoms):
+        ref = _cmat(out[a * step:(a + 1) * step], nbasis)
+        got = dh[a, ..., 0] + 1j * dh[a, ..., 1]
+        if on.surface[a]:
+            nsurf += 1
+            patterns.add(tuple(on.nbr[4 * a:4 * a + 4] >= 0))
+            # 1e-15 relative to the shift, one rounding of a ~10 eV diagonal
+            assert np.abs(got - ref).max() <= 2e-15 * shift, (a, np.abs(got - ref).max())
+        else:  # four bonds: nothing to passivate, in either code
+            assert np.abs(ref).max() == 0.0 and np.abs(got).max() == 0.0
+    assert nsurf > 100
+    assert len(patterns) >= 10, patterns  # most of the 15 bond-loss patterns occur
