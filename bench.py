@@ -1,20 +1,31 @@
-"""Benchmark: seconds to 8 band-edge eigenpairs of a ~1.0M-atom InAs dot.
+"""Benchmark: seconds to 8 band-edge eigenpairs of a ~2.0M-atom InAs dot.
 
-Workload: InAs lens (base 20 nm, height 5 nm) on a one-monolayer InAs wetting
-layer in a GaAs box of 58 x 58 x 38 cells (1,022,656 atoms), sp3d5s* with
-spin-orbit (20 orbitals per atom, H of dimension 20,453,120), dangling bonds
-passivated (+30 eV), atom positions displaced by a seeded Gaussian (sigma =
-0.5% of the bond length) as a strain stand-in.  One step = one full solve
-through libtbgpu: topology + Slater-Koster assembly from the structure, plain
-FP64 Lanczos with the reference's convergence test for the 4 lowest electron
-and 4 highest hole states (windows bracketing them), and the second Lanczos
-pass that builds the 8 eigenvectors.  Start vector uniform in [-1, 1], seed 0.
+Workload (the headline, configuration 3 of the target): InAs lens (base
+20 nm, height 5 nm) on a one-monolayer InAs wetting layer in a GaAs box of
+72 x 72 x 48 cells (1,990,656 atoms), sp3d5s* with spin-orbit (20 orbitals
+per atom, H of dimension 39,813,120), dangling bonds passivated (+30 eV),
+atom positions displaced by a seeded Gaussian (sigma = 0.5% of the bond
+length) as a strain stand-in.  One step = one full mixed-precision solve
+through libtbgpu: topology + Slater-Koster assembly from the structure into
+the single-precision store, Lanczos on complex-float vectors with double
+alpha/beta, tridiagonal and convergence test (the reference's windowed test)
+for the 4 highest hole and 4 lowest electron states, the eigenvector pass by
+regeneration of 256-iteration segments from first-pass checkpoints four at a
+time, and the double-precision Rayleigh-Ritz refinement.  Start vector
+uniform in [-1, 1], seed 0.
 
 ``value`` times steps whose inputs are already in HBM; ``e2e`` times the same
 solve through the host-pointer C ABI (geometry and start vector copied in,
-eigenvectors copied out).  ``--impl reference`` times the CPU oracle (a plain-C
-restatement of the reference's H*x and Lanczos recurrence, OpenMP over the
-host cores) on a bounded sample of iterations and scales it to a full solve.
+eigenvectors copied out).  The same run times the plain FP64 GPU Lanczos
+(the reference's method: double store and vectors, second run of the
+recurrence for the eigenvectors) on the same dot once, and reports the ratio,
+the per-state eigenvalue difference and the FP64 residual ||Hv - lambda v||
+of each mixed eigenpair through the recomputed double-precision product (a
+product independent of the stored blocks).  ``--workload dome1M`` is
+configuration 2 (1,022,656 atoms, plain FP64, 8 electron + 8 hole states).
+``--impl reference`` times the CPU oracle (a plain-C restatement of the
+reference's H*x and Lanczos recurrence, OpenMP over the host cores) on a
+bounded sample of iterations and scales it to a full solve.
 """
 
 from __future__ import annotations
@@ -35,21 +46,31 @@ sys.path.insert(0, ROOT)
 
 from nemo3d_b200 import materials, workloads  # noqa: E402
 
-# Algorithmic bytes per atom of one H*x in FP64 with the reference's compact
-# store (blocks once per bond, on-site diagonal + spin-orbit, int32 column
-# per bond, x read once, y written once): 1864 + 640 bytes.
-BYTES_PER_ATOM = 2504
-# DRAM bytes per atom of one H*x launch on this workload, measured with ncu
-# at full size (dram__bytes_read.sum + dram__bytes_write.sum, one pass, cold
-# L2): 2.80 GB read + 0.32 GB written per launch over 1,022,656 atoms.
-NCU_TRAFFIC_PER_ATOM = 3054
+METRIC = "s to 8 band-edge eigenpairs at <=1e-6 eV vs plain FP64 GPU Lanczos; SpMV HBM GB/s"
+# Algorithmic bytes per atom of one H*x with the reference's compact store
+# (blocks once per bond, on-site diagonal + spin-orbit, int32 column per bond,
+# x read once, y written once): FP64 1864 + 640, complex-float 936 + 320.
+BYTES_PER_ATOM = {64: 2504, 32: 1256}
+# DRAM bytes per atom of one H*x launch, measured with ncu (dram__bytes_read
+# + dram__bytes_write, one launch, cold L2) on the 384,000-atom profile case
+# and scaled by atoms: the float lane kernel 488.6 MB, the FP64 default
+# kernel 3054 B/atom at full size.
+NCU_TRAFFIC_PER_ATOM = {32: 1272, 64: 3054}
 
-# band-edge windows of this dot (eV): 4 highest hole and 4 lowest electron
-# states (Erange_vb / Erange_cb of the reference's Lanczos deck)
+# band-edge windows of the dome: 4 highest hole and 4 lowest electron states
+# (Erange_vb / Erange_cb of the reference's Lanczos deck)
 SOLVE = dict(ConvCheckStartIter=200, ConvCheckSkipRate=50, imax=20000,
              requested1=4, requested2=4, emin1=1.032, emax1=1.06,
              emin2=1.44, emax2=1.475, tolerance=1e-7)
 NVEC = 8
+# configuration 2: 8 hole and 8 electron states of the 1.02M-atom dome
+SOLVE_8X8 = dict(SOLVE, requested1=8, requested2=8, emin1=0.95, emax1=1.06, emin2=1.44,
+                 emax2=1.56, imax=30000)
+# the mixed-precision solver: float store and vectors, H*x variant 5 (lane
+# per atom and spin), eigenvector pass 1 (regeneration, 4 columns,
+# 256-iteration segments)
+MIXED_VARIANT = 5
+MIXED_VEC_PASS = (1, 4, 256)
 
 
 def peaks():
@@ -106,8 +127,10 @@ class ClockSampler:
                 "samples": len(self.rows)}
 
 
-def make_structure():
-    return workloads.dome_in_box(cells=(58, 58, 38), base_nm=20.0, height_nm=5.0,
+def make_structure(cells=(72, 72, 48)):
+    """The InAs dome in a GaAs box of the given cells (default: the 1,990,656-atom
+    dot of the headline; (58, 58, 38): the 1,022,656-atom dot)."""
+    return workloads.dome_in_box(cells=cells, base_nm=20.0, height_nm=5.0,
                                  sigma_frac=0.005, seed=1)
 
 
@@ -115,12 +138,16 @@ MATS = [materials.MATERIALS["GaAs_spds"], materials.MATERIALS["InAs_spds"]]
 
 
 # ------------------------------------------------------------------------------
-def cpu_sample(st, its_total, budget_s=20.0):
-    """Oracle (plain-C restatement, OpenMP) on a bounded sample: the H build
-    plus as many Lanczos iterations as fit the budget; scaled to a solve of
-    ``its_total`` iterations (both passes)."""
+def cpu_sample(st, its_total, budget_s=20.0, threads=None):
+    """Oracle (plain-C restatement of the reference's FP64 H*x and Lanczos
+    recurrence, OpenMP) on a bounded sample: the H build plus as many Lanczos
+    iterations as fit the budget, on ``threads`` host threads (all by
+    default); scaled to a solve of ``its_total`` iterations (both passes of
+    the plain method)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
+    cores = threads or os.cpu_count() or 1
+    os.environ["OMP_NUM_THREADS"] = str(cores)
     t0 = time.perf_counter()
     H = oracle.OracleHamiltonian(st, 10, 2, MATS)
     t_build = time.perf_counter() - t0
@@ -129,23 +156,24 @@ def cpu_sample(st, its_total, budget_s=20.0):
     t1 = time.perf_counter()
     H.lanczos(r0, imax=2, req=(1, 1), conv_start=10 ** 9)
     per = time.perf_counter() - t1
-    n_it = int(max(2, min(200, (budget_s - t_build) / max(per, 1e-6))))
+    n_it = int(max(2, min(400, (budget_s - t_build) / max(per, 1e-6))))
     t2 = time.perf_counter()
     H.lanczos(r0, imax=n_it + 1, req=(1, 1), conv_start=10 ** 9)
     per = (time.perf_counter() - t2) / n_it
-    cores = os.cpu_count() or 1
     est = t_build + per * its_total
     return dict(value=est, unit="s", cores=cores, kind="port",
-                sample=(f"oracle H build ({t_build:.1f} s) + {n_it} Lanczos iterations "
-                        f"({per * 1e3:.1f} ms each) on {H.natoms} atoms; scaled to "
-                        f"{its_total} iterations (first pass + eigenvector pass)"))
+                sample=(f"oracle H build ({t_build:.1f} s, timed) + {n_it} Lanczos iterations "
+                        f"(timed, {per * 1e3:.1f} ms each, no convergence checks) on {H.natoms} "
+                        f"atoms with {cores} threads; extrapolated to {its_total} iterations "
+                        f"(first pass + eigenvector pass of the plain FP64 method)"))
 
 
 # ------------------------------------------------------------------------------
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    st = make_structure()
+    cells = (58, 58, 38) if args.workload == "dome1M" else (72, 72, 48)
+    st = make_structure(cells)
     its = args.ref_iterations
     vals = []
     for i in range(args.warmup + args.steps):
@@ -154,12 +182,14 @@ def run_reference(args, rank, world):
             vals.append(cb["value"])
     v = float(np.mean(vals))
     cb["value"] = v
-    line = {"metric": "s to 8 band-edge eigenpairs at <=1e-6 eV vs plain FP64 GPU Lanczos; SpMV HBM GB/s",
+    line = {"metric": METRIC,
             "impl": "reference", "value": v, "unit": "s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3,
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "InAs dome 58x58x38 cells, 1,022,656 atoms, sp3d5s*+SO",
+            "config": {"workload": f"InAs dome {cells[0]}x{cells[1]}x{cells[2]} cells, "
+                                   f"{st.nsites} atoms, sp3d5s*+SO, plain FP64 Lanczos "
+                                   "(the reference's method)",
                        "states": "4 e + 4 h", "iterations": its},
             "cpu_baseline": cb,
             "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -177,6 +207,12 @@ def max_over_ranks(value, dist, device):
     return float(t.item())
 
 
+def _match_states(a, b):
+    """Per-state |a_i - b_j| pairing each value of a with the nearest of b."""
+    b = np.asarray(b)
+    return [float(np.abs(b - v).min()) if b.size else None for v in np.asarray(a)]
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     from nemo3d_b200 import tbgpu
@@ -187,8 +223,13 @@ def run_ours(args, rank, world, local_rank):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=torch.device("cuda", local_rank))
-    st = make_structure()
-    n_sites = st.nsites
+    cfg2 = args.workload == "dome1M"
+    cells = (58, 58, 38) if cfg2 else (72, 72, 48)
+    solve_kw = SOLVE_8X8 if cfg2 else SOLVE
+    nvec = 16 if cfg2 else NVEC
+    mixed = not cfg2
+    bits = 32 if mixed else 64
+    st = make_structure(cells)
     types_d = torch.from_numpy(np.ascontiguousarray(st.types).reshape(-1)).cuda()
     dsp_d = torch.from_numpy(np.ascontiguousarray(st.dsp).reshape(-1)).cuda()
     stream = torch.cuda.Stream()
@@ -197,21 +238,27 @@ def run_ours(args, rank, world, local_rank):
     probe.close()
     r0_h = workloads.random_start(n, seed=0)
     r0_d = torch.from_numpy(r0_h).cuda()
-    V_d = torch.empty(NVEC * 2 * n, dtype=torch.float64, device="cuda")
+    V_d = torch.empty(nvec * 2 * n, dtype=torch.float64, device="cuda")
     torch.cuda.synchronize()
 
-    stats_acc = []
-
-    def step(profile=False):
+    def solve(precision, V, profile=False):
+        """One full solve from device-resident inputs: build + solve (+ refine)."""
+        opts = dict(ham_bits=32, lanczos_bits=32) if precision == 32 else {}
         H = tbgpu.Hamiltonian(st, "sp3d5s*_so", MATS, build=False,
-                              device_inputs=(types_d.data_ptr(), dsp_d.data_ptr()))
+                              device_inputs=(types_d.data_ptr(), dsp_d.data_ptr()), **opts)
         H.set_stream(stream.cuda_stream)
-        H.set_spmv_variant(args.spmv_variant)
+        if precision == 32:
+            H.set_spmv_variant(MIXED_VARIANT)
+            H.set_eigenvector_pass(*MIXED_VEC_PASS)
+        else:
+            H.set_spmv_variant(args.spmv_variant)
         H.build()
         if profile:
             H.set_profiling(True)
-        res = H.eigensolve_lanczos_dev(r0_d.data_ptr(), V_d.data_ptr(), NVEC, **SOLVE)
+        res = H.eigensolve_lanczos_dev(r0_d.data_ptr(), V.data_ptr(), nvec, **solve_kw)
         s = H.stats()
+        if precision == 32:
+            res["state_resid"], res["state_delta"] = H.state_errors()
         H.close()
         return res, s
 
@@ -219,8 +266,9 @@ def run_ours(args, rank, world, local_rank):
         if dist is not None:
             dist.barrier()
 
+    stats_acc = []
     for _ in range(args.warmup):
-        res, s = step()
+        res, s = solve(bits, V_d)
     barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -229,12 +277,43 @@ def run_ours(args, rank, world, local_rank):
     with ClockSampler(smi_index) as clk:
         e0.record(stream)
         for _ in range(args.steps):
-            res, s = step(profile=True)
+            res, s = solve(bits, V_d, profile=True)
             stats_acc.append(s)
         e1.record(stream)
         torch.cuda.synchronize()
     barrier()
     ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, dist, "cuda")
+
+    # the plain FP64 GPU Lanczos on the same dot (the reference's method)
+    fp64 = None
+    if mixed and not args.no_fp64_baseline:
+        Vf = torch.empty_like(V_d)
+        torch.cuda.synchronize()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        rf, sf = solve(64, Vf)
+        f1.record(stream)
+        torch.cuda.synchronize()
+        fp64 = dict(res=rf, stats=sf, s=max_over_ranks(f0.elapsed_time(f1) / 1e3, dist, "cuda"))
+        del Vf
+        torch.cuda.empty_cache()
+
+    # FP64 residual ||H v - lambda v|| of each returned eigenpair through the
+    # recomputed double-precision product (independent of the stored blocks)
+    resid = []
+    if not args.no_residuals:
+        Hr = tbgpu.Hamiltonian(st, "sp3d5s*_so", MATS, build=False, recompute=True,
+                               device_inputs=(types_d.data_ptr(), dsp_d.data_ptr()))
+        Hr.build()
+        y = torch.empty(2 * n, dtype=torch.float64, device="cuda")
+        for e, lam in enumerate(res["values"][:nvec]):
+            v = V_d[e * 2 * n:(e + 1) * 2 * n]
+            Hr.hx_dev(v.data_ptr(), y.data_ptr(), float(lam))
+            torch.cuda.synchronize()
+            resid.append(float(torch.linalg.vector_norm(y).item() /
+                               torch.linalg.vector_norm(v).item()))
+        Hr.close()
+        del y
 
     # end to end through the host-pointer C ABI
     e2e_s = None
@@ -245,9 +324,14 @@ def run_ours(args, rank, world, local_rank):
             torch.cuda.synchronize()
             barrier()
             t0 = time.perf_counter()
-            H = tbgpu.Hamiltonian(st, "sp3d5s*_so", MATS)          # host geometry in
-            H.set_spmv_variant(args.spmv_variant)
-            out = H.eigensolve_lanczos(r0_h, vectors=NVEC, **SOLVE)  # host r0 in, vectors out
+            opts = dict(ham_bits=32, lanczos_bits=32) if mixed else {}
+            H = tbgpu.Hamiltonian(st, "sp3d5s*_so", MATS, **opts)   # host geometry in
+            if mixed:
+                H.set_spmv_variant(MIXED_VARIANT)
+                H.set_eigenvector_pass(*MIXED_VEC_PASS)
+            else:
+                H.set_spmv_variant(args.spmv_variant)
+            out = H.eigensolve_lanczos(r0_h, vectors=nvec, **solve_kw)  # host r0 in, vectors out
             H.close()
             torch.cuda.synchronize()
             times.append(time.perf_counter() - t0)
@@ -259,39 +343,56 @@ def run_ours(args, rank, world, local_rank):
         pk, pk_kind = peaks()
         last = stats_acc[-1]
         spmv_ms = last["spmv_ms"] / max(last["spmv_launches"], 1)
-        achieved = BYTES_PER_ATOM * natoms / (spmv_ms * 1e-3) / 1e9
+        achieved = BYTES_PER_ATOM[bits] * natoms / (spmv_ms * 1e-3) / 1e9
         its_total = int(res["iterations"] + (max(res["conv_iterations"])
                                               if len(res["conv_iterations"]) else 0))
+        name = (f"InAs dome {cells[0]}x{cells[1]}x{cells[2]} cells, {natoms:,} atoms, sp3d5s*+SO, "
+                + ("mixed-precision Lanczos (complex-float store and vectors, FP64 alpha/beta, "
+                   "tridiagonal and Rayleigh-Ritz refinement), eigenvectors regenerated from "
+                   "checkpoints" if mixed else "plain FP64 Lanczos, 8 e + 8 h"))
+        cfg = {"workload": name, "natoms": natoms, "dimension": n,
+               "states": "4 e + 4 h (8 eigenpairs)" if mixed else "8 e + 8 h (16 eigenpairs)",
+               "parallelism": f"replicas x{world} (one dot per GPU)",
+               "l2": "inputs larger than L2 (H 1.9-6.4 GB, vectors 318-636 MB each)",
+               "eigenvalues": [round(float(v), 12) for v in res["values"]],
+               "iterations_first_pass": int(res["iterations"]),
+               "build_ms": last["build_ms"], "solve_ms": last["solve_ms"],
+               "vectors_ms": last["vectors_ms"], "refine_ms": last["refine_ms"],
+               "vec_segments": last["vec_segments"], "vec_mismatch": last["vec_mismatch"],
+               "residual_per_state_ev": resid, "tolerance": solve_kw["tolerance"]}
+        if mixed:
+            cfg["refine_residual_per_state_ev"] = [float(v) for v in res["state_resid"]]
+        if fp64 is not None:
+            cfg["fp64_plain"] = {
+                "s": fp64["s"], "iterations_first_pass": int(fp64["res"]["iterations"]),
+                "first_pass_ms": fp64["stats"]["solve_ms"],
+                "vectors_ms": fp64["stats"]["vectors_ms"],
+                "eigenvalues": [round(float(v), 12) for v in fp64["res"]["values"]]}
+            cfg["speedup_vs_fp64_plain"] = fp64["s"] / (ms / 1e3)
+            cfg["error_per_state_ev_vs_fp64"] = _match_states(res["values"], fp64["res"]["values"])
         line = {
-            "metric": "s to 8 band-edge eigenpairs at <=1e-6 eV vs plain FP64 GPU Lanczos; SpMV HBM GB/s",
+            "metric": METRIC,
             "value": ms / 1e3, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "scaling": "weak", "vs_baseline": None, "dtype": "c32+f64" if mixed else "f64",
             "data": "synthetic (seeded InAs dome in GaAs, Gaussian displacements)",
-            "config": {"workload": "InAs dome 58x58x38 cells, 1,022,656 atoms, sp3d5s*+SO, plain FP64 Lanczos",
-                       "natoms": natoms, "dimension": n, "states": "4 e + 4 h (8 eigenpairs)",
-                       "parallelism": f"replicas x{world} (one dot per GPU)",
-                       "l2": "inputs larger than L2 (H 3.3 GB, vectors 327 MB each)",
-                       "eigenvalues": [round(v, 9) for v in res["values"].tolist()],
-                       "iterations_first_pass": int(res["iterations"]),
-                       "iterations_total": its_total,
-                       "build_ms": last["build_ms"], "solve_ms": last["solve_ms"],
-                       "vectors_ms": last["vectors_ms"]},
+            "config": cfg,
             "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "steps": args.e2e_steps},
-            "gpu_launches": int(sum(s["kernel_launches"] for s in stats_acc) // len(stats_acc) + 4),
+            "gpu_launches": int(sum(x["kernel_launches"] for x in stats_acc) // len(stats_acc) + 4),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"],
                          "unit": "GB/s", "frac": achieved / pk["hbm_gbs"],
                          "peak_source": pk_kind,
-                         "traffic": (None if NCU_TRAFFIC_PER_ATOM is None
-                                     else NCU_TRAFFIC_PER_ATOM * natoms),
-                         "kernel": "k_spmv (H*x with fused alpha)",
-                         "algorithmic_bytes": BYTES_PER_ATOM * natoms,
+                         "traffic": NCU_TRAFFIC_PER_ATOM[bits] * natoms,
+                         "kernel": "H*x with fused alpha (first pass), "
+                                   + ("complex-float lane kernel" if mixed else "FP64"),
+                         "algorithmic_bytes": BYTES_PER_ATOM[bits] * natoms,
                          "avg_launch_ms": spmv_ms},
             "clocks": clk.summary(),
         }
         if not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_sample(st, its_total, budget_s=args.cpu_budget)
+            fp_its = (int(fp64["res"]["iterations"]) * 2 if fp64 is not None else its_total)
+            line["cpu_baseline"] = cpu_sample(st, fp_its, budget_s=args.cpu_budget)
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
@@ -306,8 +407,8 @@ def run_profile_case(args):
     import torch
     from nemo3d_b200 import tbgpu
     torch.cuda.set_device(0)
-    if args.profile_full:  # the bench's own 1.02M-atom dot (for 1-pass captures)
-        st = make_structure()
+    if args.profile_full:  # the 1.02M-atom dot (for 1-pass captures)
+        st = make_structure((58, 58, 38))
     else:
         st = workloads.dome_in_box(cells=(40, 40, 30), base_nm=14.0, height_nm=4.0,
                                    sigma_frac=0.005, seed=1)
@@ -381,12 +482,15 @@ def run_extra(args):
     torch.cuda.set_device(0)
     w = args.workload
     if w == "kernels":
-        st = make_structure()
+        st = make_structure((58, 58, 38))
         for name, opts, f32, var in (
                 ("fp64 store", {}, False, 0),
                 ("fp64 store, two-cell units (variant 3)", {}, False, 3),
                 ("fp64 store, every piece by cp.async (variant 4)", {}, False, 4),
+                ("fp64 store, lane per atom and spin (variant 5)", {}, False, 5),
                 ("float store, float vectors", dict(ham_bits=32, lanczos_bits=32), True, 0),
+                ("float store, float vectors, lane per atom and spin (variant 5)",
+                 dict(ham_bits=32, lanczos_bits=32), True, 5),
                 ("recompute fp64", dict(recompute=True), False, 0),
                 ("recompute float", dict(recompute=True, lanczos_bits=32), True, 0)):
             H = tbgpu.Hamiltonian(st, "sp3d5s*_so", MATS, **opts)
@@ -408,14 +512,33 @@ def run_extra(args):
         st = workloads.dome_in_box(cells=(72, 72, 48), base_nm=20.0, height_nm=5.0,
                                    sigma_frac=0.005, seed=1)
         ref = None
-        for name, opts in (("fp64", {}), ("mixed, float store", dict(ham_bits=32, lanczos_bits=32)),
-                           ("mixed, recompute", dict(recompute=True, lanczos_bits=32))):
+        f32 = dict(ham_bits=32, lanczos_bits=32)
+        # (name, options, H*x variant, eigenvector pass (mode, columns,
+        # segment) or None, tolerance)
+        variants = [("fp64", {}, 0, None, 1e-7),
+                    ("mixed, float store", f32, 0, None, 1e-7),
+                    ("mixed, float store, lane kernel", f32, 5, None, 1e-7),
+                    ("mixed, float store, regenerated vectors P=4 L=256", f32, 5, (1, 4, 256), 1e-7),
+                    ("mixed, float store, regenerated vectors P=2 L=256", f32, 5, (1, 2, 256), 1e-7),
+                    ("mixed, float store, regenerated vectors P=4 L=256, tol 1e-6", f32, 5,
+                     (1, 4, 256), 1e-6),
+                    ("mixed, float store, regenerated vectors P=4 L=256, tol 1e-5", f32, 5,
+                     (1, 4, 256), 1e-5),
+                    ("fp64, regenerated vectors P=2 L=256", {}, 5, (1, 2, 256), 1e-7)]
+        if args.mixed_recompute:
+            variants.append(("mixed, recompute", dict(recompute=True, lanczos_bits=32), 0, None,
+                             1e-7))
+        for name, opts, var, vpass, tol in variants:
             H = tbgpu.Hamiltonian(st, "sp3d5s*_so", MATS, **opts)
+            H.set_spmv_variant(var)
+            if vpass:
+                H.set_eigenvector_pass(*vpass)
             r0 = torch.from_numpy(workloads.random_start(H.n, seed=0)).cuda()
             V = torch.empty((NVEC, 2 * H.n), dtype=torch.float64, device="cuda")
             torch.cuda.synchronize()
             t = time.time()
-            res = H.eigensolve_lanczos_dev(r0.data_ptr(), V.data_ptr(), NVEC, **SOLVE)
+            res = H.eigensolve_lanczos_dev(r0.data_ptr(), V.data_ptr(), NVEC,
+                                           **dict(SOLVE, tolerance=tol))
             torch.cuda.synchronize()
             wall = time.time() - t
             stt = H.stats()
@@ -423,6 +546,7 @@ def run_extra(args):
                     "natoms": H.natoms, "value": wall, "unit": "s",
                     "first_pass_ms": stt["solve_ms"], "vectors_ms": stt["vectors_ms"],
                     "refine_ms": stt["refine_ms"], "iterations": res["iterations"],
+                    "vec_segments": stt["vec_segments"], "vec_mismatch": stt["vec_mismatch"],
                     "eigenvalues": [round(float(v), 12) for v in res["values"]]}
             if ref is None:
                 ref = res["values"]
@@ -590,6 +714,10 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64-baseline", action="store_true",
+                    help="skip the plain FP64 solve of the same dot")
+    ap.add_argument("--no-residuals", action="store_true",
+                    help="skip the FP64 residuals of the returned eigenpairs")
     ap.add_argument("--profile-case", action="store_true",
                     help="small-case run of the solver kernels for ncu captures")
     ap.add_argument("--profile-iterations", type=int, default=6)
@@ -603,24 +731,29 @@ def main():
                     help="with --profile-case: a converging solve with the eigenvector pass")
     ap.add_argument("--profile-vff", action="store_true",
                     help="with --profile-case: a few Keating VFF iterations instead")
-    ap.add_argument("--spmv-variant", type=int, default=0, choices=[0, 1, 2, 3, 4],
+    ap.add_argument("--spmv-variant", type=int, default=0, choices=[0, 1, 2, 3, 4, 5],
                     help="H*x kernel of the solve (tbgpu_set_spmv_variant)")
+    ap.add_argument("--mixed-recompute", action="store_true",
+                    help="--workload mixed2M: also the mixed solve on the recompute product")
     ap.add_argument("--warm-train", type=int, default=64,
                     help="--workload warm: training dots")
     ap.add_argument("--warm-test", type=int, default=16, help="--workload warm: held-out dots")
     ap.add_argument("--warm-epochs", type=int, default=300, help="--workload warm: epochs")
-    ap.add_argument("--workload", default="dome1M",
-                    choices=["dome1M", "kernels", "mixed2M", "batch256", "vff1M", "warm"],
-                    help="dome1M: the headline bench; the others: measurements beside it")
-    ap.add_argument("--ref-iterations", type=int, default=19002,
-                    help="iterations of a full solve (both passes) the CPU sample is scaled to")
+    ap.add_argument("--workload", default="dot2M",
+                    choices=["dot2M", "dome1M", "kernels", "mixed2M", "batch256", "vff1M", "warm"],
+                    help="dot2M: the headline bench (mixed precision, 1,990,656 atoms); "
+                         "dome1M: plain FP64, 8 e + 8 h on 1,022,656 atoms; the others: "
+                         "measurements beside it")
+    ap.add_argument("--ref-iterations", type=int, default=19802,
+                    help="iterations of a full solve (both passes of the plain FP64 method) "
+                         "the CPU sample is scaled to")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     if args.profile_case:
         run_profile_case(args)
-    elif args.workload != "dome1M":
+    elif args.workload not in ("dot2M", "dome1M"):
         if rank == 0:
             run_extra(args)
     elif args.impl == "reference":

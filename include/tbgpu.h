@@ -324,13 +324,16 @@ int tbgpu_hx_dot_noalloc(tbgpu_ctx *ctx, double shift, const double *x_dev,
  * 7 warps x 2 stages, 3 = two-cell unit kernel (bulk copies of each unit's
  * contiguous pieces; 10-orbital models with the 64-bit store at the Gamma
  * point, else as 0), 4 = the default kernel with every piece, the cation
- * block runs included, by 16-byte cp.async.  Variants 0, 2, 3 and 4 give
- * the same y bit for bit; 1 sums in its own order (equal to rounding). */
+ * block runs included, by 16-byte cp.async, 5 = one lane per (atom, spin)
+ * with block rows loaded straight to registers (10-orbital models with a
+ * stored Hamiltonian at the Gamma point, else as 0).  Variants 0, 2, 3 and
+ * 4 give the same y bit for bit; 1 and 5 sum in their own orders (equal to
+ * rounding). */
 int tbgpu_set_spmv_variant(tbgpu_ctx *ctx, int variant);
 
 /* Autotuner: times the H*x variants that are distinct kernels for the built
- * context (all five for the 10-orbital models with the 64-bit store at the
- * Gamma point, 0 and 1 with the 32-bit store, only 0 for 5-orbital models,
+ * context (all six for the 10-orbital models with the 64-bit store at the
+ * Gamma point, 0, 1 and 5 with the 32-bit store, only 0 for 5-orbital models,
  * Bloch phases and recompute storage), reps launches each with the fused
  * Lanczos dot after two untimed ones (CUDA events on the context stream;
  * two temporary device vectors), selects the fastest (ties: the lower
@@ -464,8 +467,29 @@ typedef struct {
   long lanczos_iterations;
   long kernel_launches;       /* all kernels launched by the last solve       */
   double refine_ms;           /* double-precision refinement (mixed solve)    */
+  long vec_segments;          /* eigenvector pass 1: segments regenerated     */
+  long vec_mismatch;          /* ... whose last vector differed, bit for bit, */
+                              /* from the first pass's checkpoint (0 expected) */
 } tbgpu_stats;
 int tbgpu_set_profiling(tbgpu_ctx *ctx, int on);
+
+/* Eigenvector pass of the Lanczos solves (no counterpart in the reference,
+ * whose eigenvectorsLanczos reruns the whole recurrence from the start
+ * vector, eigen/src/lanczos.c:1364-1689).  mode 0 (default) is that second
+ * run.  mode 1: the first pass also saves the two Lanczos vectors that start
+ * every segment of `segment` iterations (2 vectors per segment in device
+ * memory), and the eigenvector pass regenerates `columns` segments at once:
+ * one product reads each bond block once for all of them (10-orbital models
+ * with a stored Hamiltonian at the Gamma point; columns 1..4 for the
+ * mixed-precision solve, 1..2 for double vectors), with the three-term
+ * update fused into the product.  Every product of both passes then uses the
+ * lane-per-(atom, spin) kernel (H*x variant 5), whose columns compute
+ * exactly as a one-column launch: the regenerated vectors equal the first
+ * pass's bit for bit (checked at every segment end, tbgpu_stats.vec_mismatch),
+ * so the eigenvalues are those of mode 0 and the eigenvectors differ only by
+ * the order of the accumulation.  Where the mode does not apply, or the
+ * checkpoints do not fit in device memory, the solve uses mode 0. */
+int tbgpu_set_eigenvector_pass(tbgpu_ctx *ctx, int mode, int columns, int segment);
 int tbgpu_get_stats(const tbgpu_ctx *ctx, tbgpu_stats *out);
 
 /* Failure-detection self-test: one warp waits, with the bounded poll loop

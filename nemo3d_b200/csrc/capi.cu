@@ -43,7 +43,8 @@ static void free_ctx(Ctx *c) {
   void *ptrs[] = {c->d_type, c->d_dsp, c->d_par, c->d_par_ok, c->d_site_index, c->d_atom_site,
                   c->d_nbr, c->d_site_m, c->d_surface, c->d_onsite, c->d_blocks, c->d_partial,
                   c->d_counter, c->d_status, c->d_x, c->d_y, c->d_phase, c->d_groups,
-                  c->d_blocks32, c->d_onsite32, c->d_rc_order, c->d_units, c->d_start};
+                  c->d_blocks32, c->d_onsite32, c->d_rc_order, c->d_units, c->d_start,
+                  c->d_lane_tasks};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -443,15 +444,16 @@ int tbgpu_export_hamiltonian(const tbgpu_ctx *ctx, double *onsite, double *block
 }
 
 int tbgpu_set_spmv_variant(tbgpu_ctx *ctx, int variant) {
-  if (!ctx || variant < 0 || variant > 4) return set_error(TBGPU_E_ARG);
+  if (!ctx || variant < 0 || variant > 5) return set_error(TBGPU_E_ARG);
   C(ctx)->spmv_variant = variant;
   return TBGPU_OK;
 }
 
-// The variants that launch distinct kernels for this context: all five for
+// The variants that launch distinct kernels for this context: all six for
 // the 10-orbital models with the double store at the Gamma point; the
-// warp-staged and the lane-gather kernel with the float store; one kernel
-// otherwise (5-orbital models, Bloch phases, recompute storage).
+// warp-staged, the lane-gather and the lane-per-(atom, spin) kernel with the
+// float store; one kernel otherwise (5-orbital models, Bloch phases,
+// recompute storage).
 static int distinct_variants(const Ctx &c, int *v) {
   if (c.norb != 10 || c.bloch || c.recompute) {
     v[0] = 0;
@@ -460,10 +462,11 @@ static int distinct_variants(const Ctx &c, int *v) {
   if (c.ham_fp32) {
     v[0] = 0;
     v[1] = 1;
-    return 2;
+    v[2] = 5;
+    return 3;
   }
-  for (int i = 0; i < 5; i++) v[i] = i;
-  return 5;
+  for (int i = 0; i < 6; i++) v[i] = i;
+  return 6;
 }
 
 // Times the context's distinct H*x variants (the product with the fused
@@ -489,7 +492,7 @@ int tbgpu_autotune_spmv(tbgpu_ctx *ctx, int reps, int *variant_out, double *ms_o
              cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
     rc = TBGPU_E_CUDA;
   }
-  int cand[5];
+  int cand[6];
   const int ncand = distinct_variants(c, cand);
   for (int ci = 0; ci < ncand && rc == TBGPU_OK; ci++) {
     const int v = cand[ci];
@@ -585,6 +588,17 @@ int tbgpu_set_profiling(tbgpu_ctx *ctx, int on) {
 int tbgpu_get_stats(const tbgpu_ctx *ctx, tbgpu_stats *out) {
   if (!ctx || !out) return set_error(TBGPU_E_ARG);
   *out = C(ctx)->stats;
+  return TBGPU_OK;
+}
+
+int tbgpu_set_eigenvector_pass(tbgpu_ctx *ctx, int mode, int columns, int segment) {
+  if (!ctx || mode < 0 || mode > 1 || columns < 1 || columns > lane_max_cols(true) ||
+      segment < 16 || segment > (1 << 20))
+    return set_error(TBGPU_E_ARG);
+  Ctx &c = *C(ctx);
+  c.vec_pass = mode;
+  c.vec_columns = columns;
+  c.vec_segment = segment;
   return TBGPU_OK;
 }
 

@@ -26,6 +26,7 @@
 #include <vector>
 
 #include "host_par.h"
+#include "lanczos_step.cuh"
 #include "reduce.cuh"
 #include "tbgpu_internal.cuh"
 
@@ -105,13 +106,9 @@ __global__ void __launch_bounds__(kRedThreads)
   for (long j = blockIdx.x * (long)blockDim.x + threadIdx.x; j < n2;
        j += (long)gridDim.x * blockDim.x) {
     const double2 wv = widen(w[j]), cv = widen(rc[j]);
-    const double2 q = make_double2(cv.x * iq, cv.y * iq);
-    double2 p = make_double2(0.0, 0.0);
-    if (it > 0) {
-      const double2 pv = widen(rp[j]);
-      p = make_double2(pv.x * ip, pv.y * ip);
-    }
-    const VT r = narrow<VT>(wv.x - (al * q.x + bprev * p.x), wv.y - (al * q.y + bprev * p.y));
+    const double2 pv = it > 0 ? widen(rp[j]) : make_double2(0.0, 0.0);
+    const double2 rr = lanczos_update_entry(wv, cv, pv, al, bprev, iq, ip);
+    const VT r = narrow<VT>(rr.x, rr.y);
     rout[j] = r;
     const double2 rw = widen(r);  // the norm of the vector as stored
     s += rw.x * rw.x + rw.y * rw.y;
@@ -121,15 +118,20 @@ __global__ void __launch_bounds__(kRedThreads)
 
 constexpr int kMaxChunk = 32;
 constexpr int kVecGroup = 16;
-template <typename VT>
+// the regenerating eigenvector pass accumulates up to 64 rows (its columns'
+// chunks together) into groups of 8 eigenvectors
+constexpr int kRegenRows = 64;
+constexpr int kRegenGroup = 8;
+template <typename VT, int ROWS = kMaxChunk>
 struct ChunkPtrs {
-  const VT *r[kMaxChunk];
+  const VT *r[ROWS];
 };
 
 // Coefficients of one chunk, passed by value: the kernel reads them from the
 // parameter bank as FMA operands (no shared-memory traffic per element).
+template <int ROWS = kMaxChunk, int VG = kVecGroup>
 struct ChunkCoef {
-  double c[kMaxChunk][kVecGroup];
+  double c[ROWS][VG];
 };
 
 // V[e] += sum_k coef[k][e] * R_k for one group of NV vectors (memory bound:
@@ -147,16 +149,16 @@ template <int NV, typename VT>
 constexpr int accum_min_blocks() {  // float vectors: more registers to widen them
   return sizeof(VT) != sizeof(double2) ? (NV <= 12 ? 2 : 1) : NV <= 8 ? 4 : NV <= 12 ? 2 : 1;
 }
-template <int NV, typename VT>
+template <int NV, typename VT, int ROWS, int VG>
 __global__ void __launch_bounds__(256, accum_min_blocks<NV, VT>())
-    k_accum(long n2, ChunkPtrs<VT> R, ChunkCoef C, double2 *__restrict__ V) {
+    k_accum(long n2, ChunkPtrs<VT, ROWS> R, ChunkCoef<ROWS, VG> C, double2 *__restrict__ V) {
   for (long j = blockIdx.x * (long)blockDim.x + threadIdx.x; j < n2;
        j += (long)gridDim.x * blockDim.x) {
     double2 acc[NV];
 #pragma unroll
     for (int e = 0; e < NV; e++) acc[e] = V[e * n2 + j];
 #pragma unroll
-    for (int k0 = 0; k0 < kMaxChunk; k0 += kAccumBatch) {
+    for (int k0 = 0; k0 < ROWS; k0 += kAccumBatch) {
       double2 r[kAccumBatch];
 #pragma unroll
       for (int b = 0; b < kAccumBatch; b++) r[b] = widen(__ldg(R.r[k0 + b] + j));
@@ -173,12 +175,15 @@ __global__ void __launch_bounds__(256, accum_min_blocks<NV, VT>())
   }
 }
 
-template <typename VT>
+template <typename VT, int ROWS = kMaxChunk, int VG = kVecGroup>
 static void launch_accum(int nv, unsigned grid, cudaStream_t s, long n2,
-                         const ChunkPtrs<VT> &R, const ChunkCoef &C, double2 *V) {
+                         const ChunkPtrs<VT, ROWS> &R, const ChunkCoef<ROWS, VG> &C,
+                         double2 *V) {
   switch (nv) {
 #define TBGPU_ACCUM_CASE(N) \
-  case N: k_accum<N, VT><<<grid, 256, 0, s>>>(n2, R, C, V); break;
+  case N:                   \
+    if constexpr (N <= VG) k_accum<N, VT, ROWS, VG><<<grid, 256, 0, s>>>(n2, R, C, V); \
+    break;
     TBGPU_ACCUM_CASE(1) TBGPU_ACCUM_CASE(2) TBGPU_ACCUM_CASE(3) TBGPU_ACCUM_CASE(4)
     TBGPU_ACCUM_CASE(5) TBGPU_ACCUM_CASE(6) TBGPU_ACCUM_CASE(7) TBGPU_ACCUM_CASE(8)
     TBGPU_ACCUM_CASE(9) TBGPU_ACCUM_CASE(10) TBGPU_ACCUM_CASE(11) TBGPU_ACCUM_CASE(12)
@@ -186,6 +191,17 @@ static void launch_accum(int nv, unsigned grid, cudaStream_t s, long n2,
 #undef TBGPU_ACCUM_CASE
     default: break;
   }
+}
+
+// number of 32-bit words of two vectors that differ (bit comparison)
+__global__ void k_count_diff(long nwords, const unsigned *__restrict__ a,
+                             const unsigned *__restrict__ b, unsigned long long *count) {
+  unsigned long long d = 0;
+  for (long j = blockIdx.x * (long)blockDim.x + threadIdx.x; j < nwords;
+       j += (long)gridDim.x * blockDim.x)
+    d += a[j] != b[j];
+  for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+  if ((threadIdx.x & 31) == 0 && d) atomicAdd(count, d);
 }
 
 // ---------------------------------------------------------------------------
@@ -458,6 +474,8 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
   c.state_resid.clear();
   c.state_delta.clear();
   c.stats.refine_ms = 0.0;
+  c.stats.vec_segments = 0;
+  c.stats.vec_mismatch = 0;
   const long n2 = c.natoms * c.nb;  // complex entries
   const size_t vbytes = sizeof(VT) * n2;        // one Lanczos vector
   const size_t ebytes = sizeof(double2) * n2;   // one eigenvector (always double)
@@ -476,7 +494,30 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
   double *d_alpha = nullptr, *d_bet = nullptr, *d_tmp = nullptr;
   double *h_alpha = nullptr, *h_bet = nullptr;
   std::vector<cudaEvent_t> spmv_ev;
+  // eigenvector pass by regeneration (tbgpu_set_eigenvector_pass): the
+  // first pass saves r_it and r_{it-1} at every it = 0, L, 2L, ..., and both
+  // passes run the lane kernel, whose columns compute as one-column launches
+  bool regen = c.vec_pass == 1 && V_dev && maxvec > 0 && lane_supported(c) &&
+               (!kMixed || c.ham_fp32);
+  const int keep_variant = c.spmv_variant;
+  if (regen) c.spmv_variant = 5;
+  const int L = std::max(c.vec_segment, 16);
+  const int P = std::max(1, std::min(c.vec_columns, lane_max_cols(kMixed)));
+  std::vector<VT *> ck_cur, ck_prev, rr;  // checkpoints; the pass-2 rings
+  unsigned long long *d_diff = nullptr;
+  auto drop_checkpoints = [&]() {
+    for (VT *q : ck_cur) if (q) cudaFreeAsync(q, s);
+    for (VT *q : ck_prev) if (q) cudaFreeAsync(q, s);
+    ck_cur.clear();
+    ck_prev.clear();
+  };
   auto cleanup = [&]() {
+    c.spmv_variant = keep_variant;
+    drop_checkpoints();
+    for (VT *q : rr) if (q) cudaFreeAsync(q, s);
+    rr.clear();
+    if (d_diff) cudaFreeAsync(d_diff, s);
+    d_diff = nullptr;
     for (int i = 0; i <= kMaxChunk; i++)
       if (ring[i]) cudaFree(ring[i]);
     if (W) cudaFree(W);
@@ -577,9 +618,38 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
     cudaEvent_t ev;
   };
   std::vector<Pending> pend;
+  // checkpoint of iteration it: copies of r_it and r_{it-1} (stream ordered,
+  // after the step that wrote them, before any step overwrites them); when
+  // device memory runs short the solve falls back to the second run
+  const size_t ring_need = size_t(P) * (kRegenRows / P + 2) * vbytes + (512ull << 20);
+  auto checkpoint = [&](int it) -> int {
+    size_t fre = 0, tot = 0;
+    cudaMemGetInfo(&fre, &tot);
+    VT *a = nullptr, *b = nullptr;
+    bool ok = fre > 2 * vbytes + ring_need && cudaMallocAsync(&a, vbytes, s) == cudaSuccess;
+    if (ok && it > 0) ok = cudaMallocAsync(&b, vbytes, s) == cudaSuccess;
+    if (!ok) {
+      cudaGetLastError();  // a failed allocation is not an error of the solve
+      if (a) cudaFreeAsync(a, s);
+      drop_checkpoints();
+      regen = false;
+      return TBGPU_OK;
+    }
+    if (cudaMemcpyAsync(a, ring[it % S1], vbytes, cudaMemcpyDeviceToDevice, s) != cudaSuccess ||
+        (b && cudaMemcpyAsync(b, ring[(it + S1 - 1) % S1], vbytes, cudaMemcpyDeviceToDevice,
+                              s) != cudaSuccess))
+      return set_error(TBGPU_E_CUDA);
+    ck_cur.push_back(a);
+    ck_prev.push_back(b);
+    return TBGPU_OK;
+  };
   auto enqueue_until = [&](int upto) -> int {  // launch iterations [launched, upto)
     const int lim = std::min(upto, A.imax - 1);
     for (; launched < lim; launched++) {
+      if (regen && launched % L == 0) {
+        int r_ = checkpoint(launched);
+        if (r_) return r_;
+      }
       int r_ = step(launched, S1, d_bet);
       if (r_) return r_;
     }
@@ -673,11 +743,15 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
 
   // ---- second pass: eigenvectors -------------------------------------------
   const int nvec = std::min(ne, std::max(maxvec, 0));
+  std::vector<double> coef_all;
+  if (!V_dev || nvec <= 0) drop_checkpoints();
   if (V_dev && nvec > 0) {
     // Ritz coefficients on the truncated tridiagonal of each eigenvalue
     int maxit = 0;
     for (int k = 0; k < nvec; k++) maxit = std::max(maxit, found[k].second);
-    std::vector<double> coef(size_t(maxit) * nvec, 0.0), x;
+    std::vector<double> &coef = coef_all;
+    coef.assign(size_t(maxit) * nvec, 0.0);
+    std::vector<double> x;
     for (int k = 0; k < nvec; k++) {
       const int req = found[k].second;
       if (!inverse_iteration(req, Ta.data(), Tb.data(), found[k].first, rng, x)) {
@@ -689,6 +763,117 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
     }
     // bet of the first pass up to maxit is needed on the host
     if (maxit > final_it) maxit = final_it;
+    const int nseg = (maxit + L - 1) / L;
+    if (regen && int(ck_cur.size()) < nseg) regen = false;  // (cannot happen: maxit <= launched)
+    c.stats.vec_segments = 0;
+    c.stats.vec_mismatch = 0;
+  }
+  if (V_dev && nvec > 0 && regen) {
+    // ---- eigenvector pass by regeneration: P segments at a time ------------
+    int maxit = 0;
+    for (int k = 0; k < nvec; k++) maxit = std::max(maxit, found[k].second);
+    if (maxit > final_it) maxit = final_it;
+    const int nseg = (maxit + L - 1) / L;
+    const int K = kRegenRows / P;  // accumulation rows per column
+    const int R = K + 2;           // ring per column: K inputs, the previous r, the output
+    rr.assign(size_t(P) * R, nullptr);
+    for (auto &q : rr) SOLVE_CUDA(cudaMallocAsync(&q, vbytes, s));
+    SOLVE_CUDA(cudaMallocAsync(&d_diff, sizeof(unsigned long long) * std::max(nseg, 1), s));
+    SOLVE_CUDA(cudaMemsetAsync(d_diff, 0, sizeof(unsigned long long) * std::max(nseg, 1), s));
+    SOLVE_CUDA(cudaMemsetAsync(V_dev, 0, ebytes * nvec, s));
+    cudaEventRecord(tm.t2, s);
+    std::vector<char> checked(nseg, 0);
+    for (int g0 = 0; g0 < nseg; g0 += P) {
+      const int ncol = std::min(P, nseg - g0);
+      int len[4] = {0, 0, 0, 0}, steps = 0;
+      for (int q = 0; q < ncol; q++) {
+        const int seg = g0 + q;
+        len[q] = std::min(L, maxit - seg * L);
+        steps = std::max(steps, len[q]);
+        SOLVE_CUDA(cudaMemcpyAsync(rr[q * R], ck_cur[seg], vbytes, cudaMemcpyDeviceToDevice, s));
+        if (seg > 0)
+          SOLVE_CUDA(cudaMemcpyAsync(rr[q * R + R - 1], ck_prev[seg], vbytes,
+                                     cudaMemcpyDeviceToDevice, s));
+      }
+      int j0 = 0;
+      for (int j = 0; j < steps; j++) {
+        int na = 0;  // only the last segment can be short: the active columns are a prefix
+        while (na < ncol && len[na] > j) na++;
+        const VT *xs[4] = {nullptr, nullptr, nullptr, nullptr};
+        const VT *rps[4] = {nullptr, nullptr, nullptr, nullptr};
+        VT *ys[4] = {nullptr, nullptr, nullptr, nullptr};
+        int its[4] = {0, 0, 0, 0};
+        for (int q = 0; q < na; q++) {
+          const int seg = g0 + q;
+          xs[q] = rr[q * R + j % R];
+          rps[q] = (seg == 0 && j == 0) ? nullptr : rr[q * R + (j + R - 1) % R];
+          ys[q] = rr[q * R + (j + 1) % R];
+          its[q] = seg * L + j;
+        }
+        SOLVE_RC(launch_lane_regen<VT>(c, na, xs, ys, rps, its, d_bet, d_alpha, s));
+        launches++;
+        if (j + 1 - j0 == K || j == steps - 1) {  // accumulate the columns' inputs j0..j
+          ChunkPtrs<VT, kRegenRows> Pr{};
+          int rowit[kRegenRows];
+          int nr = 0;
+          for (int q = 0; q < ncol; q++)
+            for (int jj = j0; jj <= j && jj < len[q]; jj++) {
+              Pr.r[nr] = rr[q * R + jj % R];
+              rowit[nr++] = (g0 + q) * L + jj;
+            }
+          for (int k = nr; k < kRegenRows; k++) Pr.r[k] = Pr.r[0];  // zero coefficients
+          for (int g = 0; g < nvec; g += kRegenGroup) {
+            const int nv = std::min(kRegenGroup, nvec - g);
+            ChunkCoef<kRegenRows, kRegenGroup> Cf{};
+            for (int k = 0; k < nr; k++)
+              for (int e = 0; e < nv; e++) Cf.c[k][e] = coef_all[size_t(rowit[k]) * nvec + g + e];
+            launch_accum<VT, kRegenRows, kRegenGroup>(
+                nv, rg, s, n2, Pr, Cf, reinterpret_cast<double2 *>(V_dev) + size_t(g) * n2);
+            launches++;
+          }
+          j0 = j + 1;
+        }
+      }
+      // a full segment's last output is the next segment's first-pass start
+      for (int q = 0; q < ncol; q++) {
+        const int seg = g0 + q;
+        if (len[q] == L && seg + 1 < int(ck_cur.size())) {
+          k_count_diff<<<rg, kRedThreads, 0, s>>>(long(vbytes / 4),
+                                                   reinterpret_cast<const unsigned *>(rr[q * R + L % R]),
+                                                   reinterpret_cast<const unsigned *>(ck_cur[seg + 1]),
+                                                   d_diff + seg);
+          launches++;
+          checked[seg] = 1;
+        }
+      }
+    }
+    cudaEventRecord(tm.t3, s);
+    std::vector<unsigned long long> hd(std::max(nseg, 1), 0ull);
+    SOLVE_CUDA(cudaMemcpyAsync(hd.data(), d_diff, sizeof(unsigned long long) * hd.size(),
+                               cudaMemcpyDeviceToHost, s));
+    SOLVE_CUDA(cudaStreamSynchronize(s));
+    cudaEventElapsedTime(&ms, tm.t2, tm.t3);
+    c.stats.vectors_ms = ms;
+    c.stats.vec_segments = nseg;
+    for (int q = 0; q < nseg; q++) c.stats.vec_mismatch += checked[q] && hd[q] != 0;
+    if (kMixed) {  // double-precision Rayleigh-Ritz of the Ritz vectors
+      cudaEventRecord(tm.t2, s);
+      c.state_resid.assign(nvec, 0.0);
+      c.state_delta.assign(nvec, 0.0);
+      const long off = 0;
+      SOLVE_RC(refine_ritz(c, V_dev, nvec, n2, 1, &off, &n2, values, c.state_resid.data(),
+                           c.state_delta.data(), s));
+      cudaEventRecord(tm.t3, s);
+      SOLVE_CUDA(cudaStreamSynchronize(s));
+      cudaEventElapsedTime(&ms, tm.t2, tm.t3);
+      c.stats.refine_ms = ms;
+    }
+  } else if (V_dev && nvec > 0) {
+    // ---- eigenvector pass: the reference's second run ----------------------
+    int maxit = 0;
+    for (int k = 0; k < nvec; k++) maxit = std::max(maxit, found[k].second);
+    if (maxit > final_it) maxit = final_it;
+    const std::vector<double> &coef = coef_all;
     // chunk size limited by free memory
     size_t fre = 0, tot = 0;
     cudaMemGetInfo(&fre, &tot);
@@ -703,16 +888,16 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
     for (int it = 0; it < maxit; it++) {
       SOLVE_RC(step(it, S2, d_bet));
       if ((it + 1 - it0) == K || it == maxit - 1) {
-        ChunkPtrs<VT> P{};
+        ChunkPtrs<VT> Pr{};
         const int nk = it + 1 - it0;
         for (int k = 0; k < kMaxChunk; k++)  // rows past nk: a valid vector, zero coefficients
-          P.r[k] = ring[(it0 + (k < nk ? k : 0)) % S2];
+          Pr.r[k] = ring[(it0 + (k < nk ? k : 0)) % S2];
         for (int g = 0; g < nvec; g += kVecGroup) {
           const int nv = std::min(kVecGroup, nvec - g);
-          ChunkCoef C{};
+          ChunkCoef<> Cf{};
           for (int k = 0; k < nk; k++)
-            for (int e = 0; e < nv; e++) C.c[k][e] = coef[size_t(it0 + k) * nvec + g + e];
-          launch_accum<VT>(nv, rg, s, n2, P, C, reinterpret_cast<double2 *>(V_dev) + size_t(g) * n2);
+            for (int e = 0; e < nv; e++) Cf.c[k][e] = coef[size_t(it0 + k) * nvec + g + e];
+          launch_accum<VT>(nv, rg, s, n2, Pr, Cf, reinterpret_cast<double2 *>(V_dev) + size_t(g) * n2);
           launches++;
         }
         it0 = it + 1;

@@ -117,6 +117,17 @@ struct Ctx {
   double *d_x = nullptr, *d_y = nullptr;
   // start vector set by tbgpu_set_start_vector (used when a solve gets none)
   double *d_start = nullptr;
+  // task list of the lane-per-(atom, spin) H*x kernel (spmv_lane.cu; built on
+  // first use): lane_ntasks tasks of lane_apw atom indices (-1 padded)
+  int *d_lane_tasks = nullptr;
+  long lane_ntasks = 0;
+  int lane_apw = 0;
+  int lane_jblock = 0;   // pencils per j-block of its work order (0: 8)
+  // eigenvector pass of the Lanczos solve: 0 = the reference's second run of
+  // the recurrence from the start vector; 1 = regeneration of vec_segment-
+  // iteration segments from checkpoints saved by the first pass,
+  // vec_columns segments at a time (lane kernel products, update fused)
+  int vec_pass = 0, vec_columns = 4, vec_segment = 256;
 };
 
 // the stored Hamiltonian in its element type
@@ -194,6 +205,22 @@ int launch_spmv_async(Ctx &c, const double *x, double *y, double shift,
 int launch_spmv_async_f32(Ctx &c, const float *x, float *y, double shift,
                           const double *xscale_dev, int scale_index, double *alpha_out,
                           int alpha_index, cudaStream_t s);
+// spmv_lane.cu: lane per (atom, spin), 10-orbital models, stored blocks,
+// Gamma point (variant 5)
+// columns one regenerating pass can take: 4 complex-float or 2 complex-double
+constexpr int lane_max_cols(bool f32) { return f32 ? 4 : 2; }
+bool lane_supported(const Ctx &c);
+int launch_spmv_lane(Ctx &c, const double *x, double *y, double shift,
+                     const double *xscale_dev, int scale_index, double *alpha_out,
+                     int alpha_index, cudaStream_t s);
+int launch_spmv_lane_f32(Ctx &c, const float *x, float *y, double shift,
+                         const double *xscale_dev, int scale_index, double *alpha_out,
+                         int alpha_index, cudaStream_t s);
+// p Lanczos segments advanced by one step in one pass, the update fused:
+// y[j] = next r of the segment whose current r is x[j] at iteration it[j]
+template <typename VT>
+int launch_lane_regen(Ctx &c, int p, const VT *const *x, VT *const *y, const VT *const *rp,
+                      const int *it, const double *bet, const double *alpha, cudaStream_t s);
 // spmv_tile.cu: variant 3 (falls back to launch_spmv_async where it does not apply)
 int launch_spmv_tile(Ctx &c, const double *x, double *y, double shift,
                      const double *xscale_dev, int scale_index, double *alpha_out,

@@ -48,7 +48,8 @@ class Stats(C.Structure):
     _fields_ = [("build_ms", C.c_double), ("solve_ms", C.c_double),
                 ("vectors_ms", C.c_double), ("spmv_ms", C.c_double),
                 ("spmv_launches", C.c_long), ("lanczos_iterations", C.c_long),
-                ("kernel_launches", C.c_long), ("refine_ms", C.c_double)]
+                ("kernel_launches", C.c_long), ("refine_ms", C.c_double),
+                ("vec_segments", C.c_long), ("vec_mismatch", C.c_long)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -441,10 +442,19 @@ class Hamiltonian:
             raise TbgpuError(rc, "tbgpu_set_bloch_k")
 
     def set_spmv_variant(self, variant: int):
-        """0: warp-staged cp.async kernel (default, 10 orbitals); 1: lane-gather; 2: 2-stage."""
+        """0: warp-staged cp.async kernel (default, 10 orbitals); 1: lane-gather; 2: 2-stage;
+        3: two-cell units; 4: all cp.async; 5: lane per (atom, spin)."""
         rc = _lib().tbgpu_set_spmv_variant(self._ctx, int(variant))
         if rc:
             raise TbgpuError(rc, "tbgpu_set_spmv_variant")
+
+    def set_eigenvector_pass(self, mode: int, columns: int = 4, segment: int = 256):
+        """0: the reference's second run of the recurrence; 1: regenerate
+        ``segment``-iteration segments from first-pass checkpoints,
+        ``columns`` at a time (tbgpu_set_eigenvector_pass)."""
+        rc = _lib().tbgpu_set_eigenvector_pass(self._ctx, int(mode), int(columns), int(segment))
+        if rc:
+            raise TbgpuError(rc, "tbgpu_set_eigenvector_pass")
 
     def set_start_vector(self, r_0):
         """Keep a start vector in the context (tbgpu_set_start_vector); solves

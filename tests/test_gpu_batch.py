@@ -50,9 +50,9 @@ def test_batch_matches_dots_alone(model, fam):
                                      vectors=3, **KW)
         vb, va = res["values"][d], alone["values"]
         # alpha is formed from the unnormalised product here (<r, Hr>/beta^2),
-        # so T differs by rounding and a borderline check may pass one
-        # interval apart, accepting a value more or less
-        assert abs(res["iterations"][d] - alone["iterations"]) <= KW["ConvCheckSkipRate"]
+        # so T differs by rounding and a borderline check may pass up to two
+        # intervals apart, accepting a value more or less
+        assert abs(res["iterations"][d] - alone["iterations"]) <= 2 * KW["ConvCheckSkipRate"]
         if res["iterations"][d] == alone["iterations"]:
             assert len(vb) == len(va) >= 3
             assert np.abs(vb - va).max() < 1e-9, d

@@ -83,4 +83,7 @@ def test_batched_block_and_momentum_report_and_clear_status():
     P1, _ = d.momentum_matrix(r1["vectors"])
     P2, _ = d2.momentum_matrix(r1["vectors"])
     np.testing.assert_array_equal(P1, P2)
+    # the status word is clear: the next synchronous call reports success
+    x1 = workloads.random_start(d.n, seed=5)
+    np.testing.assert_array_equal(d.matvect_mult(x1), d2.matvect_mult(x1))
     assert L.tbgpu_last_error() == 0

@@ -234,3 +234,41 @@ def test_lanczos_sp3d5s_so_dome_matches_oracle():
                     tol=1e-7)
     assert len(res["values"]) == len(ref["evals"]) >= 2
     assert np.abs(np.sort(res["values"]) - np.sort(ref["evals"])).max() < 1e-6
+
+
+def test_cfg1_eigenvalues_nearest_sigma():
+    """The CPU-runnable case as stated: GaAs cube of 8x8x8 cells (4096 atoms),
+    sp3s*, +30 eV passivation, start vector uniform in [-1, 1] from seed 0,
+    the 8 eigenvalues nearest sigma = 1.6 eV.  Windows (sigma - 0.33, sigma]
+    and (sigma, sigma + 0.33] with 8 requested in each run the solve to its
+    iteration limit (the first window lies in the gap).  The 8 nearest
+    eigenvalues with multiplicity come from LAPACK on the oracle's dense H
+    (tests/golden/cfg1_dense.npz); single-vector Lanczos returns each
+    degenerate level once, so the bar is: every distinct level among those 8
+    is found, within 1e-6 eV, every value found is a dense eigenvalue
+    within 1e-6 eV, and the GPU set equals the oracle's run."""
+    import os
+    sigma = 1.6
+    dense = np.load(os.path.join(os.path.dirname(__file__), "golden", "cfg1_dense.npz"))
+    w = dense["eigenvalues"]
+    near8 = w[np.argsort(np.abs(w - sigma), kind="stable")[:8]]
+    st = workloads.gaas_cube(8)
+    g, o = pair(st, "sp3s*")
+    assert g.natoms == int(dense["natoms"]) == 4096
+    kw = dict(requested1=8, requested2=8, emin1=sigma - 0.33, emax1=sigma, emin2=sigma,
+              emax2=sigma + 0.33, tolerance=1e-7, imax=6000, ConvCheckStartIter=200,
+              ConvCheckSkipRate=50)
+    r0 = workloads.random_start(g.n, seed=0)
+    res = g.eigensolve_lanczos(r0, **kw)
+    found = np.sort(res["values"])
+    for lev in np.unique(np.round(near8, 9)):
+        assert np.abs(found - lev).min() < 1e-6, (lev, found)
+    for v in found:
+        assert np.abs(w - v).min() < 1e-6, v
+    ref = o.lanczos(r0, imax=kw["imax"], req=(8, 8), erange1=(kw["emin1"], kw["emax1"]),
+                    erange2=(kw["emin2"], kw["emax2"]), tol=1e-7, conv_start=200, conv_skip=50)
+    assert len(found) == len(ref["evals"])
+    assert np.abs(found - np.sort(ref["evals"])).max() < 1e-6
+    nearest = found[np.argsort(np.abs(found - sigma))[:8]]
+    print("8 nearest distinct levels found:", np.round(np.sort(nearest), 9),
+          "iterations", res["iterations"])

@@ -53,3 +53,16 @@ def test_si_bulk_lanczos_sets(golden, chunk):
         want = np.unique(ref[ref[:, 0] == kx, 3])
         assert len(got) == len(want), (kx, got, want)
         assert np.abs(got - want).max() < 1e-6, (kx, got, want)
+
+
+def test_cfg1_dense_fixture_shape():
+    """The dense fixture of the 4096-atom cube: sorted eigenvalues in the gap
+    region's window, the conduction-band edge first (no level between 1.0 eV
+    and it), and the multiplicities of the cube's symmetric states."""
+    import os
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "cfg1_dense.npz"))
+    w = d["eigenvalues"]
+    assert int(d["natoms"]) == 4096
+    assert np.all(np.diff(w) >= 0) and w[0] > 1.6 and w[-1] < 2.0
+    assert abs(w[0] - 1.66814453) < 1e-7          # the conduction-band edge of the cube
+    assert abs(w[1] - w[2]) < 1e-9                 # a doubly degenerate level next
