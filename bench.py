@@ -488,9 +488,12 @@ def run_extra(args):
                 ("fp64 store, two-cell units (variant 3)", {}, False, 3),
                 ("fp64 store, every piece by cp.async (variant 4)", {}, False, 4),
                 ("fp64 store, lane per atom and spin (variant 5)", {}, False, 5),
+                ("fp64 store, pencil layout (variant 6)", {}, False, 6),
                 ("float store, float vectors", dict(ham_bits=32, lanczos_bits=32), True, 0),
                 ("float store, float vectors, lane per atom and spin (variant 5)",
                  dict(ham_bits=32, lanczos_bits=32), True, 5),
+                ("float store, float vectors, pencil layout (variant 6)",
+                 dict(ham_bits=32, lanczos_bits=32), True, 6),
                 ("recompute fp64", dict(recompute=True), False, 0),
                 ("recompute float", dict(recompute=True, lanczos_bits=32), True, 0)):
             H = tbgpu.Hamiltonian(st, "sp3d5s*_so", MATS, **opts)
@@ -505,8 +508,21 @@ def run_extra(args):
                 f = (lambda: H.hx_dev_f32(x.data_ptr(), y.data_ptr())) if f32 else \
                     (lambda: H.hx_dev(x.data_ptr(), y.data_ptr()))
                 ms = _event_time(f, 20, stream)
+            # inside the Lanczos recurrence: the product with the fused alpha on
+            # the solver's own vectors (the pencil layout for variant 6), CUDA
+            # events around every launch of a 60-iteration run without checks
+            r0 = torch.from_numpy(workloads.random_start(H.n, seed=0)).cuda()
+            H.set_profiling(True)
+            H.eigensolve_lanczos_dev(r0.data_ptr(), 0, 0, imax=61, requested1=1, requested2=1,
+                                     ConvCheckStartIter=10 ** 9)
+            stt = H.stats()
+            ms_solve = stt["spmv_ms"] / max(stt["spmv_launches"], 1)
+            bpa = 1256 if f32 else 2504
             print(json.dumps({"workload": "kernels", "metric": "H*x ms per launch", "variant": name,
-                              "natoms": H.natoms, "value": ms, "unit": "ms"}), flush=True)
+                              "natoms": H.natoms, "value": ms, "unit": "ms",
+                              "in_solve_ms": ms_solve,
+                              "in_solve_frac_of_peak": bpa * H.natoms / (ms_solve * 1e-3) / 1e9
+                              / peaks()[0]["hbm_gbs"]}), flush=True)
             H.close()
     elif w == "mixed2M":
         st = workloads.dome_in_box(cells=(72, 72, 48), base_nm=20.0, height_nm=5.0,
@@ -515,16 +531,17 @@ def run_extra(args):
         f32 = dict(ham_bits=32, lanczos_bits=32)
         # (name, options, H*x variant, eigenvector pass (mode, columns,
         # segment) or None, tolerance)
-        variants = [("fp64", {}, 0, None, 1e-7),
-                    ("mixed, float store", f32, 0, None, 1e-7),
-                    ("mixed, float store, lane kernel", f32, 5, None, 1e-7),
-                    ("mixed, float store, regenerated vectors P=4 L=256", f32, 5, (1, 4, 256), 1e-7),
-                    ("mixed, float store, regenerated vectors P=2 L=256", f32, 5, (1, 2, 256), 1e-7),
-                    ("mixed, float store, regenerated vectors P=4 L=256, tol 1e-6", f32, 5,
-                     (1, 4, 256), 1e-6),
-                    ("mixed, float store, regenerated vectors P=4 L=256, tol 1e-5", f32, 5,
-                     (1, 4, 256), 1e-5),
-                    ("fp64, regenerated vectors P=2 L=256", {}, 5, (1, 2, 256), 1e-7)]
+        variants = [("fp64 (warp-staged kernel, second run for the vectors)", {}, 0, None, 1e-7),
+                    ("fp64, pencil kernel", {}, 6, None, 1e-7),
+                    ("fp64, pencil kernel, regenerated vectors P=2 L=256", {}, 6, (1, 2, 256),
+                     1e-7),
+                    ("mixed, float store, warp-staged kernel", f32, 0, None, 1e-7),
+                    ("mixed, float store, lane kernel, regenerated vectors P=4 L=256", f32, 5,
+                     (1, 4, 256), 1e-7),
+                    ("mixed, float store, pencil kernel, regenerated vectors P=4 L=256", f32, 6,
+                     (1, 4, 256), 1e-7),
+                    ("mixed, float store, pencil kernel, regenerated vectors P=4 L=128", f32, 6,
+                     (1, 4, 128), 1e-7)]
         if args.mixed_recompute:
             variants.append(("mixed, recompute", dict(recompute=True, lanczos_bits=32), 0, None,
                              1e-7))
@@ -731,7 +748,7 @@ def main():
                     help="with --profile-case: a converging solve with the eigenvector pass")
     ap.add_argument("--profile-vff", action="store_true",
                     help="with --profile-case: a few Keating VFF iterations instead")
-    ap.add_argument("--spmv-variant", type=int, default=0, choices=[0, 1, 2, 3, 4, 5],
+    ap.add_argument("--spmv-variant", type=int, default=0, choices=[0, 1, 2, 3, 4, 5, 6],
                     help="H*x kernel of the solve (tbgpu_set_spmv_variant)")
     ap.add_argument("--mixed-recompute", action="store_true",
                     help="--workload mixed2M: also the mixed solve on the recompute product")

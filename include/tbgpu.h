@@ -326,14 +326,18 @@ int tbgpu_hx_dot_noalloc(tbgpu_ctx *ctx, double shift, const double *x_dev,
  * point, else as 0), 4 = the default kernel with every piece, the cation
  * block runs included, by 16-byte cp.async, 5 = one lane per (atom, spin)
  * with block rows loaded straight to registers (10-orbital models with a
- * stored Hamiltonian at the Gamma point, else as 0).  Variants 0, 2, 3 and
- * 4 give the same y bit for bit; 1 and 5 sum in their own orders (equal to
- * rounding). */
+ * stored Hamiltonian at the Gamma point, else as 0), 6 = the same lane
+ * mapping on a pencil-interleaved copy of the Hamiltonian (every quantity
+ * stored with the k index of its cell fastest, so a warp's loads are
+ * contiguous; the solves keep their Lanczos vectors in that layout, these
+ * products permute the caller's vectors around the kernel; Gamma point, not
+ * in batched solves, else as 0).  Variants 0, 2, 3 and 4 give the same y bit
+ * for bit; 1, 5 and 6 sum in their own orders (equal to rounding). */
 int tbgpu_set_spmv_variant(tbgpu_ctx *ctx, int variant);
 
 /* Autotuner: times the H*x variants that are distinct kernels for the built
- * context (all six for the 10-orbital models with the 64-bit store at the
- * Gamma point, 0, 1 and 5 with the 32-bit store, only 0 for 5-orbital models,
+ * context (all seven for the 10-orbital models with the 64-bit store at the
+ * Gamma point, 0, 1, 5 and 6 with the 32-bit store, only 0 for 5-orbital models,
  * Bloch phases and recompute storage), reps launches each with the fused
  * Lanczos dot after two untimed ones (CUDA events on the context stream;
  * two temporary device vectors), selects the fastest (ties: the lower
@@ -483,8 +487,8 @@ int tbgpu_set_profiling(tbgpu_ctx *ctx, int on);
  * with a stored Hamiltonian at the Gamma point; columns 1..4 for the
  * mixed-precision solve, 1..2 for double vectors), with the three-term
  * update fused into the product.  Every product of both passes then uses the
- * lane-per-(atom, spin) kernel (H*x variant 5), whose columns compute
- * exactly as a one-column launch: the regenerated vectors equal the first
+ * lane-per-(atom, spin) kernel (H*x variant 5), or the pencil kernel when
+ * variant 6 is set, whose columns compute exactly as a one-column launch: the regenerated vectors equal the first
  * pass's bit for bit (checked at every segment end, tbgpu_stats.vec_mismatch),
  * so the eigenvalues are those of mode 0 and the eigenvectors differ only by
  * the order of the accumulation.  Where the mode does not apply, or the

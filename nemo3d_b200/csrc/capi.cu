@@ -44,7 +44,8 @@ static void free_ctx(Ctx *c) {
                   c->d_nbr, c->d_site_m, c->d_surface, c->d_onsite, c->d_blocks, c->d_partial,
                   c->d_counter, c->d_status, c->d_x, c->d_y, c->d_phase, c->d_groups,
                   c->d_blocks32, c->d_onsite32, c->d_rc_order, c->d_units, c->d_start,
-                  c->d_lane_tasks};
+                  c->d_lane_tasks, c->d_pen_blk, c->d_pen_ons, c->d_pen_ok,
+                  c->d_pen_scratch};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -444,16 +445,16 @@ int tbgpu_export_hamiltonian(const tbgpu_ctx *ctx, double *onsite, double *block
 }
 
 int tbgpu_set_spmv_variant(tbgpu_ctx *ctx, int variant) {
-  if (!ctx || variant < 0 || variant > 5) return set_error(TBGPU_E_ARG);
+  if (!ctx || variant < 0 || variant > 6) return set_error(TBGPU_E_ARG);
   C(ctx)->spmv_variant = variant;
   return TBGPU_OK;
 }
 
-// The variants that launch distinct kernels for this context: all six for
+// The variants that launch distinct kernels for this context: all seven for
 // the 10-orbital models with the double store at the Gamma point; the
-// warp-staged, the lane-gather and the lane-per-(atom, spin) kernel with the
-// float store; one kernel otherwise (5-orbital models, Bloch phases,
-// recompute storage).
+// warp-staged, the lane-gather, the lane-per-(atom, spin) and the pencil
+// kernel with the float store; one kernel otherwise (5-orbital models, Bloch
+// phases, recompute storage).
 static int distinct_variants(const Ctx &c, int *v) {
   if (c.norb != 10 || c.bloch || c.recompute) {
     v[0] = 0;
@@ -463,10 +464,11 @@ static int distinct_variants(const Ctx &c, int *v) {
     v[0] = 0;
     v[1] = 1;
     v[2] = 5;
-    return 3;
+    v[3] = 6;
+    return 4;
   }
-  for (int i = 0; i < 6; i++) v[i] = i;
-  return 6;
+  for (int i = 0; i < 7; i++) v[i] = i;
+  return 7;
 }
 
 // Times the context's distinct H*x variants (the product with the fused
@@ -492,7 +494,7 @@ int tbgpu_autotune_spmv(tbgpu_ctx *ctx, int reps, int *variant_out, double *ms_o
              cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
     rc = TBGPU_E_CUDA;
   }
-  int cand[6];
+  int cand[7];
   const int ncand = distinct_variants(c, cand);
   for (int ci = 0; ci < ncand && rc == TBGPU_OK; ci++) {
     const int v = cand[ci];

@@ -476,7 +476,20 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
   c.stats.refine_ms = 0.0;
   c.stats.vec_segments = 0;
   c.stats.vec_mismatch = 0;
-  const long n2 = c.natoms * c.nb;  // complex entries
+  // eigenvector pass by regeneration (tbgpu_set_eigenvector_pass): both
+  // passes run a register-streaming kernel whose columns compute as
+  // one-column launches -- the pencil kernel when variant 6 is set and
+  // applies, else the lane kernel (variant 5)
+  const bool f32_ok = !kMixed || c.ham_fp32;
+  bool regen = c.vec_pass == 1 && V_dev && maxvec > 0 && lane_supported(c) && f32_ok;
+  const int keep_variant = c.spmv_variant;
+  if (regen) c.spmv_variant = pen_supported(c) && keep_variant == 6 ? 6 : 5;
+  // the pencil kernel keeps the Lanczos vectors in its own layout: the start
+  // vector is permuted in and the eigenvectors out
+  const bool pen = c.spmv_variant == 6 && pen_supported(c) && f32_ok;
+  if (!pen && c.spmv_variant == 6) c.spmv_variant = regen ? 5 : 0;
+  const long n2_ref = c.natoms * c.nb;           // complex entries, reference order
+  const long n2 = pen ? pen_length(c) : n2_ref;  // of the solver's vectors
   const size_t vbytes = sizeof(VT) * n2;        // one Lanczos vector
   const size_t ebytes = sizeof(double2) * n2;   // one eigenvector (always double)
   cudaStream_t s = c.stream;
@@ -494,17 +507,14 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
   double *d_alpha = nullptr, *d_bet = nullptr, *d_tmp = nullptr;
   double *h_alpha = nullptr, *h_bet = nullptr;
   std::vector<cudaEvent_t> spmv_ev;
-  // eigenvector pass by regeneration (tbgpu_set_eigenvector_pass): the
-  // first pass saves r_it and r_{it-1} at every it = 0, L, 2L, ..., and both
-  // passes run the lane kernel, whose columns compute as one-column launches
-  bool regen = c.vec_pass == 1 && V_dev && maxvec > 0 && lane_supported(c) &&
-               (!kMixed || c.ham_fp32);
-  const int keep_variant = c.spmv_variant;
-  if (regen) c.spmv_variant = 5;
+  // regeneration: the first pass saves r_it and r_{it-1} at every it = 0,
+  // L, 2L, ...
   const int L = std::max(c.vec_segment, 16);
   const int P = std::max(1, std::min(c.vec_columns, lane_max_cols(kMixed)));
   std::vector<VT *> ck_cur, ck_prev, rr;  // checkpoints; the pass-2 rings
   unsigned long long *d_diff = nullptr;
+  double *r0_pen = nullptr;  // pencil layout: the start vector
+  double *V_pen = nullptr;   // ... and the eigenvectors before they go out
   auto drop_checkpoints = [&]() {
     for (VT *q : ck_cur) if (q) cudaFreeAsync(q, s);
     for (VT *q : ck_prev) if (q) cudaFreeAsync(q, s);
@@ -518,6 +528,10 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
     rr.clear();
     if (d_diff) cudaFreeAsync(d_diff, s);
     d_diff = nullptr;
+    if (r0_pen) cudaFreeAsync(r0_pen, s);
+    r0_pen = nullptr;
+    if (V_pen) cudaFreeAsync(V_pen, s);
+    V_pen = nullptr;
     for (int i = 0; i <= kMaxChunk; i++)
       if (ring[i]) cudaFree(ring[i]);
     if (W) cudaFree(W);
@@ -556,6 +570,12 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
   cudaEventCreate(&tm.t2);
   cudaEventCreate(&tm.t3);
 
+  if (pen) {
+    SOLVE_CUDA(cudaMallocAsync(&r0_pen, ebytes, s));
+    SOLVE_RC(pen_permute<double2>(c, reinterpret_cast<const double2 *>(r0_dev),
+                                  reinterpret_cast<double2 *>(r0_pen), true, s));
+    r0_dev = r0_pen;
+  }
   // start vector: r = r0 / ||r0||; bet[0] = ||r||
   auto start = [&](double *bet) -> int {
     k_norm<double2><<<rg, kRedThreads, 0, s>>>(n2, reinterpret_cast<const double2 *>(r0_dev),
@@ -575,7 +595,8 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
       cudaEventCreate(&e1);
       cudaEventRecord(e0, s);
     }
-    int r_ = spmv_step(c, rc_, W, bet, it, d_alpha, s);
+    int r_ = pen ? launch_spmv_pen_internal<VT>(c, rc_, W, 0.0, bet, it, d_alpha, it, s)
+                 : spmv_step(c, rc_, W, bet, it, d_alpha, s);
     if (r_) return r_;
     if (c.profiling) {
       cudaEventRecord(e1, s);
@@ -743,6 +764,27 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
 
   // ---- second pass: eigenvectors -------------------------------------------
   const int nvec = std::min(ne, std::max(maxvec, 0));
+  // the eigenvectors accumulate in the solver's layout (Vacc) and, in the
+  // pencil layout, are permuted into V_dev at the end
+  double *Vacc = V_dev;
+  auto vec_target = [&]() -> int {
+    if (pen) {
+      if (cudaMallocAsync(&V_pen, ebytes * nvec, s) != cudaSuccess) return set_error(TBGPU_E_NOMEM);
+      Vacc = V_pen;
+    }
+    return cudaMemsetAsync(Vacc, 0, ebytes * nvec, s) == cudaSuccess ? TBGPU_OK
+                                                                    : set_error(TBGPU_E_CUDA);
+  };
+  auto vec_out = [&]() -> int {
+    if (!pen) return TBGPU_OK;
+    for (int e = 0; e < nvec; e++) {
+      int r_ = pen_permute<double2>(c, reinterpret_cast<const double2 *>(V_pen) + size_t(e) * n2,
+                                    reinterpret_cast<double2 *>(V_dev) + size_t(e) * n2_ref,
+                                    false, s);
+      if (r_) return r_;
+    }
+    return TBGPU_OK;
+  };
   std::vector<double> coef_all;
   if (!V_dev || nvec <= 0) drop_checkpoints();
   if (V_dev && nvec > 0) {
@@ -780,7 +822,7 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
     for (auto &q : rr) SOLVE_CUDA(cudaMallocAsync(&q, vbytes, s));
     SOLVE_CUDA(cudaMallocAsync(&d_diff, sizeof(unsigned long long) * std::max(nseg, 1), s));
     SOLVE_CUDA(cudaMemsetAsync(d_diff, 0, sizeof(unsigned long long) * std::max(nseg, 1), s));
-    SOLVE_CUDA(cudaMemsetAsync(V_dev, 0, ebytes * nvec, s));
+    SOLVE_RC(vec_target());
     cudaEventRecord(tm.t2, s);
     std::vector<char> checked(nseg, 0);
     for (int g0 = 0; g0 < nseg; g0 += P) {
@@ -810,7 +852,8 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
           ys[q] = rr[q * R + (j + 1) % R];
           its[q] = seg * L + j;
         }
-        SOLVE_RC(launch_lane_regen<VT>(c, na, xs, ys, rps, its, d_bet, d_alpha, s));
+        SOLVE_RC(pen ? launch_pen_regen<VT>(c, na, xs, ys, rps, its, d_bet, d_alpha, s)
+                     : launch_lane_regen<VT>(c, na, xs, ys, rps, its, d_bet, d_alpha, s));
         launches++;
         if (j + 1 - j0 == K || j == steps - 1) {  // accumulate the columns' inputs j0..j
           ChunkPtrs<VT, kRegenRows> Pr{};
@@ -828,7 +871,7 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
             for (int k = 0; k < nr; k++)
               for (int e = 0; e < nv; e++) Cf.c[k][e] = coef_all[size_t(rowit[k]) * nvec + g + e];
             launch_accum<VT, kRegenRows, kRegenGroup>(
-                nv, rg, s, n2, Pr, Cf, reinterpret_cast<double2 *>(V_dev) + size_t(g) * n2);
+                nv, rg, s, n2, Pr, Cf, reinterpret_cast<double2 *>(Vacc) + size_t(g) * n2);
             launches++;
           }
           j0 = j + 1;
@@ -856,12 +899,13 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
     c.stats.vectors_ms = ms;
     c.stats.vec_segments = nseg;
     for (int q = 0; q < nseg; q++) c.stats.vec_mismatch += checked[q] && hd[q] != 0;
+    SOLVE_RC(vec_out());
     if (kMixed) {  // double-precision Rayleigh-Ritz of the Ritz vectors
       cudaEventRecord(tm.t2, s);
       c.state_resid.assign(nvec, 0.0);
       c.state_delta.assign(nvec, 0.0);
       const long off = 0;
-      SOLVE_RC(refine_ritz(c, V_dev, nvec, n2, 1, &off, &n2, values, c.state_resid.data(),
+      SOLVE_RC(refine_ritz(c, V_dev, nvec, n2_ref, 1, &off, &n2_ref, values, c.state_resid.data(),
                            c.state_delta.data(), s));
       cudaEventRecord(tm.t3, s);
       SOLVE_CUDA(cudaStreamSynchronize(s));
@@ -881,7 +925,7 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
     while (K > 2 && size_t(K + 1 - S1) * vbytes + (256ull << 20) > fre) K /= 2;
     const int S2 = K + 1;
     for (int i = S1; i < S2; i++) SOLVE_CUDA(cudaMalloc(&ring[i], vbytes));
-    SOLVE_CUDA(cudaMemsetAsync(V_dev, 0, ebytes * nvec, s));
+    SOLVE_RC(vec_target());
     cudaEventRecord(tm.t2, s);
     SOLVE_RC(start(d_bet));
     int it0 = 0;
@@ -897,7 +941,7 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
           ChunkCoef<> Cf{};
           for (int k = 0; k < nk; k++)
             for (int e = 0; e < nv; e++) Cf.c[k][e] = coef[size_t(it0 + k) * nvec + g + e];
-          launch_accum<VT>(nv, rg, s, n2, Pr, Cf, reinterpret_cast<double2 *>(V_dev) + size_t(g) * n2);
+          launch_accum<VT>(nv, rg, s, n2, Pr, Cf, reinterpret_cast<double2 *>(Vacc) + size_t(g) * n2);
           launches++;
         }
         it0 = it + 1;
@@ -907,12 +951,13 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
     SOLVE_CUDA(cudaStreamSynchronize(s));
     cudaEventElapsedTime(&ms, tm.t2, tm.t3);
     c.stats.vectors_ms = ms;
+    SOLVE_RC(vec_out());
     if (kMixed) {  // double-precision Rayleigh-Ritz of the Ritz vectors
       cudaEventRecord(tm.t2, s);
       c.state_resid.assign(nvec, 0.0);
       c.state_delta.assign(nvec, 0.0);
       const long off = 0;
-      SOLVE_RC(refine_ritz(c, V_dev, nvec, n2, 1, &off, &n2, values, c.state_resid.data(),
+      SOLVE_RC(refine_ritz(c, V_dev, nvec, n2_ref, 1, &off, &n2_ref, values, c.state_resid.data(),
                            c.state_delta.data(), s));
       cudaEventRecord(tm.t3, s);
       SOLVE_CUDA(cudaStreamSynchronize(s));

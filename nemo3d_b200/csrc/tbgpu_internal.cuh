@@ -123,6 +123,14 @@ struct Ctx {
   long lane_ntasks = 0;
   int lane_apw = 0;
   int lane_jblock = 0;   // pencils per j-block of its work order (0: 8)
+  // the pencil layout of the stored Hamiltonian (spmv_pen.cu; built on first
+  // use): bond blocks as column pairs, on-site records, site mask; scratch
+  // for products on vectors in the reference's order
+  void *d_pen_blk = nullptr, *d_pen_ons = nullptr;
+  unsigned char *d_pen_ok = nullptr;
+  bool pen_fp32 = false;
+  void *d_pen_scratch = nullptr;
+  size_t pen_scratch_bytes = 0;
   // eigenvector pass of the Lanczos solve: 0 = the reference's second run of
   // the recurrence from the start vector; 1 = regeneration of vec_segment-
   // iteration segments from checkpoints saved by the first pass,
@@ -221,6 +229,25 @@ int launch_spmv_lane_f32(Ctx &c, const float *x, float *y, double shift,
 template <typename VT>
 int launch_lane_regen(Ctx &c, int p, const VT *const *x, VT *const *y, const VT *const *rp,
                       const int *it, const double *bet, const double *alpha, cudaStream_t s);
+// spmv_pen.cu: pencil-interleaved layout (variant 6), 10-orbital models,
+// stored blocks, Gamma point, no skip mask
+bool pen_supported(const Ctx &c);
+long pen_length(const Ctx &c);  // complex entries of a pencil-layout vector
+int launch_spmv_pen(Ctx &c, const double *x, double *y, double shift, const double *xscale_dev,
+                    int scale_index, double *alpha_out, int alpha_index, cudaStream_t s);
+int launch_spmv_pen_f32(Ctx &c, const float *x, float *y, double shift,
+                        const double *xscale_dev, int scale_index, double *alpha_out,
+                        int alpha_index, cudaStream_t s);
+// on vectors already in the pencil layout (the solver's)
+template <typename VT>
+int launch_spmv_pen_internal(Ctx &c, const VT *x, VT *y, double shift, const double *xnorm,
+                             int xidx, double *alpha_out, int aidx, cudaStream_t s);
+// reference order <-> pencil layout (to_pen: out is zeroed first)
+template <typename VT>
+int pen_permute(Ctx &c, const VT *in, VT *out, bool to_pen, cudaStream_t s);
+template <typename VT>
+int launch_pen_regen(Ctx &c, int p, const VT *const *x, VT *const *y, const VT *const *rp,
+                     const int *it, const double *bet, const double *alpha, cudaStream_t s);
 // spmv_tile.cu: variant 3 (falls back to launch_spmv_async where it does not apply)
 int launch_spmv_tile(Ctx &c, const double *x, double *y, double shift,
                      const double *xscale_dev, int scale_index, double *alpha_out,

@@ -7,7 +7,7 @@ Bars:
   float-rounded entries to the same bar; with float vectors, against the
   warp-staged float kernel to float rounding (5e-6 of max |y|);
 * the same at the bench's full size (1,022,656 atoms), default kernel and
-  variant 5;
+  variants 5 and 6;
 * Lanczos on variant 5: the oracle's eigenvalue set within 1e-6 eV;
 * eigenvector pass by regeneration (tbgpu_set_eigenvector_pass(1)): every
   regenerated segment end equal, bit for bit, to the first pass's checkpoint
@@ -91,7 +91,7 @@ def test_lane_float_vectors():
 def test_full_size_hx_matches_oracle():
     """The bench's own dot: 58 x 58 x 38 cells, 1,022,656 atoms, sp3d5s*+SO,
     displaced positions, passivated surface; the default kernel and
-    variant 5, the shift of the bench's band gap."""
+    variants 5 and 6, the shift of the bench's band gap."""
     from nemo3d_b200.tbgpu import Hamiltonian
     mats = [materials.MATERIALS[m] for m in SPDS]
     st = workloads.dome_in_box(cells=(58, 58, 38), base_nm=20.0, height_nm=5.0,
@@ -101,7 +101,7 @@ def test_full_size_hx_matches_oracle():
     o = oracle.OracleHamiltonian(st, 10, 2, mats)
     x = workloads.random_start(g.n, seed=0)
     yo = o.hx(x, 1.25)
-    for variant in (0, 5):
+    for variant in (0, 5, 6):
         g.set_spmv_variant(variant)
         y = g.matvect_mult(x, 1.25)
         err = np.abs(y - yo).max() / np.abs(yo).max()
@@ -141,6 +141,7 @@ def test_regenerated_eigenvectors_double(columns, segment):
     r0 = r0[:2 * g0.n]
     a = g0.eigensolve_lanczos(r0, vectors=4, **KW)
     g1 = Hamiltonian(st, "sp3d5s*_so", mats)
+    g1.set_spmv_variant(5)
     g1.set_eigenvector_pass(1, columns, segment)
     b = g1.eigensolve_lanczos(r0, vectors=4, **KW)
     s1 = g1.stats()
@@ -164,6 +165,7 @@ def test_regenerated_eigenvectors_mixed():
     r0 = workloads.random_start(g0.n, seed=0)
     a = g0.eigensolve_lanczos(r0, vectors=4, **KW)
     g1 = Hamiltonian(st, "sp3d5s*_so", mats, ham_bits=32, lanczos_bits=32)
+    g1.set_spmv_variant(5)
     g1.set_eigenvector_pass(1, 4, 64)
     b = g1.eigensolve_lanczos(r0, vectors=4, **KW)
     s1 = g1.stats()
