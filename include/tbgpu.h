@@ -285,6 +285,35 @@ int tbgpu_eigensolve_blk_lanczos_dev(tbgpu_ctx *ctx, int ConvCheckStartIter,
 int tbgpu_get_tridiagonal(const tbgpu_ctx *ctx, double *alpha, double *beta,
                           int cap);
 
+/* The saved state of eigensolve_lanczos (eigen/src/lanczos.c:1692-1809):
+ * tridiagonal matrix file (int iterations, int processors, double
+ * t[2*iterations], t[2i] = alpha_i, t[2i-1] = beta_{i-1}) and eigenvalue file
+ * (int n, double value[n]), native endian.  Reading a matrix file keeps
+ * iterations - 200 of what is stored, as the reference's
+ * restoreTridiagonalMatrix does (lanczos.c:1765), and returns that count
+ * (alpha[i], beta[i] for i < min(count, cap); beta couples i and i+1).
+ * Reading an eigenvalue file returns n.  Host only; TBGPU_E_ARG when a file
+ * cannot be opened or is short. */
+int tbgpu_write_tridiagonal_file(const char *path, const double *alpha, const double *beta,
+                                 int iterations, int processors);
+int tbgpu_read_tridiagonal_file(const char *path, int cap, double *alpha, double *beta,
+                                int *processors);
+int tbgpu_write_eigenvalue_file(const char *path, const double *values, int n);
+int tbgpu_read_eigenvalue_file(const char *path, int cap, double *values);
+
+/* Eigenvectors of nvalues eigenvalues from a given tridiagonal matrix of
+ * `iterations` Lanczos steps (alpha[iterations], beta[iterations - 1]) and
+ * the start vector r_0 it was built from -- the restoreState path of
+ * eigensolve_lanczos (lanczos.c:1912-1955, 2022-2057): no first pass, the
+ * recurrence is rerun from r_0 for `iterations` steps and every value's Ritz
+ * vector uses the whole matrix.  Values are taken in ascending order;
+ * min(nvalues, max_vectors) vectors (host, complex) are written and that
+ * count returned. */
+int tbgpu_eigenvectors_from_tridiagonal(tbgpu_ctx *ctx, int iterations, const double *alpha,
+                                        const double *beta, int nvalues, const double *values,
+                                        const tbgpu_dcomplex *r_0, tbgpu_dcomplex *vectors,
+                                        int max_vectors);
+
 /* Export for parity tests (tbgpu_export_pattern mirrors the topology of
  * get_total_hamiltonian_dimension_and_offsets / remove_few_bonded_atoms /
  * FindSurfaceAtoms): atom_site[n_atoms] site index of each atom,
@@ -476,6 +505,31 @@ typedef struct {
                               /* from the first pass's checkpoint (0 expected) */
 } tbgpu_stats;
 int tbgpu_set_profiling(tbgpu_ctx *ctx, int on);
+
+/* Folded-spectrum operator F = factor * (H - shift2)(H - shift1) + offset,
+ * the reference's matvect_mult2 (nemo3d/src/base/h_cvectr_mult.c:156-198,
+ * whose constants 1.38, 1.58, -10, 0 are the defaults here): eigenvalues of H
+ * nearest (shift1 + shift2) / 2 become the largest of F when factor < 0.
+ * tbgpu_set_fold(ctx, 1, ...) makes the Lanczos solves
+ * (tbgpu_eigensolve_lanczos(_dev)) run on F: two products and one combining
+ * pass per step (which also reduces alpha), the windows and the returned
+ * values are those of F (as with the reference's driver on matvect_mult2),
+ * the eigenvectors come from the second run of the recurrence, and
+ * tbgpu_get_fold_energies returns <v, H v> / <v, v> of each returned
+ * eigenvector (the energies of H).  Double precision only (a mixed-precision
+ * context returns TBGPU_E_UNSUPPORTED).  0 turns it off.  Each product reads
+ * H once, so F costs two reads of H per application. */
+int tbgpu_set_fold(tbgpu_ctx *ctx, int on, double shift1, double shift2, double factor,
+                   double offset);
+/* Drop-in for the reference's matvect_mult2 (h_cvectr_mult.c:156): the
+ * matmul signature, y = F x over host vectors (argList[1] is ignored, as
+ * there).  Failures through tbgpu_last_error(). */
+void tbgpu_matvect_mult2(const int **argList, tbgpu_dcomplex *y, const tbgpu_dcomplex *x);
+/* y = F x on device vectors (16-byte aligned, distinct); asynchronous. */
+int tbgpu_hx_fold_dev(tbgpu_ctx *ctx, const double *x_dev, double *y_dev);
+/* <v, H v> / <v, v> of the eigenvectors of the last folded solve; returns
+ * their count (writes at most cap). */
+int tbgpu_get_fold_energies(const tbgpu_ctx *ctx, int cap, double *energies);
 
 /* Eigenvector pass of the Lanczos solves (no counterpart in the reference,
  * whose eigenvectorsLanczos reruns the whole recurrence from the start

@@ -1,5 +1,6 @@
 // C ABI entry points of libtbgpu.so (declared in include/tbgpu.h).
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -45,7 +46,7 @@ static void free_ctx(Ctx *c) {
                   c->d_counter, c->d_status, c->d_x, c->d_y, c->d_phase, c->d_groups,
                   c->d_blocks32, c->d_onsite32, c->d_rc_order, c->d_units, c->d_start,
                   c->d_lane_tasks, c->d_pen_blk, c->d_pen_ons, c->d_pen_ok,
-                  c->d_pen_scratch};
+                  c->d_pen_scratch, c->d_fold_tmp};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -359,6 +360,50 @@ int tbgpu_eigensolve_lanczos(tbgpu_ctx *ctx, int ConvCheckStartIter, int ConvChe
   return ne;
 }
 
+int tbgpu_eigenvectors_from_tridiagonal(tbgpu_ctx *ctx, int iterations, const double *alpha,
+                                        const double *beta, int nvalues, const double *values,
+                                        const tbgpu_dcomplex *r_0, tbgpu_dcomplex *vectors,
+                                        int max_vectors) {
+  if (!ctx || iterations < 2 || !alpha || !beta || nvalues < 1 || !values || !r_0 || !vectors ||
+      max_vectors < 1)
+    return set_error(TBGPU_E_ARG);
+  Ctx &c = *C(ctx);
+  if (!c.built) return set_error(TBGPU_E_STATE);
+  const size_t bytes = sizeof(double) * 2 * size_t(c.natoms) * c.nb;
+  const int nv = nvalues < max_vectors ? nvalues : max_vectors;
+  double *r0 = nullptr, *V = nullptr;
+  if (cudaMalloc(&r0, bytes) != cudaSuccess) return set_error(TBGPU_E_NOMEM);
+  if (cudaMalloc(&V, bytes * nv) != cudaSuccess) {
+    cudaFree(r0);
+    return set_error(TBGPU_E_NOMEM);
+  }
+  int rc = cudaMemcpyAsync(r0, r_0, bytes, cudaMemcpyHostToDevice, c.stream) == cudaSuccess
+               ? TBGPU_OK
+               : set_error(TBGPU_E_CUDA);
+  std::vector<double> vals(values, values + nvalues), out(nvalues);
+  std::sort(vals.begin(), vals.end());
+  if (rc == TBGPU_OK) {
+    SolveArgs A{0, 1, iterations + 1, 0, 0, 0.0, 0.0, 0.0, 0.0, 1e-7};
+    A.restore_its = iterations;
+    A.restore_n = nvalues;
+    A.restore_alpha = alpha;
+    A.restore_beta = beta;
+    A.restore_values = vals.data();
+    rc = solve(c, A, r0, out.data(), nullptr, nullptr, V, nv);
+    if (rc > 0) {
+      const int st = take_status(c);
+      if (st) rc = st;
+    }
+  }
+  if (rc > 0 && (cudaMemcpyAsync(vectors, V, bytes * nv, cudaMemcpyDeviceToHost, c.stream) !=
+                     cudaSuccess ||
+                 cudaStreamSynchronize(c.stream) != cudaSuccess))
+    rc = set_error(TBGPU_E_CUDA);
+  cudaFree(r0);
+  cudaFree(V);
+  return rc > 0 ? nv : rc;
+}
+
 int tbgpu_get_tridiagonal(const tbgpu_ctx *ctx, double *alpha, double *beta, int cap) {
   if (!ctx || !alpha || !beta) return set_error(TBGPU_E_ARG);
   const Ctx &c = *C(ctx);
@@ -591,6 +636,70 @@ int tbgpu_get_stats(const tbgpu_ctx *ctx, tbgpu_stats *out) {
   if (!ctx || !out) return set_error(TBGPU_E_ARG);
   *out = C(ctx)->stats;
   return TBGPU_OK;
+}
+
+int tbgpu_set_fold(tbgpu_ctx *ctx, int on, double shift1, double shift2, double factor,
+                   double offset) {
+  if (!ctx || (on != 0 && on != 1) || !std::isfinite(shift1) || !std::isfinite(shift2) ||
+      !std::isfinite(factor) || !std::isfinite(offset) || factor == 0.0)
+    return set_error(TBGPU_E_ARG);
+  Ctx &c = *C(ctx);
+  c.fold = on != 0;
+  c.fold_s1 = shift1;
+  c.fold_s2 = shift2;
+  c.fold_factor = factor;
+  c.fold_offset = offset;
+  return TBGPU_OK;
+}
+
+int tbgpu_hx_fold_dev(tbgpu_ctx *ctx, const double *x_dev, double *y_dev) {
+  if (!ctx || !x_dev || !y_dev || x_dev == y_dev || misaligned16(x_dev) || misaligned16(y_dev))
+    return set_error(TBGPU_E_ARG);
+  Ctx &c = *C(ctx);
+  if (!c.built) return set_error(TBGPU_E_STATE);
+  const size_t bytes = sizeof(double) * 2 * size_t(c.natoms) * c.nb;
+  if (!c.d_fold_tmp && cudaMalloc(&c.d_fold_tmp, bytes) != cudaSuccess)
+    return set_error(TBGPU_E_NOMEM);
+  return fold_product(c, x_dev, y_dev, c.d_fold_tmp, c.stream);
+}
+
+void tbgpu_matvect_mult2(const int **argList, tbgpu_dcomplex *y, const tbgpu_dcomplex *x) {
+  set_error(TBGPU_OK);  // void entry point: status is read back via tbgpu_last_error
+  if (!argList || !argList[0] || !x || !y) {
+    set_error(TBGPU_E_ARG);
+    return;
+  }
+  Ctx &c = *reinterpret_cast<Ctx *>(const_cast<int *>(argList[0]));
+  if (!c.built) {
+    set_error(TBGPU_E_STATE);
+    return;
+  }
+  const size_t bytes = sizeof(double) * 2 * size_t(c.natoms) * c.nb;
+  if ((!c.d_x && (cudaMalloc(&c.d_x, bytes) != cudaSuccess ||
+                  cudaMalloc(&c.d_y, bytes) != cudaSuccess)) ||
+      (!c.d_fold_tmp && cudaMalloc(&c.d_fold_tmp, bytes) != cudaSuccess)) {
+    set_error(TBGPU_E_NOMEM);
+    return;
+  }
+  if (cudaMemcpyAsync(c.d_x, x, bytes, cudaMemcpyHostToDevice, c.stream) != cudaSuccess) {
+    set_error(TBGPU_E_CUDA);
+    return;
+  }
+  if (fold_product(c, c.d_x, c.d_y, c.d_fold_tmp, c.stream)) return;
+  if (cudaMemcpyAsync(y, c.d_y, bytes, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
+      cudaStreamSynchronize(c.stream) != cudaSuccess) {
+    set_error(TBGPU_E_CUDA);
+    return;
+  }
+  take_status(c);
+}
+
+int tbgpu_get_fold_energies(const tbgpu_ctx *ctx, int cap, double *energies) {
+  if (!ctx || cap < 0 || (cap > 0 && !energies)) return set_error(TBGPU_E_ARG);
+  const Ctx &c = *C(ctx);
+  const int n = int(c.fold_energy.size());
+  for (int i = 0; i < n && i < cap; i++) energies[i] = c.fold_energy[i];
+  return n;
 }
 
 int tbgpu_set_eigenvector_pass(tbgpu_ctx *ctx, int mode, int columns, int segment) {

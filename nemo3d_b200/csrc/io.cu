@@ -114,3 +114,72 @@ extern "C" int tbgpu_write_eigenvector(const tbgpu_ctx *ctx, const char *path,
   std::fclose(fp);
   return ok ? TBGPU_OK : set_error(TBGPU_E_ARG);
 }
+
+// The tridiagonal matrix and eigenvalue files of eigensolve_lanczos's saved
+// state (eigen/src/lanczos.c:1692-1809): native-endian binary,
+//   T:       int iterations, int processors, double t[2*iterations] with
+//            t[2i] = alpha_i and t[2i-1] = beta_{i-1} (the last slot unused);
+//   values:  int n, double value[n].
+// On reading, the reference keeps iterations - 200 of the stored matrix
+// (restoreTridiagonalMatrix, lanczos.c:1765); so does this reader.
+extern "C" int tbgpu_write_tridiagonal_file(const char *path, const double *alpha,
+                                            const double *beta, int iterations,
+                                            int processors) {
+  if (!path || !alpha || !beta || iterations < 1) return set_error(TBGPU_E_ARG);
+  std::vector<double> t(2 * size_t(iterations), 0.0);
+  for (int i = 0; i < iterations; i++) t[2 * size_t(i)] = alpha[i];
+  for (int i = 1; i < iterations; i++) t[2 * size_t(i) - 1] = beta[i - 1];
+  FILE *fp = std::fopen(path, "wb");
+  if (!fp) return set_error(TBGPU_E_ARG);
+  const bool ok = std::fwrite(&iterations, sizeof(int), 1, fp) == 1 &&
+                  std::fwrite(&processors, sizeof(int), 1, fp) == 1 &&
+                  std::fwrite(t.data(), sizeof(double), t.size(), fp) == t.size();
+  return (std::fclose(fp) == 0 && ok) ? TBGPU_OK : set_error(TBGPU_E_ARG);
+}
+
+extern "C" int tbgpu_read_tridiagonal_file(const char *path, int cap, double *alpha,
+                                           double *beta, int *processors) {
+  if (!path || cap < 0 || (cap > 0 && (!alpha || !beta))) return set_error(TBGPU_E_ARG);
+  FILE *fp = std::fopen(path, "rb");
+  if (!fp) return set_error(TBGPU_E_ARG);
+  int stored = 0, procs = 0;
+  bool ok = std::fread(&stored, sizeof(int), 1, fp) == 1 &&
+            std::fread(&procs, sizeof(int), 1, fp) == 1 && stored > 200;
+  const int its = stored - 200;
+  std::vector<double> t;
+  if (ok) {
+    t.resize(2 * size_t(its));
+    ok = std::fread(t.data(), sizeof(double), t.size(), fp) == t.size();
+  }
+  std::fclose(fp);
+  if (!ok) return set_error(TBGPU_E_ARG);
+  if (processors) *processors = procs;
+  for (int i = 0; i < its && i < cap; i++) {
+    alpha[i] = t[2 * size_t(i)];
+    beta[i] = i + 1 < its ? t[2 * size_t(i) + 1] : 0.0;
+  }
+  return its;
+}
+
+extern "C" int tbgpu_write_eigenvalue_file(const char *path, const double *values, int n) {
+  if (!path || n < 0 || (n > 0 && !values)) return set_error(TBGPU_E_ARG);
+  FILE *fp = std::fopen(path, "wb");
+  if (!fp) return set_error(TBGPU_E_ARG);
+  const bool ok = std::fwrite(&n, sizeof(int), 1, fp) == 1 &&
+                  std::fwrite(values, sizeof(double), size_t(n), fp) == size_t(n);
+  return (std::fclose(fp) == 0 && ok) ? TBGPU_OK : set_error(TBGPU_E_ARG);
+}
+
+extern "C" int tbgpu_read_eigenvalue_file(const char *path, int cap, double *values) {
+  if (!path || cap < 0 || (cap > 0 && !values)) return set_error(TBGPU_E_ARG);
+  FILE *fp = std::fopen(path, "rb");
+  if (!fp) return set_error(TBGPU_E_ARG);
+  int n = 0;
+  bool ok = std::fread(&n, sizeof(int), 1, fp) == 1 && n >= 0;
+  std::vector<double> v(ok ? size_t(n) : 0);
+  if (ok) ok = std::fread(v.data(), sizeof(double), v.size(), fp) == v.size();
+  std::fclose(fp);
+  if (!ok) return set_error(TBGPU_E_ARG);
+  for (int i = 0; i < n && i < cap; i++) values[i] = v[i];
+  return n;
+}

@@ -116,6 +116,86 @@ __global__ void __launch_bounds__(kRedThreads)
   grid_reduce<kRedThreads>(s, partial, counter, bet, it + 1, true);
 }
 
+// Folded operator F = factor (H - s2)(H - s1) + offset (matvect_mult2,
+// nemo3d/src/base/h_cvectr_mult.c:156-198), after its two products:
+// w = factor * w + offset * q with q = rc / bet[it] (rc itself when bet is
+// null), and, with alpha_out, alpha = Re<q, w> reduced deterministically.
+template <typename VT>
+__global__ void __launch_bounds__(kRedThreads)
+    k_fold_combine(long n2, const VT *__restrict__ rc, const double *bet, int it, double factor,
+                   double offset, VT *__restrict__ w, double *partial, unsigned *counter,
+                   double *alpha_out, int aidx) {
+  const double iq = bet ? 1.0 / bet[it] : 1.0;
+  double s = 0.0;
+  for (long j = blockIdx.x * (long)blockDim.x + threadIdx.x; j < n2;
+       j += (long)gridDim.x * blockDim.x) {
+    const double2 cv = widen(rc[j]), wv = widen(w[j]);
+    const double qx = cv.x * iq, qy = cv.y * iq;
+    const VT o = narrow<VT>(factor * wv.x + offset * qx, factor * wv.y + offset * qy);
+    w[j] = o;
+    const double2 ov = widen(o);
+    s += qx * ov.x + qy * ov.y;
+  }
+  if (alpha_out) grid_reduce<kRedThreads>(s, partial, counter, alpha_out, aidx, false);
+}
+
+// out[idx] = Re<a, b> (deterministic)
+__global__ void __launch_bounds__(kRedThreads)
+    k_rdot(long n2, const double2 *__restrict__ a, const double2 *__restrict__ b,
+           double *partial, unsigned *counter, double *out, int idx) {
+  double s = 0.0;
+  for (long j = blockIdx.x * (long)blockDim.x + threadIdx.x; j < n2;
+       j += (long)gridDim.x * blockDim.x)
+    s += a[j].x * b[j].x + a[j].y * b[j].y;
+  grid_reduce<kRedThreads>(s, partial, counter, out, idx, false);
+}
+
+// y = F x on double vectors in the reference's order (tmp: one vector)
+int fold_product(Ctx &c, const double *x, double *y, double *tmp, cudaStream_t s) {
+  int rc = launch_spmv(c, x, tmp, c.fold_s1, nullptr, 0, nullptr, 0, s);
+  if (!rc) rc = launch_spmv(c, tmp, y, c.fold_s2, nullptr, 0, nullptr, 0, s);
+  if (rc) return rc;
+  const long n2 = c.natoms * c.nb;
+  k_fold_combine<double2><<<red_grid(c, n2), kRedThreads, 0, s>>>(
+      n2, reinterpret_cast<const double2 *>(x), nullptr, 0, c.fold_factor, c.fold_offset,
+      reinterpret_cast<double2 *>(y), nullptr, nullptr, nullptr, 0);
+  TB_CUDA(cudaGetLastError());
+  return TBGPU_OK;
+}
+
+// Rayleigh quotients <v, H v> / <v, v> of nv double vectors in the reference's
+// order (the energies of a folded solve's eigenvectors)
+static int rayleigh_quotients(Ctx &c, const double *V, int nv, std::vector<double> &out,
+                              cudaStream_t s) {
+  const long n2 = c.natoms * c.nb;
+  double *y = nullptr, *d = nullptr;
+  out.assign(nv, 0.0);
+  if (cudaMallocAsync(&y, sizeof(double2) * n2, s) != cudaSuccess ||
+      cudaMallocAsync(&d, sizeof(double) * 2 * std::max(nv, 1), s) != cudaSuccess) {
+    if (y) cudaFreeAsync(y, s);
+    return set_error(TBGPU_E_NOMEM);
+  }
+  const unsigned rg = red_grid(c, n2);
+  int rc = ensure_partials(c, int(rg));
+  for (int e = 0; e < nv && !rc; e++) {
+    const double2 *v = reinterpret_cast<const double2 *>(V) + size_t(e) * n2;
+    rc = launch_spmv(c, reinterpret_cast<const double *>(v), y, 0.0, nullptr, 0, nullptr, 0, s);
+    if (rc) break;
+    k_rdot<<<rg, kRedThreads, 0, s>>>(n2, v, reinterpret_cast<const double2 *>(y), c.d_partial,
+                                      c.d_counter, d, 2 * e);
+    k_rdot<<<rg, kRedThreads, 0, s>>>(n2, v, v, c.d_partial, c.d_counter, d, 2 * e + 1);
+  }
+  std::vector<double> h(2 * std::max(nv, 1));
+  if (!rc && (cudaMemcpyAsync(h.data(), d, sizeof(double) * 2 * nv, cudaMemcpyDeviceToHost, s) !=
+                  cudaSuccess ||
+              cudaStreamSynchronize(s) != cudaSuccess))
+    rc = set_error(TBGPU_E_CUDA);
+  for (int e = 0; e < nv && !rc; e++) out[e] = h[2 * e] / h[2 * e + 1];
+  cudaFreeAsync(y, s);
+  cudaFreeAsync(d, s);
+  return rc;
+}
+
 constexpr int kMaxChunk = 32;
 constexpr int kVecGroup = 16;
 // the regenerating eigenvector pass accumulates up to 64 rows (its columns'
@@ -481,7 +561,12 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
   // one-column launches -- the pencil kernel when variant 6 is set and
   // applies, else the lane kernel (variant 5)
   const bool f32_ok = !kMixed || c.ham_fp32;
-  bool regen = c.vec_pass == 1 && V_dev && maxvec > 0 && lane_supported(c) && f32_ok;
+  // folded-spectrum operator (tbgpu_set_fold): two products per step, plain
+  // second run for the eigenvectors, double precision only
+  const bool fold = c.fold;
+  if (fold && kMixed) return set_error(TBGPU_E_UNSUPPORTED);
+  c.fold_energy.clear();
+  bool regen = !fold && c.vec_pass == 1 && V_dev && maxvec > 0 && lane_supported(c) && f32_ok;
   const int keep_variant = c.spmv_variant;
   if (regen) c.spmv_variant = pen_supported(c) && keep_variant == 6 ? 6 : 5;
   // the pencil kernel keeps the Lanczos vectors in its own layout: the start
@@ -515,6 +600,7 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
   unsigned long long *d_diff = nullptr;
   double *r0_pen = nullptr;  // pencil layout: the start vector
   double *V_pen = nullptr;   // ... and the eigenvectors before they go out
+  VT *Tf = nullptr;          // folded operator: the first product
   auto drop_checkpoints = [&]() {
     for (VT *q : ck_cur) if (q) cudaFreeAsync(q, s);
     for (VT *q : ck_prev) if (q) cudaFreeAsync(q, s);
@@ -532,6 +618,8 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
     r0_pen = nullptr;
     if (V_pen) cudaFreeAsync(V_pen, s);
     V_pen = nullptr;
+    if (Tf) cudaFreeAsync(Tf, s);
+    Tf = nullptr;
     for (int i = 0; i <= kMaxChunk; i++)
       if (ring[i]) cudaFree(ring[i]);
     if (W) cudaFree(W);
@@ -559,6 +647,7 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
   } while (0)
   for (int i = 0; i < S1; i++) SOLVE_CUDA(cudaMalloc(&ring[i], vbytes));
   SOLVE_CUDA(cudaMalloc(&W, vbytes));
+  if (fold) SOLVE_CUDA(cudaMallocAsync(&Tf, vbytes, s));
   SOLVE_CUDA(cudaMalloc(&d_alpha, sizeof(double) * (A.imax + 1)));
   SOLVE_CUDA(cudaMalloc(&d_bet, sizeof(double) * (A.imax + 2)));
   SOLVE_CUDA(cudaMalloc(&d_tmp, sizeof(double) * 4));
@@ -595,8 +684,26 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
       cudaEventCreate(&e1);
       cudaEventRecord(e0, s);
     }
-    int r_ = pen ? launch_spmv_pen_internal<VT>(c, rc_, W, 0.0, bet, it, d_alpha, it, s)
-                 : spmv_step(c, rc_, W, bet, it, d_alpha, s);
+    int r_;
+    if (fold) {  // W = F q: T = (H - s1) q, W = (H - s2) T, W = factor W + offset q, alpha
+      r_ = pen ? launch_spmv_pen_internal<VT>(c, rc_, Tf, c.fold_s1, bet, it, nullptr, 0, s)
+               : launch_spmv(c, reinterpret_cast<const double *>(rc_),
+                             reinterpret_cast<double *>(Tf), c.fold_s1, bet, it, nullptr, 0, s);
+      if (!r_)
+        r_ = pen ? launch_spmv_pen_internal<VT>(c, Tf, W, c.fold_s2, nullptr, 0, nullptr, 0, s)
+                 : launch_spmv(c, reinterpret_cast<const double *>(Tf),
+                               reinterpret_cast<double *>(W), c.fold_s2, nullptr, 0, nullptr, 0,
+                               s);
+      if (!r_) {
+        k_fold_combine<VT><<<rg, kRedThreads, 0, s>>>(n2, rc_, bet, it, c.fold_factor,
+                                                      c.fold_offset, W, c.d_partial, c.d_counter,
+                                                      d_alpha, it);
+        launches += 2;
+      }
+    } else {
+      r_ = pen ? launch_spmv_pen_internal<VT>(c, rc_, W, 0.0, bet, it, d_alpha, it, s)
+               : spmv_step(c, rc_, W, bet, it, d_alpha, s);
+    }
     if (r_) return r_;
     if (c.profiling) {
       cudaEventRecord(e1, s);
@@ -696,6 +803,23 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
   };
   std::vector<double> Ta, Tb;
   const double *hb_final = h_bet;  // beta copy used by the second pass
+  std::vector<double> hb_restore;
+  const bool restore = A.restore_its > 0;
+  if (restore) {
+    // the tridiagonal matrix and eigenvalues of an earlier solve
+    // (eigensolve_lanczos with restoreState, lanczos.c:1912-1955): no first
+    // pass; every value's eigenvector uses the whole restored matrix
+    final_it = launched = A.restore_its;
+    Ta.assign(A.restore_alpha, A.restore_alpha + final_it);
+    Tb.assign(A.restore_beta, A.restore_beta + final_it);
+    hb_restore.assign(size_t(final_it) + 1, 1.0);  // bet[0]: the normalised start
+    for (int it = 1; it <= final_it; it++) hb_restore[it] = Tb[it - 1];
+    hb_final = hb_restore.data();
+    for (int k = 0; k < A.restore_n; k++) {
+      c2.push_back(A.restore_values[k]);
+      i2.push_back(final_it);
+    }
+  } else {
   SOLVE_RC(fill());
   while (!pend.empty()) {
     Pending p = pend.front();
@@ -732,9 +856,10 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
     SOLVE_RC(enqueue_until(A.imax));
     final_it = launched;
   }
+  }  // first pass
   SOLVE_CUDA(cudaEventRecord(tm.t1, s));
   SOLVE_CUDA(cudaStreamSynchronize(s));
-  if (final_it == launched) {  // stopped by the iteration limit: T up to there
+  if (!restore && final_it == launched) {  // stopped by the iteration limit: T up to there
     SOLVE_CUDA(cudaMemcpy(h_alpha, d_alpha, sizeof(double) * final_it, cudaMemcpyDeviceToHost));
     SOLVE_CUDA(cudaMemcpy(h_bet, d_bet, sizeof(double) * (final_it + 1), cudaMemcpyDeviceToHost));
     Ta.assign(h_alpha, h_alpha + final_it);
@@ -965,6 +1090,8 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
       c.stats.refine_ms = ms;
     }
   }
+  if (fold && V_dev && nvec > 0)  // the energies of the folded solve's eigenvectors
+    SOLVE_RC(rayleigh_quotients(c, V_dev, nvec, c.fold_energy, s));
   if (c.profiling) {
     SOLVE_CUDA(cudaStreamSynchronize(s));
     double tot = 0.0;

@@ -136,6 +136,13 @@ struct Ctx {
   // iteration segments from checkpoints saved by the first pass,
   // vec_columns segments at a time (lane kernel products, update fused)
   int vec_pass = 0, vec_columns = 4, vec_segment = 256;
+  // folded-spectrum operator F = factor (H - s2)(H - s1) + offset of
+  // matvect_mult2 (nemo3d/src/base/h_cvectr_mult.c:156-198; its constants
+  // by default); fold on: the Lanczos solves run on F
+  bool fold = false;
+  double fold_s1 = 1.48 - 0.1, fold_s2 = 1.48 + 0.1, fold_factor = -10.0, fold_offset = 0.0;
+  std::vector<double> fold_energy;  // <v, H v> of the last folded solve's vectors
+  double *d_fold_tmp = nullptr;     // scratch of the host-pointer folded matvec
 };
 
 // the stored Hamiltonian in its element type
@@ -260,9 +267,16 @@ int launch_spmv_async_scratch(Ctx &c, const double *x, double *y, double shift,
                               cudaStream_t s);
 // lanczos.cu
 int ensure_partials(Ctx &c, int nblocks);
+// y = F x (the folded operator) on double vectors in the reference's order
+int fold_product(Ctx &c, const double *x, double *y, double *tmp, cudaStream_t s);
 struct SolveArgs {
   int conv_start, conv_skip, imax, req1, req2;
   double emin1, emax1, emin2, emax2, tol;
+  // restoreState: eigenvectors of restore_n values from a given tridiagonal
+  // matrix of restore_its iterations (alpha[its], beta[its]), no first pass
+  int restore_its = 0, restore_n = 0;
+  const double *restore_alpha = nullptr, *restore_beta = nullptr,
+               *restore_values = nullptr;
 };
 int solve(Ctx &c, const SolveArgs &A, const double *r0_dev, double *values, int *conv_iters,
           int *iterations, double *V_dev, int maxvec);

@@ -111,6 +111,12 @@ def _lib():
         L.tbgpu_matvect_mult_dev.restype = None
         L.tbgpu_matvect_mult_dev.argtypes = [C.POINTER(vp), vp, vp]
         L.tbgpu_get_stats.argtypes = [vp, C.POINTER(Stats)]
+        L.tbgpu_set_fold.argtypes = [vp, ip, dp, dp, dp, dp]
+        L.tbgpu_matvect_mult2.restype = None
+        L.tbgpu_matvect_mult2.argtypes = [C.POINTER(vp), vp, vp]
+        L.tbgpu_hx_fold_dev.argtypes = [vp, vp, vp]
+        L.tbgpu_get_fold_energies.argtypes = [vp, ip, vp]
+        L.tbgpu_set_eigenvector_pass.argtypes = [vp, ip, ip, ip]
         _LIB = L
     return _LIB
 
@@ -447,6 +453,35 @@ class Hamiltonian:
         rc = _lib().tbgpu_set_spmv_variant(self._ctx, int(variant))
         if rc:
             raise TbgpuError(rc, "tbgpu_set_spmv_variant")
+
+    def set_fold(self, on=True, shift1=1.38, shift2=1.58, factor=-10.0, offset=0.0):
+        """Folded-spectrum operator F = factor (H - shift2)(H - shift1) + offset for
+        the Lanczos solves (tbgpu_set_fold; the defaults are matvect_mult2's)."""
+        rc = _lib().tbgpu_set_fold(self._ctx, int(bool(on)), C.c_double(shift1),
+                                   C.c_double(shift2), C.c_double(factor), C.c_double(offset))
+        if rc:
+            raise TbgpuError(rc, "tbgpu_set_fold")
+
+    def matvect_mult2(self, x: np.ndarray) -> np.ndarray:
+        """y = F x through the matvect_mult2 drop-in (host vectors)."""
+        x = np.ascontiguousarray(x, np.float64)
+        if x.size != 2 * self.n:
+            raise ValueError("x must hold 2*dimension doubles")
+        y = np.empty_like(x)
+        args = (C.c_void_p * 3)(self._ctx.value, None, None)
+        _lib().tbgpu_matvect_mult2(args, _p(y), _p(x))
+        rc = _lib().tbgpu_last_error()
+        if rc:
+            raise TbgpuError(rc, "tbgpu_matvect_mult2")
+        return y
+
+    def fold_energies(self):
+        """<v, H v> / <v, v> of the eigenvectors of the last folded solve."""
+        out = np.zeros(4096)
+        n = _lib().tbgpu_get_fold_energies(self._ctx, 4096, _p(out))
+        if n < 0:
+            raise TbgpuError(n, "tbgpu_get_fold_energies")
+        return out[:n].copy()
 
     def set_eigenvector_pass(self, mode: int, columns: int = 4, segment: int = 256):
         """0: the reference's second run of the recurrence; 1: regenerate
