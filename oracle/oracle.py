@@ -70,6 +70,7 @@ def lib():
         L.orc_build.argtypes = [C.POINTER(_Geom), C.POINTER(_Model), C.c_long,
                                 C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                 C.c_void_p, C.c_void_p]
+        L.orc_set_threads.argtypes = [C.c_int]
         L.orc_hx.argtypes = [C.c_int, C.c_int, C.c_long] + [C.c_void_p] * 6 + \
             [C.c_double, C.c_void_p, C.c_void_p]
         L.orc_dense.argtypes = [C.c_int, C.c_int, C.c_long] + [C.c_void_p] * 7
@@ -209,6 +210,48 @@ class OracleHamiltonian:
             v = vec[:2 * self.n * ne].reshape(ne, self.n, 2)
             out["evecs"] = v[..., 0] + 1j * v[..., 1]
         return out
+
+
+class _OracleH(C.Structure):
+    _fields_ = [("norb", C.c_int), ("nspin", C.c_int), ("natoms", C.c_long),
+                ("atom_slot", C.c_void_p), ("nbr", C.c_void_p), ("wrap", C.c_void_p),
+                ("kvec", C.c_void_p), ("onsite", C.c_void_p), ("blocks", C.c_void_p)]
+
+
+_REF_LANCZOS = None
+REF_LANCZOS_PATH = os.path.join(HERE, "_ref", "libref_lanczos.so")
+
+
+def ref_lanczos_available() -> bool:
+    return os.path.exists(REF_LANCZOS_PATH)
+
+
+def ref_eigenvalues_lanczos(o, r0, imax=2000, req=(1, 1), erange1=(-1, 0), erange2=(1, 2),
+                            tol=1e-7, conv_start=200, conv_skip=50):
+    """The reference's own first Lanczos pass (eigenvaluesLanczos of
+    eigen/src/lanczos.c, compiled from its source into
+    oracle/_ref/libref_lanczos.so by oracle/build_ref.sh) on the oracle's
+    stored Hamiltonian ``o`` (its H*x as the reference's matmul).  Returns
+    dict(evals, conv_it, iterations)."""
+    global _REF_LANCZOS
+    if _REF_LANCZOS is None:
+        L = C.CDLL(REF_LANCZOS_PATH)
+        L.ref_eigenvalues_lanczos.restype = C.c_int
+        L.ref_eigenvalues_lanczos.argtypes = [
+            C.c_void_p, C.c_long, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+            C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_void_p, C.c_void_p,
+            C.c_void_p]
+        _REF_LANCZOS = L
+    h = _OracleH(o.norb, o.nspin, o.natoms, _p(o.atom_slot), _p(o.nbr), _p(o.wrap),
+                 _p(o.kvec), _p(o.onsite), _p(o.blocks))
+    r0 = np.ascontiguousarray(r0, np.float64)
+    ev = np.zeros(imax)
+    cit = np.zeros(imax, np.int32)
+    its = np.zeros(1, np.int32)
+    ne = _REF_LANCZOS.ref_eigenvalues_lanczos(
+        C.byref(h), o.n, _p(r0), conv_start, conv_skip, imax, req[0], req[1], erange1[0],
+        erange1[1], erange2[0], erange2[1], tol, _p(ev), _p(cit), _p(its))
+    return dict(evals=ev[:ne].copy(), conv_it=cit[:ne].copy(), iterations=int(its[0]))
 
 
 def tridiag_eigs(d, e, vl, vu, abstol=1e-13):

@@ -12,6 +12,19 @@
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* Host threads of the oracle's OpenMP loops (the CPU baseline times the
+ * reference's serial path with 1 and the parallel restatement with all). */
+void orc_set_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+#else
+  (void)n;
+#endif
+}
 
 /* The reference's sqrt(3) constant (mb_ham_spds_micro.c:42).  It is not the
  * correctly rounded sqrt(3); H entries only agree to 1e-12 with it. */

@@ -134,6 +134,9 @@ int orc_vff_relax(const orc_geom *g, long natoms, const int *atom_slot, const in
                   const unsigned char *surface, int ns, const double *vff, int bc, int itmax,
                   double tol, int end_if_small_step, double *u, double *energy);
 
+/* Host threads of the oracle's OpenMP loops. */
+void orc_set_threads(int n);
+
 #ifdef __cplusplus
 }
 #endif

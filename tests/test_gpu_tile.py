@@ -154,7 +154,7 @@ def test_tile_variant_range():
     from nemo3d_b200.tbgpu import TbgpuError
     g, _ = _ham(STRUCTURES["dome_7x6x5"](), "sp3d5s*")
     with pytest.raises(TbgpuError):
-        g.set_spmv_variant(6)
+        g.set_spmv_variant(7)
     with pytest.raises(TbgpuError):
         g.set_spmv_variant(-1)
 

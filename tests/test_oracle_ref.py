@@ -186,3 +186,35 @@ def test_dangling_bond_passivation(ref_sk, model, nbasis, norb):
             assert np.abs(ref).max() == 0.0 and np.abs(got).max() == 0.0
     assert nsurf > 100
     assert len(patterns) >= 10, patterns  # most of the 15 bond-loss patterns occur
+
+
+@pytest.mark.parametrize("case", ["cube_sp3s", "dome_spds_so"])
+def test_oracle_lanczos_matches_reference_lanczos(case):
+    """The oracle's restatement of the Lanczos driver (oracle/tb_oracle.c)
+    against the reference's own eigenvaluesLanczos (eigen/src/lanczos.c,
+    compiled from its source into oracle/_ref/libref_lanczos.so), both on
+    the oracle's H*x: the same eigenvalues (1e-10 eV) and iteration count;
+    the iteration at which each value was accepted agrees to one check
+    interval (the inverse iterations of the test start from a seeded
+    generator here and from glibc rand() there, which can move a borderline
+    acceptance by one check)."""
+    from nemo3d_b200 import workloads as W
+    if not O.ref_lanczos_available():
+        pytest.skip("oracle/_ref/libref_lanczos.so not built (reference sources absent)")
+    if case == "cube_sp3s":
+        st = W.gaas_cube(4)
+        o = O.OracleHamiltonian(st, 5, 1, [M.MATERIALS["GaAs_sps"], M.MATERIALS["InAs_sps"]])
+        kw = dict(imax=3000, req=(3, 3), erange1=(-0.5, 0.0), erange2=(1.5, 2.5))
+    else:
+        st = W.dome_in_box(cells=(5, 5, 4), base_nm=1.8, height_nm=0.8, wl_z_nm=0.6,
+                           sigma_frac=0.01, seed=4)
+        o = O.OracleHamiltonian(st, 10, 2, [M.MATERIALS["GaAs_spds"], M.MATERIALS["InAs_spds"]])
+        kw = dict(imax=2500, req=(2, 2), erange1=(-0.6, 0.75), erange2=(1.5, 2.8))
+    r0 = W.random_start(o.n, seed=0)
+    kw.update(tol=1e-7, conv_start=100, conv_skip=50)
+    ref = O.ref_eigenvalues_lanczos(o, r0, **kw)
+    got = o.lanczos(r0, **kw)
+    assert len(ref["evals"]) == len(got["evals"]) >= 2
+    assert np.abs(ref["evals"] - got["evals"]).max() < 1e-10
+    assert ref["iterations"] == got["iterations"]
+    assert np.abs(ref["conv_it"] - got["conv_it"]).max() <= kw["conv_skip"]
