@@ -281,6 +281,27 @@ int tbgpu_eigensolve_blk_lanczos_dev(tbgpu_ctx *ctx, int ConvCheckStartIter,
                                      int *found_cb, int *iterations,
                                      double *vectors_dev, int max_vectors);
 
+/* Block dots G = X^H Y of two blocks of p (1..8) complex vectors on the
+ * tensor cores, to double precision: the p x p inner products of the block
+ * QR and of Q^H W in every block Lanczos step (eigen/src/lanczos_blk.c:
+ * 150-219, 273-357).  x_dev, y_dev: p vectors of n2 complex entries back to
+ * back (interleaved re, im; 16-byte aligned), device memory.  G (host) gets
+ * the row-major p x p complex matrix, G[2(ip+j)] + i G[2(ip+j)+1] = x_i^H y_j.
+ * The entries are cut into eight 7-bit integer slices (56 bits) with one
+ * exponent per 256 entries and vector part, and multiplied by tcgen05.mma
+ * kind::i8 with int32 accumulators; per entry the error is below 2^-50 of
+ * max|x| max|y| over its 256-entry chunk (a double dot: 2^-53 of each
+ * product, plus the rounding of its sums).  Runs on the
+ * context's stream and synchronises it; status word checked (TBGPU_E_TIMEOUT
+ * when a tensor-core wait ran out). */
+int tbgpu_block_dots_dev(tbgpu_ctx *ctx, int p, const double *x_dev, const double *y_dev,
+                         long n2, double *G);
+
+/* Which kernel forms the block dots of tbgpu_eigensolve_blk_lanczos(_dev):
+ * 0 (default) the double-precision CUDA-core kernel, 1 the tensor-core kernel
+ * of tbgpu_block_dots_dev.  TBGPU_E_ARG for another mode. */
+int tbgpu_set_block_dots(tbgpu_ctx *ctx, int mode);
+
 /* Tridiagonal matrix of the last solve: alpha[n], beta[n] (n <= cap). */
 int tbgpu_get_tridiagonal(const tbgpu_ctx *ctx, double *alpha, double *beta,
                           int cap);

@@ -12,7 +12,7 @@ LIB = os.path.join(HERE, "libtbgpu.so")
 SOURCES = ["topology.cu", "build.cu", "spmv.cu", "spmv_async.cu", "lanczos.cu", "capi.cu",
            "noalloc.cu", "band_eig.cu", "blk_lanczos.cu", "spmm_async.cu", "io.cu",
            "recompute.cu", "optics.cu", "vff.cu",
-           "batch.cu", "spmv_tile.cu", "warmstart.cu", "spmv_lane.cu", "spmv_pen.cu"]
+           "batch.cu", "spmv_tile.cu", "warmstart.cu", "spmv_lane.cu", "spmv_pen.cu", "bdots_tc.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3",
               "-std=c++17", "-Xcompiler", "-fPIC", "-shared"]
 

@@ -384,6 +384,17 @@ static int blk_run(Ctx &c, const BlkArgs &A, const double *r0_dev, std::vector<d
     return set_error(TBGPU_E_NOMEM);
   }
   if (cudaMemsetAsync(counter, 0, sizeof(unsigned), s) != cudaSuccess) rc = TBGPU_E_CUDA;
+  // the tensor-core dots keep 256 partial sums per CTA and the full 8 x 8
+  // product
+  const bool tc = c.block_dots == 1;
+  const int tc_grid = tc ? bdots_tc_grid(c, n2) : 0;
+  double *tc_part = nullptr, *tc_out = nullptr;
+  if (tc && (cudaMalloc(&tc_part, sizeof(double) * 256 * size_t(tc_grid)) != cudaSuccess ||
+             cudaMalloc(&tc_out, sizeof(double) * 2 * kMaxP * kMaxP) != cudaSuccess)) {
+    cudaFree(tc_part); cudaFree(tc_out);
+    cudaFree(Q); cudaFree(Qo); cudaFree(R); cudaFree(partial); cudaFree(dres); cudaFree(counter);
+    return set_error(TBGPU_E_NOMEM);
+  }
   auto ptrs = [&](double2 *base) {
     BlockPtrs b{};
     for (int i = 0; i < P; i++) b.v[i] = base + size_t(i) * n2;
@@ -396,19 +407,40 @@ static int blk_run(Ctx &c, const BlkArgs &A, const double *r0_dev, std::vector<d
   };
   // lower-triangle dots -> full Hermitian p x p matrix G[i][j] = X_i^H Y_j
   auto dots = [&](double2 *X, double2 *Y, Mat &G) -> int {
-    k_bdots<P><<<grid, kDotThreads, 0, s>>>(n2, ptrs(X), ptrs(Y), partial, counter, dres);
-    if (cudaGetLastError() != cudaSuccess) return fail(TBGPU_E_CUDA);
-    double h[2 * K];
-    if (cudaMemcpyAsync(h, dres, sizeof(h), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-        cudaStreamSynchronize(s) != cudaSuccess)
-      return fail(TBGPU_E_CUDA);
     G.assign(size_t(P) * P, cplx(0.0, 0.0));
-    int t = 0;
-    for (int i = 0; i < P; i++)
-      for (int j = 0; j <= i; j++, t++) {
-        G[i * P + j] = cplx(h[2 * t], h[2 * t + 1]);
-        G[j * P + i] = std::conj(G[i * P + j]);
+    if (tc) {
+      const double2 *xp[P], *yp[P];
+      for (int i = 0; i < P; i++) {
+        xp[i] = X + size_t(i) * n2;
+        yp[i] = Y + size_t(i) * n2;
       }
+      if (launch_bdots_tc(c, P, xp, yp, n2, tc_part, counter, tc_grid, tc_out, s))
+        return fail(TBGPU_E_CUDA);
+      double h[2 * kMaxP * kMaxP];
+      if (cudaMemcpyAsync(h, tc_out, sizeof(h), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+          cudaStreamSynchronize(s) != cudaSuccess)
+        return fail(TBGPU_E_CUDA);
+      if (int st = take_status(c)) return fail(st);
+      // the lower triangle, as the CUDA-core kernel forms it
+      for (int i = 0; i < P; i++)
+        for (int j = 0; j <= i; j++) {
+          G[i * P + j] = cplx(h[2 * (i * kMaxP + j)], h[2 * (i * kMaxP + j) + 1]);
+          G[j * P + i] = std::conj(G[i * P + j]);
+        }
+    } else {
+      k_bdots<P><<<grid, kDotThreads, 0, s>>>(n2, ptrs(X), ptrs(Y), partial, counter, dres);
+      if (cudaGetLastError() != cudaSuccess) return fail(TBGPU_E_CUDA);
+      double h[2 * K];
+      if (cudaMemcpyAsync(h, dres, sizeof(h), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+          cudaStreamSynchronize(s) != cudaSuccess)
+        return fail(TBGPU_E_CUDA);
+      int t = 0;
+      for (int i = 0; i < P; i++)
+        for (int j = 0; j <= i; j++, t++) {
+          G[i * P + j] = cplx(h[2 * t], h[2 * t + 1]);
+          G[j * P + i] = std::conj(G[i * P + j]);
+        }
+    }
     for (int i = 0; i < P; i++) G[i * P + i] = cplx(G[i * P + i].real(), 0.0);
     return TBGPU_OK;
   };
@@ -657,6 +689,7 @@ static int blk_run(Ctx &c, const BlkArgs &A, const double *r0_dev, std::vector<d
   cudaFree(Cand);
   (void)converged;
   cudaStreamSynchronize(s);
+  cudaFree(tc_part); cudaFree(tc_out);
   cudaFree(Q); cudaFree(Qo); cudaFree(R); cudaFree(partial); cudaFree(dres); cudaFree(counter);
   if (rc) return set_error(rc);
   found1_out = int(conv1.size());

@@ -713,6 +713,12 @@ int tbgpu_set_eigenvector_pass(tbgpu_ctx *ctx, int mode, int columns, int segmen
   return TBGPU_OK;
 }
 
+int tbgpu_set_block_dots(tbgpu_ctx *ctx, int mode) {
+  if (!ctx || mode < 0 || mode > 1) return set_error(TBGPU_E_ARG);
+  C(ctx)->block_dots = mode;
+  return TBGPU_OK;
+}
+
 int tbgpu_last_error(void) { return g_last_error; }
 
 const char *tbgpu_error_string(int code) {

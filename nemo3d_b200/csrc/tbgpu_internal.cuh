@@ -136,6 +136,9 @@ struct Ctx {
   // iteration segments from checkpoints saved by the first pass,
   // vec_columns segments at a time (lane kernel products, update fused)
   int vec_pass = 0, vec_columns = 4, vec_segment = 256;
+  // block Lanczos dots: 0 = double-precision CUDA-core kernel, 1 = the
+  // tensor-core (tcgen05 kind::i8 slice) kernel
+  int block_dots = 0;
   // folded-spectrum operator F = factor (H - s2)(H - s1) + offset of
   // matvect_mult2 (nemo3d/src/base/h_cvectr_mult.c:156-198; its constants
   // by default); fold on: the Lanczos solves run on F
@@ -255,6 +258,13 @@ int pen_permute(Ctx &c, const VT *in, VT *out, bool to_pen, cudaStream_t s);
 template <typename VT>
 int launch_pen_regen(Ctx &c, int p, const VT *const *x, VT *const *y, const VT *const *rp,
                      const int *it, const double *bet, const double *alpha, cudaStream_t s);
+// bdots_tc.cu: G (2*8*8 doubles, device, row-major 8 x 8 complex) = X^H Y of
+// blocks of p <= 8 vectors on tcgen05 (int8 slices, exact int32 sums,
+// double scaling); partial >= grid * 256 doubles, counter zeroed
+int launch_bdots_tc(Ctx &c, int p, const double2 *const *x, const double2 *const *y, long n2,
+                    double *partial, unsigned int *counter, int grid, double *G_dev,
+                    cudaStream_t s);
+int bdots_tc_grid(const Ctx &c, long n2);
 // spmv_tile.cu: variant 3 (falls back to launch_spmv_async where it does not apply)
 int launch_spmv_tile(Ctx &c, const double *x, double *y, double shift,
                      const double *xscale_dev, int scale_index, double *alpha_out,

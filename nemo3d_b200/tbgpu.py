@@ -83,6 +83,8 @@ def _lib():
         L.tbgpu_write_eigenvalues.argtypes = [C.c_char_p, C.c_char, vp, ip, vp]
         L.tbgpu_write_eigenvector.argtypes = [vp, C.c_char_p, vp, ip]
         L.tbgpu_hx_block_dev.argtypes = [vp, ip, dp, vp, vp]
+        L.tbgpu_block_dots_dev.argtypes = [vp, ip, vp, vp, C.c_long, vp]
+        L.tbgpu_set_block_dots.argtypes = [vp, ip]
         L.tbgpu_eigensolve_blk_lanczos.argtypes = [vp, ip, ip, ip, ip, ip, dp, dp, dp, dp, dp,
                                                    ip, ip, vp, vp, vp, vp, vp, vp, ip]
         L.tbgpu_ctx_create.argtypes = [C.POINTER(_Geom), C.POINTER(_Model), C.POINTER(vp)]
@@ -287,6 +289,23 @@ class Hamiltonian:
                                        C.c_void_p(y_ptr))
         if rc:
             raise TbgpuError(rc, "tbgpu_hx_block_dev")
+
+    def block_dots_dev(self, p: int, x_ptr: int, y_ptr: int, n2: int):
+        """G = X^H Y (p x p complex) of two blocks of p device vectors of n2
+        complex entries stored back to back, on the tensor cores."""
+        G = np.empty(2 * p * p)
+        rc = _lib().tbgpu_block_dots_dev(self._ctx, int(p), C.c_void_p(x_ptr),
+                                         C.c_void_p(y_ptr), int(n2), _p(G))
+        if rc:
+            raise TbgpuError(rc, "tbgpu_block_dots_dev")
+        return (G[0::2] + 1j * G[1::2]).reshape(p, p)
+
+    def set_block_dots(self, mode: int):
+        """Block Lanczos dots on the CUDA cores in double (0) or on the tensor
+        cores (1, int8 slices of the double entries)."""
+        rc = _lib().tbgpu_set_block_dots(self._ctx, int(mode))
+        if rc:
+            raise TbgpuError(rc, "tbgpu_set_block_dots")
 
     # -- eigensolver ----------------------------------------------------------
     def eigensolve_lanczos(self, r_0, ConvCheckStartIter=200, ConvCheckSkipRate=50,
