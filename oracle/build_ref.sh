@@ -41,17 +41,25 @@ g++ $FLAGS $DEFS $INC -c "$HERE/ref_sk_driver.cc" -o "$OUT/ref_sk_driver.o"
 # dropped by --gc-sections together with their unresolved references
 g++ -Wl,--gc-sections -o "$OUT/ref_sk" "$OUT/ref_sk_driver.o" "$OUT/mb_ham_spds_micro.o" \
   "$OUT/Cell.o" -lm
-# the reference's Lanczos driver (eigen/src/lanczos.c) and its serial MPI
-# layer, with nml routines, dstebz forwarded to scipy's bundled OpenBLAS
+# the reference's Lanczos drivers (eigen/src/lanczos.c, lanczos_blk.c) and
+# its serial MPI layer, with nml routines, dstebz forwarded to scipy's bundled OpenBLAS
 # and the oracle's H*x as its matmul: oracle/_ref/libref_lanczos.so
 BLAS=$(python3 -c "import glob, os, scipy; print(sorted(glob.glob(os.path.join(os.path.dirname(os.path.dirname(scipy.__file__)), 'scipy.libs', 'libscipy_openblas-*.so')))[0])" 2>/dev/null || true)
 if [ -n "$BLAS" ] && [ -f "$HERE/liboracle.so" ]; then
   FPIC="-fPIC"
   g++ -x c++ $FLAGS $FPIC $DEFS $INC -c "$R/eigen/src/lanczos.c" -o "$OUT/lanczos.o"
   g++ -x c++ $FLAGS $FPIC $DEFS $INC -c "$R/eigen/src/mpi_fake.c" -o "$OUT/mpi_fake.o"
-  g++ $FLAGS $FPIC $DEFS $INC -I"$HERE" -c "$HERE/ref_lanczos_driver.cc" -o "$OUT/ref_lanczos_driver.o"
+  # the block Lanczos (LAPACK names with one trailing underscore; the
+  # function form of the serial Allreduce_MPI_sp, which the driver defines
+  # with MPI's meaning, for the double and complex pointers the source passes;
+  # ref_blk_compat.h also supplies the memset header the source omits)
+  g++ -x c++ $FLAGS $FPIC $DEFS -DFORTRAN_UNDERSCORE -DNoGnuStatementExpre $INC \
+    -include "$HERE/ref_blk_compat.h" \
+    -c "$R/eigen/src/lanczos_blk.c" -o "$OUT/lanczos_blk.o"
+  g++ $FLAGS $FPIC $DEFS -DNoGnuStatementExpre $INC -I"$HERE" -c "$HERE/ref_lanczos_driver.cc" \
+    -o "$OUT/ref_lanczos_driver.o"
   g++ -shared -o "$OUT/libref_lanczos.so" "$OUT/ref_lanczos_driver.o" "$OUT/lanczos.o" \
-    "$OUT/mpi_fake.o" "$HERE/liboracle.so" "$BLAS" -Wl,-rpath,"$HERE" \
+    "$OUT/lanczos_blk.o" "$OUT/mpi_fake.o" "$HERE/liboracle.so" "$BLAS" -Wl,-rpath,"$HERE" \
     -Wl,-rpath,"$(dirname "$BLAS")" -Wl,--no-undefined -lm
   echo "$OUT/libref_lanczos.so"
 fi

@@ -254,6 +254,48 @@ def ref_eigenvalues_lanczos(o, r0, imax=2000, req=(1, 1), erange1=(-1, 0), erang
     return dict(evals=ev[:ne].copy(), conv_it=cit[:ne].copy(), iterations=int(its[0]))
 
 
+_REF_BLK = None
+
+
+def ref_block_lanczos(o, r0_block, imax=400, req=(0, 1), erange1=(-1, 0), erange2=(1, 2),
+                      tol=1e-7, conv_start=200, conv_skip=50, max_no_success=0):
+    """The reference's own block Lanczos eigenvalue pass (block_Lanczos_QR
+    and block_lanczos_blocktridiagonal of eigen/src/lanczos_blk.c, compiled
+    from its source into oracle/_ref/libref_lanczos.so by
+    oracle/build_ref.sh) from the start block r0_block (p rows of 2n doubles)
+    on the oracle's stored Hamiltonian ``o``.  Returns dict(evals, found_vb,
+    found_cb, iterations).  The routine prints progress on stdout.
+
+    Its valence window (window 1) reports W[M-i], i = 0.., of zhbevx's M
+    values (lanczos_blk.c:960-975): one entry past the values found, which
+    zhbevx leaves unset, comes first and the highest value is dropped.  Pins
+    therefore use window 2 (W[i], the lowest values of its range), placed
+    over whichever energies they test."""
+    global _REF_BLK
+    if _REF_BLK is None:
+        L = C.CDLL(REF_LANCZOS_PATH)
+        L.ref_block_lanczos.restype = C.c_int
+        L.ref_block_lanczos.argtypes = [
+            C.c_void_p, C.c_long, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
+            C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
+            C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        _REF_BLK = L
+    h = _OracleH(o.norb, o.nspin, o.natoms, _p(o.atom_slot), _p(o.nbr), _p(o.wrap),
+                 _p(o.kvec), _p(o.onsite), _p(o.blocks))
+    r0 = np.ascontiguousarray(r0_block, np.float64)
+    p = r0.shape[0]
+    ev = np.zeros(imax * p)
+    fvb = np.zeros(1, np.int32)
+    fcb = np.zeros(1, np.int32)
+    its = np.zeros(1, np.int32)
+    ne = _REF_BLK.ref_block_lanczos(
+        C.byref(h), o.n, p, _p(r0), conv_start, conv_skip, imax, req[0], req[1], erange1[0],
+        erange1[1], erange2[0], erange2[1], tol, max_no_success, _p(ev), _p(fvb), _p(fcb),
+        _p(its))
+    return dict(evals=ev[:ne].copy(), found_vb=int(fvb[0]), found_cb=int(fcb[0]),
+                iterations=int(its[0]))
+
+
 def tridiag_eigs(d, e, vl, vu, abstol=1e-13):
     d = np.ascontiguousarray(d, np.float64)
     e = np.ascontiguousarray(e, np.float64)

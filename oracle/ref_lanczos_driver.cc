@@ -1,11 +1,13 @@
 // ref_lanczos_driver.cc -- TEST AND CPU-BASELINE INFRASTRUCTURE ONLY.
 //
-// Links the reference's own Lanczos driver (eigen/src/lanczos.c, compiled
-// where it lies by oracle/build_ref.sh, with the reference's fake MPI layer
-// eigen/src/mpi_fake.c) into oracle/_ref/libref_lanczos.so, so that the CPU
-// baseline of the benchmark and the tests can run the reference's
-// eigenvaluesLanczos -- its recurrence, convergence windows, dstebz
-// bisection and ghost handling -- on a real Hamiltonian.  The H*x it calls
+// Links the reference's own Lanczos drivers (eigen/src/lanczos.c and
+// eigen/src/lanczos_blk.c, compiled where they lie by oracle/build_ref.sh,
+// with the reference's fake MPI layer eigen/src/mpi_fake.c) into
+// oracle/_ref/libref_lanczos.so, so that the CPU baseline of the benchmark
+// and the tests can run the reference's eigenvaluesLanczos -- its
+// recurrence, convergence windows, dstebz bisection and ghost handling --
+// and its block Lanczos (block_Lanczos_QR, single_iteration, the zhbevx
+// band solve and the Method-4 convergence test) on a real Hamiltonian.  The H*x it calls
 // through its matmul pointer is the oracle's restatement of the reference's
 // stored product (orc_hx, oracle/tb_oracle.c): the reference's own
 // Hmult_stored needs its XML-driven geometry set-up and is not built.
@@ -17,17 +19,30 @@
 //    before its first element; tridiagonal bands are three vectors reached
 //    through a pointer to the middle one, T[-1], T[0], T[+1]); the nml
 //    library's own sources are generated by a template tool;
-//  * LAPACK's dstebz, forwarded to the dstebz that scipy's bundled OpenBLAS
-//    exports (the reference builds its vendored Fortran LAPACK, and no
-//    Fortran compiler is present here);
-//  * the MPI rank globals of a serial run.
+//  * LAPACK's dstebz, zhbevx, zgbtrf and zgbtrs, forwarded to the routines
+//    scipy's bundled OpenBLAS exports (the reference builds its vendored
+//    Fortran LAPACK, and no Fortran compiler is present here);
+//  * ARPACK's znaupd/zneupd, which only lanczos_blk.c's eigenvector routine
+//    calls (ARPACK is not present): stubs that stop the process if reached;
+//  * the MPI rank globals of a serial run;
+//  * Allreduce_MPI_sp as a function with MPI's meaning (copy `count`
+//    doubles).  lanczos_blk.c is compiled with the reference's
+//    NoGnuStatementExpre switch, which selects this function (and the
+//    complex-pointer overload of oracle/ref_blk_compat.h): the serial
+//    build's default statement-expression macro copies `count` elements of
+//    the pointer's own type, and dot_product (lanczos_blk.c:172) passes a
+//    complex pointer with count 2 (MPI's two doubles), writing 32 bytes into
+//    the caller's 16-byte result on the stack.
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 
+#include <vector>
+
 #include "lanczos.h"
+#include "ref_blk_compat.h"
 
 extern "C" {
 #include "tb_oracle.h"
@@ -37,6 +52,15 @@ extern "C" {
 int mpi_n3d_id = 0;
 int mpi_n3d_masterid = 0;
 int mpi_n3d_numprocs = 1;
+
+void Allreduce_MPI_sp(double *pa, double *pb, int count, MPI_Datatype, MPI_Op, MPI_Comm) {
+  for (int i = 0; i < count; ++i) pb[i] = pa[i];
+}
+void Allreduce_MPI_sp(nml_dcomplex *pa, nml_dcomplex *pb, int count, MPI_Datatype d, MPI_Op o,
+                      MPI_Comm c) {
+  Allreduce_MPI_sp(reinterpret_cast<double *>(pa), reinterpret_cast<double *>(pb), count, d, o,
+                   c);
+}
 
 // ---------------------------------------------------------------- nml
 namespace {
@@ -125,6 +149,21 @@ nml_d3bands *nml_d3_clone(const nml_d3bands *p) {
   for (int k = -1; k <= 1; ++k) memcpy(q[k], p[k], sizeof(double) * m);
   return q;
 }
+void nml_dcm_delete(nml_dcmatrix *p) {
+  if (!p) return;
+  release(p[0]);
+  release(p);
+}
+void nml_dcv_delete(nml_dcvector *p) { release(p); }
+void *nml_malloc(size_t n) {
+  void *p = calloc(1, n > 0 ? n : 1);
+  if (!p) {
+    fprintf(stderr, "ref_lanczos_driver: out of memory\n");
+    exit(2);
+  }
+  return p;
+}
+void nml_free(void *p) { free(p); }
 void nml_memory_report(char *) {}
 void error(char *fmt, ...) {
   va_list ap;
@@ -148,6 +187,57 @@ extern "C" void dstebz(const char *range, const char *order, const int *n, const
   scipy_dstebz_(range, order, n, vl, vu, il, iu, abstol, d, e, m, nsplit, w, iblock, isplit,
                 work, iwork, info, 1, 1);
 }
+
+// the band solves of lanczos_blk.c (FORTRAN_UNDERSCORE names); the complex
+// type is two doubles in both
+extern "C" void scipy_zhbevx_(const char *, const char *, const char *, const int *, const int *,
+                              void *, const int *, void *, const int *, const double *,
+                              const double *, const int *, const int *, const double *, int *,
+                              double *, void *, const int *, void *, double *, int *, int *,
+                              int *, size_t, size_t, size_t);
+extern "C" void scipy_zgbtrf_(const int *, const int *, const int *, const int *, void *,
+                              const int *, int *, int *);
+extern "C" void scipy_zgbtrs_(const char *, const int *, const int *, const int *, const int *,
+                              const void *, const int *, const int *, void *, const int *, int *,
+                              size_t);
+extern "C" {
+void zhbevx_(char *jobz, char *range, char *uplo, int *n, int *kd, void *ab, int *ldab, void *q,
+             int *ldq, double *vl, double *vu, int *il, int *iu, double *abstol, int *m,
+             double *w, void *z, int *ldz, void *work, double *rwork, int *iwork, int *ifail,
+             int *info) {
+  scipy_zhbevx_(jobz, range, uplo, n, kd, ab, ldab, q, ldq, vl, vu, il, iu, abstol, m, w, z, ldz,
+                work, rwork, iwork, ifail, info, 1, 1, 1);
+}
+void zgbtrf_(int *m, int *n, int *kl, int *ku, void *ab, int *ldab, int *ipiv, int *info) {
+  scipy_zgbtrf_(m, n, kl, ku, ab, ldab, ipiv, info);
+}
+void zgbtrs_(char *trans, int *n, int *kl, int *ku, int *nrhs, void *ab, int *ldab, int *ipiv,
+             void *b, int *ldb, int *info) {
+  scipy_zgbtrs_(trans, n, kl, ku, nrhs, ab, ldab, ipiv, b, ldb, info, 1);
+}
+void znaupd_() {
+  fprintf(stderr, "ref_lanczos_driver: ARPACK znaupd is not available\n");
+  exit(4);
+}
+void zneupd_() {
+  fprintf(stderr, "ref_lanczos_driver: ARPACK zneupd is not available\n");
+  exit(4);
+}
+}
+
+// lanczos_blk.c's routines (declared there, not in a header)
+void block_Lanczos_QR(std::vector<nml_dcvector *> *R, std::vector<nml_dcvector *> *Q,
+                      nml_dcmatrix *Beta, nml_extent m, int p);
+int block_lanczos_blocktridiagonal(
+    nml_dvector *eigv_conv, nml_dcmatrix *triad, nml_extent *pIterations, int p,
+    std::vector<nml_dcvector *> *R_n, std::vector<nml_dcvector *> *Q_n,
+    std::vector<nml_dcvector *> *Q_n1, nml_extent length, int requested1, int requested2,
+    int ConvCheckStartIter, int ConvCheckSkipRate, int imax, nml_dscalar emin1,
+    nml_dscalar emax1, nml_dscalar emin2, nml_dscalar emax2, nml_dscalar tolerance,
+    nml_dscalar resolution, void (*matmul)(const int **, nml_dcscalar *, const nml_dcscalar *),
+    const int *argument[], FILE *fp_trace, FILE *fp_log, int verbose, int *tridiag_size,
+    double deflation_tolerance, int max_no_success, int *found_vb, int *found_cb,
+    int deflation_on, int conv_method);
 
 // ---------------------------------------------------------------- H*x
 // argList[0]: the oracle's stored Hamiltonian, argList[1]: &shift
@@ -200,4 +290,56 @@ extern "C" int ref_eigenvalues_lanczos(const OracleH *h, long length, const doub
   release(q_n);
   release(q_n1);
   return int(ne);
+}
+
+// The reference's block Lanczos eigenvalue pass as eigensolve_blk_lanczos
+// runs it (lanczos_blk.c:2208-2255): the start block r0 (p vectors of
+// 2*length doubles, back to back) orthonormalised by block_Lanczos_QR, then
+// block_lanczos_blocktridiagonal with resolution 100*tolerance, no
+// deflation, no trace or log files.  values[imax*p] ascending (the
+// reference sorts them), *found_vb, *found_cb, *iterations as the routine
+// leaves them; returns the number of eigenvalues.  max_no_success <= 0 means
+// no limit.  The routine prints progress lines on stdout.
+extern "C" int ref_block_lanczos(const OracleH *h, long length, int p, const double *r0,
+                                 int conv_start, int conv_skip, int imax, int requested1,
+                                 int requested2, double emin1, double emax1, double emin2,
+                                 double emax2, double tolerance, int max_no_success,
+                                 double *values, int *found_vb, int *found_cb, int *iterations) {
+  std::vector<nml_dcvector *> R_n, Q_n, Q_n1, Q_start;
+  for (int i = 0; i < p; ++i) {
+    nml_dcvector *r = nml_dcv_new(length);
+    memcpy(r, r0 + size_t(i) * 2 * length, sizeof(nml_dcscalar) * length);
+    Q_start.push_back(r);
+    R_n.push_back(nml_dcv_new(length));
+    Q_n.push_back(nml_dcv_new(length));
+    Q_n1.push_back(nml_dcv_new(length));
+  }
+  nml_dcmatrix *tri = nml_dcm_new(nml_extent(imax) * p, p + 1);
+  nml_dcmatrix *Beta = nml_dcm_new(p, p);
+  block_Lanczos_QR(&Q_start, &Q_n, Beta, length, p);
+  nml_dvector *value = nml_dv_new(nml_extent(imax) * p);
+  double shift = 0.0;
+  const int *args[3] = {reinterpret_cast<const int *>(h), reinterpret_cast<const int *>(&shift),
+                        nullptr};
+  nml_extent its = 0;
+  int tridiag_size = 0, fvb = 0, fcb = 0;
+  const int ne = block_lanczos_blocktridiagonal(
+      value, tri, &its, p, &R_n, &Q_n, &Q_n1, length, requested1, requested2, conv_start,
+      conv_skip, imax, emin1, emax1, emin2, emax2, tolerance, 100.0 * tolerance, oracle_matmul,
+      args, nullptr, nullptr, 0, &tridiag_size, 0.0,
+      max_no_success > 0 ? max_no_success : (1 << 30), &fvb, &fcb, 0, 4);
+  for (int k = 0; k < ne; ++k) values[k] = value[k];
+  *found_vb = fvb;
+  *found_cb = fcb;
+  *iterations = int(its);
+  nml_dv_delete(value);
+  nml_dcm_delete(tri);
+  nml_dcm_delete(Beta);
+  for (int i = 0; i < p; ++i) {
+    release(R_n[i]);
+    release(Q_n[i]);
+    release(Q_n1[i]);
+    release(Q_start[i]);
+  }
+  return ne;
 }

@@ -122,3 +122,40 @@ def test_block_lanczos_eigenvectors(model, cube, p):
         assert np.linalg.norm(r) < 1e-4 * max(1.0, abs(lam)), lam
     G = V.conj() @ V.T
     assert np.abs(G - np.eye(len(V))).max() < 1e-6
+
+
+@pytest.mark.parametrize("model,cube,p,skip", [("sp3s*", 3, 3, 10), ("sp3s*_so", 2, 4, 20),
+                                               ("sp3d5s*_so", 2, 8, 10)])
+@pytest.mark.parametrize("dots", [0, 1])
+def test_block_lanczos_matches_reference_code(model, cube, p, skip, dots):
+    """The GPU block Lanczos against the reference's own block Lanczos
+    (block_Lanczos_QR + block_lanczos_blocktridiagonal of
+    eigen/src/lanczos_blk.c, compiled from its source into
+    oracle/_ref/libref_lanczos.so) on the oracle's H*x, from the same start
+    block, with the block dots on the CUDA cores (0) and on the tensor cores
+    (1): the same number of values found, the same distinct values within
+    the convergence tolerance (1e-7 eV), the same number of block steps
+    within one convergence check.  The lowest and highest parts of the
+    spectrum go through the reference's second window (its first reads one
+    entry past zhbevx's values, lanczos_blk.c:960-975)."""
+    if not oracle.ref_lanczos_available():
+        pytest.skip("oracle/_ref/libref_lanczos.so not built (reference sources absent)")
+    fam = "spds" if model.startswith("sp3d5s") else "sps"
+    g, o = _case(model, workloads.gaas_cube(cube), [materials.MATERIALS[f"GaAs_{fam}"]])
+    g.set_block_dots(dots)
+    ev = np.linalg.eigvalsh(o.dense())
+    r0 = np.random.default_rng(11).uniform(-1, 1, size=(p, 2 * g.n))
+    for win in ((ev[0] - 0.5, ev[0] + 1.0), (ev[-1] - 1.0, ev[-1] + 0.5)):
+        kw = dict(imax=min(300, g.n // p - 2), ConvCheckStartIter=30, ConvCheckSkipRate=skip,
+                  tolerance=1e-7)
+        res = g.eigensolve_blk_lanczos(r0, requested1=0, requested2=3, emin1=0.0, emax1=0.0,
+                                       emin2=win[0], emax2=win[1], **kw)
+        ref = oracle.ref_block_lanczos(o, r0, imax=kw["imax"], req=(0, 3), erange1=(0.0, 0.0),
+                                       erange2=win, tol=1e-7, conv_start=30, conv_skip=skip)
+        print(model, p, dots, win, "gpu", res["iterations"], res["values"], "ref",
+              ref["iterations"], ref["evals"])
+        assert (res["found_vb"], res["found_cb"]) == (ref["found_vb"], ref["found_cb"])
+        for u, v in ((res["values"], ref["evals"]), (ref["evals"], res["values"])):
+            assert max(np.abs(v - x).min() for x in u) < 1e-7
+        assert abs(res["iterations"] - ref["iterations"]) <= skip
+    g.set_block_dots(0)

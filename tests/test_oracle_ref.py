@@ -218,3 +218,39 @@ def test_oracle_lanczos_matches_reference_lanczos(case):
     assert np.abs(ref["evals"] - got["evals"]).max() < 1e-10
     assert ref["iterations"] == got["iterations"]
     assert np.abs(ref["conv_it"] - got["conv_it"]).max() <= kw["conv_skip"]
+
+
+@pytest.mark.parametrize("model,cube,p,skip", [("sp3s*", 3, 3, 10), ("sp3s*_so", 2, 4, 20),
+                                               ("sp3d5s*_so", 2, 8, 10)])
+def test_oracle_block_lanczos_matches_reference(model, cube, p, skip):
+    """The oracle's restatement of the block Lanczos (oracle.block_lanczos)
+    against the reference's own block_Lanczos_QR + block_lanczos_blocktridiagonal
+    (eigen/src/lanczos_blk.c, compiled from its source into
+    oracle/_ref/libref_lanczos.so), both on the oracle's H*x from the same
+    start block: the same number of block steps and of values found, each
+    value within the convergence tolerance (1e-7 eV: the Method-4 test
+    accepts a value once it moved less than that between two checks, and the
+    value reported is the one at that check).  Both the lowest and the
+    highest part of the spectrum are searched through the reference's second
+    window (its first reads one entry past zhbevx's values)."""
+    if not O.ref_lanczos_available():
+        pytest.skip("oracle/_ref/libref_lanczos.so not built (reference sources absent)")
+    from nemo3d_b200 import workloads as W
+    fam = "spds" if model.startswith("sp3d5s") else "sps"
+    norb, nspin = M.BAND_MODELS[model]
+    o = O.OracleHamiltonian(W.gaas_cube(cube), norb, nspin, [M.MATERIALS[f"GaAs_{fam}"]])
+    ev = np.linalg.eigvalsh(o.dense())
+    r0 = np.random.default_rng(11).uniform(-1, 1, size=(p, 2 * o.n))
+
+    def hx(q):
+        y = o.hx(np.column_stack([q.real, q.imag]).ravel())
+        return y[0::2] + 1j * y[1::2]
+
+    for win in ((ev[0] - 0.5, ev[0] + 1.0), (ev[-1] - 1.0, ev[-1] + 0.5)):
+        kw = dict(imax=min(300, o.n // p - 2), req=(0, 3), erange1=(0.0, 0.0), erange2=win,
+                  tol=1e-7, conv_start=30, conv_skip=skip)
+        ref = O.ref_block_lanczos(o, r0, **kw)
+        got = O.block_lanczos(hx, r0, **kw)
+        assert (ref["found_vb"], ref["found_cb"]) == (got["found_vb"], got["found_cb"]) == (0, 3)
+        assert ref["iterations"] == got["iterations"]
+        assert np.abs(np.sort(ref["evals"]) - np.sort(got["evals"])).max() < 1e-7
