@@ -310,6 +310,7 @@ def run_ours(args, rank, world, local_rank):
         if precision == 32:
             H.set_spmv_variant(MIXED_VARIANT)
             H.set_eigenvector_pass(*MIXED_VEC_PASS)
+            H.set_mixed_acceptance(args.mixed_accept)
         else:
             H.set_spmv_variant(args.spmv_variant)
         H.build()
@@ -354,26 +355,37 @@ def run_ours(args, rank, world, local_rank):
         rf, sf = solve(64, Vf)
         f1.record(stream)
         torch.cuda.synchronize()
-        fp64 = dict(res=rf, stats=sf, s=max_over_ranks(f0.elapsed_time(f1) / 1e3, dist, "cuda"))
-        del Vf
-        torch.cuda.empty_cache()
+        fp64 = dict(res=rf, stats=sf, s=max_over_ranks(f0.elapsed_time(f1) / 1e3, dist, "cuda"),
+                    V=Vf)
 
     # FP64 residual ||H v - lambda v|| of each returned eigenpair through the
-    # recomputed double-precision product (independent of the stored blocks)
-    resid = []
+    # recomputed double-precision product (independent of the stored blocks),
+    # for this solve and for the plain FP64 one
+    resid, resid64 = [], []
     if not args.no_residuals:
         Hr = tbgpu.Hamiltonian(st, "sp3d5s*_so", MATS, build=False, recompute=True,
                                device_inputs=(types_d.data_ptr(), dsp_d.data_ptr()))
         Hr.build()
         y = torch.empty(2 * n, dtype=torch.float64, device="cuda")
-        for e, lam in enumerate(res["values"][:nvec]):
-            v = V_d[e * 2 * n:(e + 1) * 2 * n]
-            Hr.hx_dev(v.data_ptr(), y.data_ptr(), float(lam))
-            torch.cuda.synchronize()
-            resid.append(float(torch.linalg.vector_norm(y).item() /
-                               torch.linalg.vector_norm(v).item()))
+
+        def residuals(values, V):
+            out = []
+            for e, lam in enumerate(values[:nvec]):
+                v = V[e * 2 * n:(e + 1) * 2 * n]
+                Hr.hx_dev(v.data_ptr(), y.data_ptr(), float(lam))
+                torch.cuda.synchronize()
+                out.append(float(torch.linalg.vector_norm(y).item() /
+                                 torch.linalg.vector_norm(v).item()))
+            return out
+
+        resid = residuals(res["values"], V_d)
+        if fp64 is not None:
+            resid64 = residuals(fp64["res"]["values"], fp64["V"])
         Hr.close()
         del y
+    if fp64 is not None:
+        del fp64["V"]
+        torch.cuda.empty_cache()
 
     # end to end through the host-pointer C ABI
     e2e_s = None
@@ -389,6 +401,7 @@ def run_ours(args, rank, world, local_rank):
             if mixed:
                 H.set_spmv_variant(MIXED_VARIANT)
                 H.set_eigenvector_pass(*MIXED_VEC_PASS)
+                H.set_mixed_acceptance(args.mixed_accept)
             else:
                 H.set_spmv_variant(args.spmv_variant)
             out = H.eigensolve_lanczos(r0_h, vectors=nvec, **solve_kw)  # host r0 in, vectors out
@@ -422,12 +435,16 @@ def run_ours(args, rank, world, local_rank):
                "residual_per_state_ev": resid, "tolerance": solve_kw["tolerance"]}
         if mixed:
             cfg["refine_residual_per_state_ev"] = [float(v) for v in res["state_resid"]]
+            cfg["mixed_acceptance_floor"] = (
+                args.mixed_accept if args.mixed_accept >= 0 else
+                "2^-24 x Gershgorin bound of T (complex-float rounding level)")
         if fp64 is not None:
             cfg["fp64_plain"] = {
                 "s": fp64["s"], "iterations_first_pass": int(fp64["res"]["iterations"]),
                 "first_pass_ms": fp64["stats"]["solve_ms"],
                 "vectors_ms": fp64["stats"]["vectors_ms"],
-                "eigenvalues": [round(float(v), 12) for v in fp64["res"]["values"]]}
+                "eigenvalues": [round(float(v), 12) for v in fp64["res"]["values"]],
+                "residual_per_state_ev": resid64}
             cfg["speedup_vs_fp64_plain"] = fp64["s"] / (ms / 1e3)
             cfg["error_per_state_ev_vs_fp64"] = _match_states(res["values"], fp64["res"]["values"])
         line = {
@@ -811,6 +828,11 @@ def main():
                     help="with --profile-case: a few Keating VFF iterations instead")
     ap.add_argument("--spmv-variant", type=int, default=0, choices=[0, 1, 2, 3, 4, 5, 6],
                     help="H*x kernel of the solve (tbgpu_set_spmv_variant)")
+    ap.add_argument("--mixed-accept", type=float, default=-1.0,
+                    help="mixed solve: floor of the convergence test's bound on the last "
+                         "components of a tridiagonal eigenvector (0: the tolerance; "
+                         "negative, the default: 2^-24 x the Gershgorin bound of T, the "
+                         "complex-float rounding level)")
     ap.add_argument("--mixed-recompute", action="store_true",
                     help="--workload mixed2M: also the mixed solve on the recompute product")
     ap.add_argument("--warm-train", type=int, default=64,

@@ -302,6 +302,22 @@ int tbgpu_block_dots_dev(tbgpu_ctx *ctx, int p, const double *x_dev, const doubl
  * of tbgpu_block_dots_dev.  TBGPU_E_ARG for another mode. */
 int tbgpu_set_block_dots(tbgpu_ctx *ctx, int mode);
 
+/* Mixed-precision Lanczos (tbgpu_set_lanczos_precision(32)): floor of the
+ * bound on the last two components of a tridiagonal eigenvector below which
+ * the convergence test accepts its Ritz value (the test of lanczos.c's
+ * eigenvaluesLanczos uses the solve's tolerance; the complex-float
+ * recurrence cannot drive those components below its rounding level, so
+ * with a tolerance under that level it accepts values late or not at all).
+ * The accepted values are refined in double precision (Rayleigh-Ritz over
+ * the double product) and tbgpu_get_state_errors reports their residuals.
+ * floor < 1; 0 (default) keeps the tolerance; a negative floor sets it at
+ * every check to 2^-24 times the Gershgorin bound of the
+ * tridiagonal matrix so far (max_i |alpha_i| + |beta_i| + |beta_i-1|), the
+ * rounding level of the complex-float vectors relative to ||H||.  The bound
+ * used is max(tolerance, floor).  Double-precision solves ignore it.
+ * TBGPU_E_ARG for floor >= 1, NaN or -infinity. */
+int tbgpu_set_mixed_acceptance(tbgpu_ctx *ctx, double floor);
+
 /* Tridiagonal matrix of the last solve: alpha[n], beta[n] (n <= cap). */
 int tbgpu_get_tridiagonal(const tbgpu_ctx *ctx, double *alpha, double *beta,
                           int cap);

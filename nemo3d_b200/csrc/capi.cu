@@ -713,6 +713,13 @@ int tbgpu_set_eigenvector_pass(tbgpu_ctx *ctx, int mode, int columns, int segmen
   return TBGPU_OK;
 }
 
+int tbgpu_set_mixed_acceptance(tbgpu_ctx *ctx, double floor) {
+  if (!ctx || !(floor < 1.0) || !(floor > -HUGE_VAL)) return set_error(TBGPU_E_ARG);
+  if (floor < 0.0) floor = -1.0;  // the automatic floor
+  C(ctx)->mixed_accept = floor;
+  return TBGPU_OK;
+}
+
 int tbgpu_set_block_dots(tbgpu_ctx *ctx, int mode) {
   if (!ctx || mode < 0 || mode > 1) return set_error(TBGPU_E_ARG);
   C(ctx)->block_dots = mode;

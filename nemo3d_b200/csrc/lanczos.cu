@@ -723,6 +723,21 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
   std::vector<int> i1, i2;
   Rng rng{0x9E3779B97F4A7C15ULL};  // starts of the eigenvector inverse iterations
   const double res = 100.0 * A.tol;
+  // the acceptance bound on a tridiagonal eigenvector's last components;
+  // the complex-float recurrence may raise it to its own rounding floor: a
+  // set floor, or (negative setting) 2^-24 times the Gershgorin bound of the
+  // tridiagonal matrix so far, the recurrence's rounding level
+  auto accept_bound = [&](int at, const double *al, const double *be) {
+    if (!kMixed || c.mixed_accept == 0.0) return A.tol;
+    double floor = c.mixed_accept;
+    if (floor < 0.0) {
+      double g = 0.0;
+      for (int i = 0; i < at; i++)
+        g = std::max(g, std::fabs(al[i]) + std::fabs(be[i]) + (i > 0 ? std::fabs(be[i - 1]) : 0.0));
+      floor = std::ldexp(g, -24);
+    }
+    return std::max(A.tol, floor);
+  };
   // check points exactly as lanczos_tridiagonal's skip counter places them
   auto next_check = [&](int after, int skip_at_after) {
     int skip = skip_at_after;
@@ -835,11 +850,12 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
         cleanup();
         return set_error(TBGPU_E_NUMERIC);
       }
+    const double tol_acc = accept_bound(p.at, Ta.data(), Tb.data());
     if (A.req1 > 0 && int(c1.size()) <= A.req1)
-      check_window(p.at, Ta.data(), Tb.data(), A.emin1, A.emax1, A.tol, res, c1, i1,
+      check_window(p.at, Ta.data(), Tb.data(), A.emin1, A.emax1, tol_acc, res, c1, i1,
                    0x51ED27ULL * p.at + 1);
     if (A.req2 > 0 && int(c2.size()) <= A.req2)
-      check_window(p.at, Ta.data(), Tb.data(), A.emin2, A.emax2, A.tol, res, c2, i2,
+      check_window(p.at, Ta.data(), Tb.data(), A.emin2, A.emax2, tol_acc, res, c2, i2,
                    0x51ED27ULL * p.at + 2);
     const bool more = (p.at + 1 < A.imax) &&
                       (int(c1.size()) < A.req1 || int(c2.size()) < A.req2);

@@ -139,6 +139,10 @@ struct Ctx {
   // block Lanczos dots: 0 = double-precision CUDA-core kernel, 1 = the
   // tensor-core (tcgen05 kind::i8 slice) kernel
   int block_dots = 0;
+  // mixed-precision recurrence: floor of the bound on the last components of
+  // a tridiagonal eigenvector that accepts its Ritz value (0: the caller's
+  // tolerance, as in double precision)
+  double mixed_accept = 0.0;
   // folded-spectrum operator F = factor (H - s2)(H - s1) + offset of
   // matvect_mult2 (nemo3d/src/base/h_cvectr_mult.c:156-198; its constants
   // by default); fold on: the Lanczos solves run on F

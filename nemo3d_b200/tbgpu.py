@@ -85,6 +85,7 @@ def _lib():
         L.tbgpu_hx_block_dev.argtypes = [vp, ip, dp, vp, vp]
         L.tbgpu_block_dots_dev.argtypes = [vp, ip, vp, vp, C.c_long, vp]
         L.tbgpu_set_block_dots.argtypes = [vp, ip]
+        L.tbgpu_set_mixed_acceptance.argtypes = [vp, dp]
         L.tbgpu_eigensolve_blk_lanczos.argtypes = [vp, ip, ip, ip, ip, ip, dp, dp, dp, dp, dp,
                                                    ip, ip, vp, vp, vp, vp, vp, vp, ip]
         L.tbgpu_ctx_create.argtypes = [C.POINTER(_Geom), C.POINTER(_Model), C.POINTER(vp)]
@@ -299,6 +300,15 @@ class Hamiltonian:
         if rc:
             raise TbgpuError(rc, "tbgpu_block_dots_dev")
         return (G[0::2] + 1j * G[1::2]).reshape(p, p)
+
+    def set_mixed_acceptance(self, floor: float):
+        """Mixed-precision solves: floor of the bound on the last components
+        of a tridiagonal eigenvector that accepts its Ritz value (0: the
+        solve's tolerance; negative: 2^-24 times the Gershgorin bound of the
+        tridiagonal matrix, the complex-float rounding level)."""
+        rc = _lib().tbgpu_set_mixed_acceptance(self._ctx, float(floor))
+        if rc:
+            raise TbgpuError(rc, "tbgpu_set_mixed_acceptance")
 
     def set_block_dots(self, mode: int):
         """Block Lanczos dots on the CUDA cores in double (0) or on the tensor
