@@ -432,6 +432,9 @@ def run_ours(args, rank, world, local_rank):
                "build_ms": last["build_ms"], "solve_ms": last["solve_ms"],
                "vectors_ms": last["vectors_ms"], "refine_ms": last["refine_ms"],
                "vec_segments": last["vec_segments"], "vec_mismatch": last["vec_mismatch"],
+               "hx_avg_ms": spmv_ms,
+               "update_avg_ms": last["update_ms"] / max(last["spmv_launches"], 1),
+               "host_check_ms": last["check_ms"], "host_wait_ms": last["wait_ms"],
                "residual_per_state_ev": resid, "tolerance": solve_kw["tolerance"]}
         if mixed:
             cfg["refine_residual_per_state_ev"] = [float(v) for v in res["state_resid"]]

@@ -540,6 +540,10 @@ typedef struct {
   long vec_segments;          /* eigenvector pass 1: segments regenerated     */
   long vec_mismatch;          /* ... whose last vector differed, bit for bit, */
                               /* from the first pass's checkpoint (0 expected) */
+  double update_ms;           /* sum over the recurrence's update launches     */
+                              /* (when profiling on)                           */
+  double check_ms;            /* host time in the convergence tests            */
+  double wait_ms;             /* host time waiting for the GPU's check batches */
 } tbgpu_stats;
 int tbgpu_set_profiling(tbgpu_ctx *ctx, int on);
 

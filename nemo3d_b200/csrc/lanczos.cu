@@ -18,6 +18,7 @@
 // reference.  Eigenvectors: second pass (eigenvectorsLanczos, method 3,
 // lanczos.c:1364-1689) with the Ritz combination accumulated in chunks of
 // iterations (k_accum) rather than one axpy per eigenvector per iteration.
+#include <chrono>
 #include <algorithm>
 #include <atomic>
 #include <thread>
@@ -544,6 +545,11 @@ static int spmv_step(Ctx &c, const float2 *x, float2 *y, const double *bet, int 
                          bet, it, alpha, it, s);
 }
 
+// check batches the first pass keeps queued ahead of the host's convergence
+// test: the iterations past convergence that run for nothing (at most
+// kAhead * ConvCheckSkipRate) against the GPU idling while a test runs
+constexpr int kAhead = 4;
+
 template <typename VT>
 static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *values,
                    int *conv_iters, int *iterations, double *V_dev, int maxvec) {
@@ -556,6 +562,9 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
   c.stats.refine_ms = 0.0;
   c.stats.vec_segments = 0;
   c.stats.vec_mismatch = 0;
+  c.stats.update_ms = 0.0;
+  c.stats.check_ms = 0.0;
+  c.stats.wait_ms = 0.0;
   // eigenvector pass by regeneration (tbgpu_set_eigenvector_pass): both
   // passes run a register-streaming kernel whose columns compute as
   // one-column launches -- the pencil kernel when variant 6 is set and
@@ -591,7 +600,7 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
   VT *W = nullptr;
   double *d_alpha = nullptr, *d_bet = nullptr, *d_tmp = nullptr;
   double *h_alpha = nullptr, *h_bet = nullptr;
-  std::vector<cudaEvent_t> spmv_ev;
+  std::vector<cudaEvent_t> spmv_ev, upd_ev;
   // regeneration: the first pass saves r_it and r_{it-1} at every it = 0,
   // L, 2L, ...
   const int L = std::max(c.vec_segment, 16);
@@ -629,6 +638,7 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
     if (h_alpha) cudaFreeHost(h_alpha);
     if (h_bet) cudaFreeHost(h_bet);
     for (auto e : spmv_ev) cudaEventDestroy(e);
+    for (auto e : upd_ev) cudaEventDestroy(e);
   };
 #define SOLVE_CUDA(call)                 \
   do {                                   \
@@ -651,8 +661,8 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
   SOLVE_CUDA(cudaMalloc(&d_alpha, sizeof(double) * (A.imax + 1)));
   SOLVE_CUDA(cudaMalloc(&d_bet, sizeof(double) * (A.imax + 2)));
   SOLVE_CUDA(cudaMalloc(&d_tmp, sizeof(double) * 4));
-  SOLVE_CUDA(cudaMallocHost(&h_alpha, sizeof(double) * (A.imax + 2) * 3));
-  SOLVE_CUDA(cudaMallocHost(&h_bet, sizeof(double) * (A.imax + 2) * 3));
+  SOLVE_CUDA(cudaMallocHost(&h_alpha, sizeof(double) * (A.imax + 2) * (kAhead + 1)));
+  SOLVE_CUDA(cudaMallocHost(&h_bet, sizeof(double) * (A.imax + 2) * (kAhead + 1)));
   Timers tm;
   cudaEventCreate(&tm.t0);
   cudaEventCreate(&tm.t1);
@@ -712,6 +722,12 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
     }
     k_update<VT><<<rg, kRedThreads, 0, s>>>(n2, W, rc_, it > 0 ? rp_ : nullptr, ro, d_alpha, bet,
                                             it, c.d_partial, c.d_counter);
+    if (c.profiling) {
+      cudaEvent_t e2 = nullptr;
+      cudaEventCreate(&e2);
+      cudaEventRecord(e2, s);
+      upd_ev.push_back(e2);  // the update runs from e1 to e2
+    }
     launches += 2;
     return cudaGetLastError() == cudaSuccess ? TBGPU_OK : set_error(TBGPU_E_CUDA);
   };
@@ -750,9 +766,9 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
   // all check points below the iteration limit
   std::vector<int> checks;
   for (int at = next_check(0, 0); at < A.imax; at = next_check(at, 0)) checks.push_back(at);
-  // The GPU runs up to kAhead check batches ahead of the host's test; each
-  // check in flight copies alpha/beta into its own pinned slot.
-  constexpr int kAhead = 2;
+  // The GPU runs up to kAhead check batches ahead of the host's test (a
+  // file-scope constant); each check in flight copies alpha/beta into its
+  // own pinned slot.
   const size_t slot = size_t(A.imax) + 2;
   int launched = 0;  // iterations enqueued
   int final_it = -1;
@@ -765,12 +781,22 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
   // after the step that wrote them, before any step overwrites them); when
   // device memory runs short the solve falls back to the second run
   const size_t ring_need = size_t(P) * (kRegenRows / P + 2) * vbytes + (512ull << 20);
+  // free device memory is read once, at the first checkpoint; the pass
+  // allocates nothing else, so the checkpoints draw on that budget
+  size_t ck_budget = 0;
+  bool ck_budget_read = false;
   auto checkpoint = [&](int it) -> int {
-    size_t fre = 0, tot = 0;
-    cudaMemGetInfo(&fre, &tot);
+    if (!ck_budget_read) {
+      size_t fre = 0, tot = 0;
+      cudaMemGetInfo(&fre, &tot);
+      ck_budget = fre > ring_need ? fre - ring_need : 0;
+      ck_budget_read = true;
+    }
+    const size_t need = (it > 0 ? 2 : 1) * vbytes;
     VT *a = nullptr, *b = nullptr;
-    bool ok = fre > 2 * vbytes + ring_need && cudaMallocAsync(&a, vbytes, s) == cudaSuccess;
+    bool ok = ck_budget > 2 * vbytes && cudaMallocAsync(&a, vbytes, s) == cudaSuccess;
     if (ok && it > 0) ok = cudaMallocAsync(&b, vbytes, s) == cudaSuccess;
+    if (ok) ck_budget -= need;
     if (!ok) {
       cudaGetLastError();  // a failed allocation is not an error of the solve
       if (a) cudaFreeAsync(a, s);
@@ -839,7 +865,10 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
   while (!pend.empty()) {
     Pending p = pend.front();
     pend.erase(pend.begin());
+    const auto w0 = std::chrono::steady_clock::now();
     SOLVE_CUDA(cudaEventSynchronize(p.ev));
+    const auto w1 = std::chrono::steady_clock::now();
+    c.stats.wait_ms += std::chrono::duration<double, std::milli>(w1 - w0).count();
     cudaEventDestroy(p.ev);
     const double *ha = h_alpha + p.slot * slot, *hb = h_bet + p.slot * slot;
     Ta.assign(ha, ha + p.at);
@@ -850,6 +879,7 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
         cleanup();
         return set_error(TBGPU_E_NUMERIC);
       }
+    const auto k0 = std::chrono::steady_clock::now();
     const double tol_acc = accept_bound(p.at, Ta.data(), Tb.data());
     if (A.req1 > 0 && int(c1.size()) <= A.req1)
       check_window(p.at, Ta.data(), Tb.data(), A.emin1, A.emax1, tol_acc, res, c1, i1,
@@ -857,6 +887,8 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
     if (A.req2 > 0 && int(c2.size()) <= A.req2)
       check_window(p.at, Ta.data(), Tb.data(), A.emin2, A.emax2, tol_acc, res, c2, i2,
                    0x51ED27ULL * p.at + 2);
+    c.stats.check_ms +=
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - k0).count();
     const bool more = (p.at + 1 < A.imax) &&
                       (int(c1.size()) < A.req1 || int(c2.size()) < A.req2);
     if (!more) {
@@ -1118,6 +1150,13 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
     }
     c.stats.spmv_ms = tot;
     c.stats.spmv_launches = long(spmv_ev.size() / 2);
+    double upd = 0.0;
+    for (size_t k = 0; k < upd_ev.size() && 2 * k + 1 < spmv_ev.size(); k++) {
+      float t = 0.f;
+      cudaEventElapsedTime(&t, spmv_ev[2 * k + 1], upd_ev[k]);
+      upd += t;
+    }
+    c.stats.update_ms = upd;
   }
   c.stats.kernel_launches = launches;
   cudaEventDestroy(tm.t0);

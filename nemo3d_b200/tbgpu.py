@@ -49,7 +49,8 @@ class Stats(C.Structure):
                 ("vectors_ms", C.c_double), ("spmv_ms", C.c_double),
                 ("spmv_launches", C.c_long), ("lanczos_iterations", C.c_long),
                 ("kernel_launches", C.c_long), ("refine_ms", C.c_double),
-                ("vec_segments", C.c_long), ("vec_mismatch", C.c_long)]
+                ("vec_segments", C.c_long), ("vec_mismatch", C.c_long),
+                ("update_ms", C.c_double), ("check_ms", C.c_double), ("wait_ms", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
