@@ -1,6 +1,6 @@
 """Benchmark: seconds to 8 band-edge eigenpairs of a ~2.0M-atom InAs dot.
 
-Workload (the headline, configuration 3 of the target): InAs lens (base
+Workload (the headline): InAs lens (base
 20 nm, height 5 nm) on a one-monolayer InAs wetting layer in a GaAs box of
 72 x 72 x 48 cells (1,990,656 atoms), sp3d5s* with spin-orbit (20 orbitals
 per atom, H of dimension 39,813,120), dangling bonds passivated (+30 eV),
@@ -21,11 +21,22 @@ eigenvectors copied out).  The same run times the plain FP64 GPU Lanczos
 recurrence for the eigenvectors) on the same dot once, and reports the ratio,
 the per-state eigenvalue difference and the FP64 residual ||Hv - lambda v||
 of each mixed eigenpair through the recomputed double-precision product (a
-product independent of the stored blocks).  ``--workload dome1M`` is
-configuration 2 (1,022,656 atoms, plain FP64, 8 electron + 8 hole states).
-``--impl reference`` times the CPU oracle (a plain-C restatement of the
-reference's H*x and Lanczos recurrence, OpenMP over the host cores) on a
-bounded sample of iterations and scales it to a full solve.
+product independent of the stored blocks).  ``--workload dome1M`` is the
+1,022,656-atom dome (58 x 58 x 38 cells), plain FP64, 8 electron + 8 hole
+states.
+``--impl reference`` times the reference's own first Lanczos pass
+(eigenvaluesLanczos of eigen/src/lanczos.c, compiled from its source into
+oracle/_ref by oracle/build_ref.sh, running on the oracle's plain-C
+restatement of the FP64 stored H*x with OpenMP over the host cores; the
+oracle alone where that library is absent) on a bounded sample of iterations
+per step and scales it to a full plain FP64 solve (both passes).
+
+The mixed solve's convergence test bounds the tridiagonal eigenvector's last
+components by max(tolerance, 2^-24 x the Gershgorin bound of T) -- the
+rounding level of the complex-float recurrence (``--mixed-accept``; 0 gives
+the tolerance alone, as the FP64 solve uses): values are then refined in
+FP64, and the line carries each state's difference from the FP64 solve and
+both solves' FP64 residuals.
 """
 
 from __future__ import annotations
@@ -63,7 +74,7 @@ SOLVE = dict(ConvCheckStartIter=200, ConvCheckSkipRate=50, imax=20000,
              requested1=4, requested2=4, emin1=1.032, emax1=1.06,
              emin2=1.44, emax2=1.475, tolerance=1e-7)
 NVEC = 8
-# configuration 2: 8 hole and 8 electron states of the 1.02M-atom dome
+# the 1.02M-atom dome: 8 hole and 8 electron states
 SOLVE_8X8 = dict(SOLVE, requested1=8, requested2=8, emin1=0.95, emax1=1.06, emin2=1.44,
                  emax2=1.56, imax=30000)
 # the mixed-precision solver: float store and vectors, H*x variant 5 (lane
@@ -283,11 +294,11 @@ def run_ours(args, rank, world, local_rank):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=torch.device("cuda", local_rank))
-    cfg2 = args.workload == "dome1M"
-    cells = (58, 58, 38) if cfg2 else (72, 72, 48)
-    solve_kw = SOLVE_8X8 if cfg2 else SOLVE
-    nvec = 16 if cfg2 else NVEC
-    mixed = not cfg2
+    dome1m = args.workload == "dome1M"
+    cells = (58, 58, 38) if dome1m else (72, 72, 48)
+    solve_kw = SOLVE_8X8 if dome1m else SOLVE
+    nvec = 16 if dome1m else NVEC
+    mixed = not dome1m
     bits = 32 if mixed else 64
     st = make_structure(cells)
     types_d = torch.from_numpy(np.ascontiguousarray(st.types).reshape(-1)).cuda()
@@ -556,12 +567,54 @@ def run_extra(args):
               In(x)Ga(1-x)As lens dots (20 x 20 x 14 cells, 44,800 sites,
               sp3d5s*+SO, 4 h + 4 e levels with vectors) as training data,
               the network trained on them, then --warm-test held-out seeds
-              solved cold and warm: iterations and wall time of each"""
+              solved cold and warm: iterations and wall time of each
+    bdots     block dots G = X^H Y of two blocks of 8 vectors, on the tensor
+              cores (tbgpu_block_dots_dev; error against torch's complex
+              matrix product), and 40 block Lanczos steps (p = 8) of a GaAs cube of
+              --bdots-cube^3 cells with the CUDA-core and the tensor-core dots"""
     import torch
     from nemo3d_b200 import tbgpu
     torch.cuda.set_device(0)
     w = args.workload
-    if w == "kernels":
+    if w == "bdots":
+        st = workloads.gaas_cube(args.bdots_cube)
+        g = tbgpu.Hamiltonian(st, "sp3d5s*_so", [materials.MATERIALS["GaAs_spds"]])
+        n2, p = g.n, 8
+        gen = torch.Generator(device="cuda").manual_seed(7)
+        X = torch.randn(p, 2 * n2, dtype=torch.float64, device="cuda", generator=gen)
+        Y = torch.randn(p, 2 * n2, dtype=torch.float64, device="cuda", generator=gen)
+        for _ in range(3):
+            G = g.block_dots_dev(p, X.data_ptr(), Y.data_ptr(), n2)
+        torch.cuda.synchronize()
+        reps = 20
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            G = g.block_dots_dev(p, X.data_ptr(), Y.data_ptr(), n2)
+        dt = (time.perf_counter() - t0) / reps
+        Xc = torch.view_as_complex(X.view(p, n2, 2))
+        Yc = torch.view_as_complex(Y.view(p, n2, 2))
+        ref = (Xc.conj() @ Yc.T).cpu().numpy()
+        norms = torch.linalg.vector_norm(X, dim=1).cpu().numpy()
+        err = float(np.abs(G - ref).max() / norms.max() ** 2)
+        r0 = np.random.default_rng(1).uniform(-1, 1, size=(p, 2 * n2))
+        kw = dict(imax=40, requested1=3, requested2=3, emin1=-1.5, emax1=0.5, emin2=1.0,
+                  emax2=3.5, tolerance=1e-7, ConvCheckStartIter=1000, ConvCheckSkipRate=50)
+        steps = {}
+        for mode in (0, 1):
+            g.set_block_dots(mode)
+            g.eigensolve_blk_lanczos(r0, **dict(kw, imax=5))
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            res = g.eigensolve_blk_lanczos(r0, **kw)
+            torch.cuda.synchronize()
+            steps[mode] = dict(steps=int(res["iterations"]), s=time.perf_counter() - t0)
+        g.close()
+        print(json.dumps({"workload": "bdots", "natoms": st.nsites, "n2": n2, "p": p,
+                          "block_dots_dev_wall_ms": dt * 1e3,
+                          "max_error_rel_to_norm2": err,
+                          "block_lanczos_cuda_core": steps[0],
+                          "block_lanczos_tensor_core": steps[1]}), flush=True)
+    elif w == "kernels":
         st = make_structure((58, 58, 38))
         for name, opts, f32, var in (
                 ("fp64 store", {}, False, 0),
@@ -843,10 +896,13 @@ def main():
     ap.add_argument("--warm-test", type=int, default=16, help="--workload warm: held-out dots")
     ap.add_argument("--warm-epochs", type=int, default=300, help="--workload warm: epochs")
     ap.add_argument("--workload", default="dot2M",
-                    choices=["dot2M", "dome1M", "kernels", "mixed2M", "batch256", "vff1M", "warm"],
+                    choices=["dot2M", "dome1M", "kernels", "mixed2M", "batch256", "vff1M", "warm",
+                             "bdots"],
                     help="dot2M: the headline bench (mixed precision, 1,990,656 atoms); "
                          "dome1M: plain FP64, 8 e + 8 h on 1,022,656 atoms; the others: "
                          "measurements beside it")
+    ap.add_argument("--bdots-cube", type=int, default=24,
+                    help="--workload bdots: GaAs cube edge in cells")
     ap.add_argument("--ref-iterations", type=int, default=19802,
                     help="iterations of a full solve (both passes of the plain FP64 method) "
                          "the CPU sample is scaled to")

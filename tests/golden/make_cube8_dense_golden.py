@@ -9,7 +9,7 @@ below 2.0 eV are kept.  The GPU
 test checks that the Lanczos solve for the 8 eigenvalues nearest 1.6 eV
 returns the 8 nearest distinct values of this list.
 
-Writes tests/golden/cfg1_dense.npz (under 2 kB).  Takes a few
+Writes tests/golden/cube8_sp3s_dense.npz (under 2 kB).  Takes a few
 minutes and ~12 GB of host memory.
 """
 import os
@@ -41,7 +41,7 @@ def main():
     w = sl.eigh(hr, eigvals_only=True, subset_by_value=WINDOW, driver="evr",
                 overwrite_a=True, check_finite=False)
     w = np.sort(w)
-    np.savez_compressed(os.path.join(HERE, "cfg1_dense.npz"), eigenvalues=w[w < KEEP_BELOW],
+    np.savez_compressed(os.path.join(HERE, "cube8_sp3s_dense.npz"), eigenvalues=w[w < KEEP_BELOW],
                         window=np.array([WINDOW[0], KEEP_BELOW]), natoms=o.natoms)
     print(o.natoms, "atoms;", len(w), "eigenvalues in", WINDOW, ":", np.round(np.sort(w), 6))
 

@@ -111,7 +111,7 @@ def test_mixed_solve_matches_dense_golden(floor, imax):
     GaAs cells, 4096 atoms, sp3s*, +30 eV passivation, start vector from
     seed 0) for the 8 eigenvalues nearest 1.6 eV, windows as the FP64 parity
     case: every refined value is an eigenvalue of the oracle's dense H
-    (tests/golden/cfg1_dense.npz, LAPACK) within 1e-6 eV.  With the
+    (tests/golden/cube8_sp3s_dense.npz, LAPACK) within 1e-6 eV.  With the
     acceptance test at the tolerance (floor 0) the complex-float recurrence
     accepts the closely spaced levels late (2 of them in 6000 iterations,
     where the FP64 solve finds all); with the automatic floor (the
@@ -120,7 +120,7 @@ def test_mixed_solve_matches_dense_golden(floor, imax):
     import os
     from nemo3d_b200.tbgpu import Hamiltonian
     sigma = 1.6
-    dense = np.load(os.path.join(os.path.dirname(__file__), "golden", "cfg1_dense.npz"))
+    dense = np.load(os.path.join(os.path.dirname(__file__), "golden", "cube8_sp3s_dense.npz"))
     w = dense["eigenvalues"]
     near8 = w[np.argsort(np.abs(w - sigma), kind="stable")[:8]]
     mats = [materials.MATERIALS["GaAs_sps"], materials.MATERIALS["InAs_sps"]]

@@ -112,15 +112,15 @@ def test_gamma_point_golden(golden):
     assert np.abs(w - want).max() < 2e-11
 
 
-def _cfg1():
+def _cube8_case():
     st = workloads.gaas_cube(8)
     return st, dict(requested1=4, requested2=3, emin1=-0.35, emax1=-0.25,
                     emin2=1.6, emax2=1.89, tolerance=1e-7, imax=4000,
                     ConvCheckStartIter=200, ConvCheckSkipRate=50)
 
 
-def test_lanczos_cfg1_eigenvalues_match_oracle():
-    st, kw = _cfg1()
+def test_lanczos_cube8_eigenvalues_match_oracle():
+    st, kw = _cube8_case()
     g, o = pair(st, "sp3s*")
     r0 = workloads.random_start(g.n, seed=0)
     res = g.eigensolve_lanczos(r0, **kw)
@@ -137,7 +137,7 @@ def test_lanczos_cfg1_eigenvalues_match_oracle():
 
 
 def test_lanczos_eigenvectors_and_determinism():
-    st, kw = _cfg1()
+    st, kw = _cube8_case()
     g, o = pair(st, "sp3s*")
     r0 = workloads.random_start(g.n, seed=0)
     r1 = g.eigensolve_lanczos(r0, vectors=8, **kw)
@@ -181,7 +181,7 @@ def test_errors_are_codes_not_aborts():
 
 
 def test_full_size_hermitian_and_linear():
-    """cfg-2-sized dot (~1.0M atoms): size-independent properties of H."""
+    """1.02M-atom dome (58 x 58 x 38 cells): size-independent properties of H."""
     import torch
     from nemo3d_b200.tbgpu import Hamiltonian
     st = workloads.dome_in_box()
@@ -236,20 +236,20 @@ def test_lanczos_sp3d5s_so_dome_matches_oracle():
     assert np.abs(np.sort(res["values"]) - np.sort(ref["evals"])).max() < 1e-6
 
 
-def test_cfg1_eigenvalues_nearest_sigma():
+def test_cube8_eigenvalues_nearest_sigma():
     """The CPU-runnable case as stated: GaAs cube of 8x8x8 cells (4096 atoms),
     sp3s*, +30 eV passivation, start vector uniform in [-1, 1] from seed 0,
     the 8 eigenvalues nearest sigma = 1.6 eV.  Windows (sigma - 0.33, sigma]
     and (sigma, sigma + 0.33] with 8 requested in each run the solve to its
     iteration limit (the first window lies in the gap).  The 8 nearest
     eigenvalues with multiplicity come from LAPACK on the oracle's dense H
-    (tests/golden/cfg1_dense.npz); single-vector Lanczos returns each
+    (tests/golden/cube8_sp3s_dense.npz); single-vector Lanczos returns each
     degenerate level once, so the bar is: every distinct level among those 8
     is found, within 1e-6 eV, every value found is a dense eigenvalue
     within 1e-6 eV, and the GPU set equals the oracle's run."""
     import os
     sigma = 1.6
-    dense = np.load(os.path.join(os.path.dirname(__file__), "golden", "cfg1_dense.npz"))
+    dense = np.load(os.path.join(os.path.dirname(__file__), "golden", "cube8_sp3s_dense.npz"))
     w = dense["eigenvalues"]
     near8 = w[np.argsort(np.abs(w - sigma), kind="stable")[:8]]
     st = workloads.gaas_cube(8)

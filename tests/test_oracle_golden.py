@@ -55,12 +55,12 @@ def test_si_bulk_lanczos_sets(golden, chunk):
         assert np.abs(got - want).max() < 1e-6, (kx, got, want)
 
 
-def test_cfg1_dense_fixture_shape():
+def test_cube8_dense_fixture_shape():
     """The dense fixture of the 4096-atom cube: sorted eigenvalues in the gap
     region's window, the conduction-band edge first (no level between 1.0 eV
     and it), and the multiplicities of the cube's symmetric states."""
     import os
-    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "cfg1_dense.npz"))
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "cube8_sp3s_dense.npz"))
     w = d["eigenvalues"]
     assert int(d["natoms"]) == 4096
     assert np.all(np.diff(w) >= 0) and w[0] > 1.6 and w[-1] < 2.0
