@@ -319,7 +319,7 @@ def run_ours(args, rank, world, local_rank):
                               device_inputs=(types_d.data_ptr(), dsp_d.data_ptr()), **opts)
         H.set_stream(stream.cuda_stream)
         if precision == 32:
-            H.set_spmv_variant(MIXED_VARIANT)
+            H.set_spmv_variant(args.mixed_variant)
             H.set_eigenvector_pass(*MIXED_VEC_PASS)
             H.set_mixed_acceptance(args.mixed_accept)
         else:
@@ -410,7 +410,7 @@ def run_ours(args, rank, world, local_rank):
             opts = dict(ham_bits=32, lanczos_bits=32) if mixed else {}
             H = tbgpu.Hamiltonian(st, "sp3d5s*_so", MATS, **opts)   # host geometry in
             if mixed:
-                H.set_spmv_variant(MIXED_VARIANT)
+                H.set_spmv_variant(args.mixed_variant)
                 H.set_eigenvector_pass(*MIXED_VEC_PASS)
                 H.set_mixed_acceptance(args.mixed_accept)
             else:
@@ -615,20 +615,28 @@ def run_extra(args):
                           "block_lanczos_cuda_core": steps[0],
                           "block_lanczos_tensor_core": steps[1]}), flush=True)
     elif w == "kernels":
-        st = make_structure((58, 58, 38))
-        for name, opts, f32, var in (
-                ("fp64 store", {}, False, 0),
-                ("fp64 store, two-cell units (variant 3)", {}, False, 3),
-                ("fp64 store, every piece by cp.async (variant 4)", {}, False, 4),
-                ("fp64 store, lane per atom and spin (variant 5)", {}, False, 5),
-                ("fp64 store, pencil layout (variant 6)", {}, False, 6),
-                ("float store, float vectors", dict(ham_bits=32, lanczos_bits=32), True, 0),
+        st1 = make_structure((58, 58, 38))
+        st2 = make_structure((72, 72, 48))
+        f32o = dict(ham_bits=32, lanczos_bits=32)
+        for name, opts, f32, var, st in (
+                ("fp64 store", {}, False, 0, st1),
+                ("fp64 store, two-cell units (variant 3)", {}, False, 3, st1),
+                ("fp64 store, every piece by cp.async (variant 4)", {}, False, 4, st1),
+                ("fp64 store, lane per atom and spin (variant 5)", {}, False, 5, st1),
+                ("fp64 store, pencil layout (variant 6)", {}, False, 6, st1),
+                ("float store, float vectors", dict(ham_bits=32, lanczos_bits=32), True, 0, st1),
                 ("float store, float vectors, lane per atom and spin (variant 5)",
-                 dict(ham_bits=32, lanczos_bits=32), True, 5),
+                 dict(ham_bits=32, lanczos_bits=32), True, 5, st1),
                 ("float store, float vectors, pencil layout (variant 6)",
-                 dict(ham_bits=32, lanczos_bits=32), True, 6),
-                ("recompute fp64", dict(recompute=True), False, 0),
-                ("recompute float", dict(recompute=True, lanczos_bits=32), True, 0)):
+                 dict(ham_bits=32, lanczos_bits=32), True, 6, st1),
+                ("recompute fp64", dict(recompute=True), False, 0, st1),
+                ("recompute float", dict(recompute=True, lanczos_bits=32), True, 0, st1),
+                ("2M dot, float store, float vectors, lane per atom and spin (variant 5)",
+                 f32o, True, 5, st2),
+                ("2M dot, float store, float vectors, pencil layout (variant 6)", f32o, True, 6,
+                 st2),
+                ("2M dot, float store, float vectors, pencil layout, staged rows (variant 7)",
+                 f32o, True, 7, st2)):
             H = tbgpu.Hamiltonian(st, "sp3d5s*_so", MATS, **opts)
             H.set_spmv_variant(var)
             stream = torch.cuda.Stream()
@@ -884,6 +892,9 @@ def main():
                     help="with --profile-case: a few Keating VFF iterations instead")
     ap.add_argument("--spmv-variant", type=int, default=0, choices=[0, 1, 2, 3, 4, 5, 6],
                     help="H*x kernel of the solve (tbgpu_set_spmv_variant)")
+    ap.add_argument("--mixed-variant", type=int, default=MIXED_VARIANT, choices=[5, 6, 7],
+                    help="H*x kernel of the mixed solve (its columns must compute as one-column "
+                         "launches for the regenerating pass: 5, 6 or 7)")
     ap.add_argument("--mixed-accept", type=float, default=-1.0,
                     help="mixed solve: floor of the convergence test's bound on the last "
                          "components of a tridiagonal eigenvector (0: the tolerance; "

@@ -397,13 +397,18 @@ int tbgpu_hx_dot_noalloc(tbgpu_ctx *ctx, double shift, const double *x_dev,
  * stored with the k index of its cell fastest, so a warp's loads are
  * contiguous; the solves keep their Lanczos vectors in that layout, these
  * products permute the caller's vectors around the kernel; Gamma point, not
- * in batched solves, else as 0).  Variants 0, 2, 3 and 4 give the same y bit
- * for bit; 1, 5 and 6 sum in their own orders (equal to rounding). */
+ * in batched solves, else as 0), 7 = variant 6 with each warp's next bond's
+ * block rows double-buffered in shared memory by 16-byte cp.async copies
+ * while it computes the current one (32-bit store, spin-orbit models, closed
+ * z boundary and nz a multiple of 16; else as 6).  Variants 0, 2, 3 and 4
+ * give the same y bit for bit, and so do 6 and 7; 1, 5 and 6 sum in their
+ * own orders (equal to rounding). */
 int tbgpu_set_spmv_variant(tbgpu_ctx *ctx, int variant);
 
 /* Autotuner: times the H*x variants that are distinct kernels for the built
- * context (all seven for the 10-orbital models with the 64-bit store at the
- * Gamma point, 0, 1, 5 and 6 with the 32-bit store, only 0 for 5-orbital models,
+ * context (0 to 6 for the 10-orbital models with the 64-bit store at the
+ * Gamma point, 0, 1, 5, 6 and, where it applies, 7 with the 32-bit store,
+ * only 0 for 5-orbital models,
  * Bloch phases and recompute storage), reps launches each with the fused
  * Lanczos dot after two untimed ones (CUDA events on the context stream;
  * two temporary device vectors), selects the fastest (ties: the lower

@@ -490,7 +490,7 @@ int tbgpu_export_hamiltonian(const tbgpu_ctx *ctx, double *onsite, double *block
 }
 
 int tbgpu_set_spmv_variant(tbgpu_ctx *ctx, int variant) {
-  if (!ctx || variant < 0 || variant > 6) return set_error(TBGPU_E_ARG);
+  if (!ctx || variant < 0 || variant > 7) return set_error(TBGPU_E_ARG);
   C(ctx)->spmv_variant = variant;
   return TBGPU_OK;
 }
@@ -510,6 +510,11 @@ static int distinct_variants(const Ctx &c, int *v) {
     v[1] = 1;
     v[2] = 5;
     v[3] = 6;
+    // the staged pencil kernel where it applies (otherwise 7 runs 6's)
+    if (c.nspin == 2 && c.nz % 16 == 0 && !c.periodic[2]) {
+      v[4] = 7;
+      return 5;
+    }
     return 4;
   }
   for (int i = 0; i < 7; i++) v[i] = i;

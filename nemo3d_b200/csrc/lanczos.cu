@@ -577,11 +577,12 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
   c.fold_energy.clear();
   bool regen = !fold && c.vec_pass == 1 && V_dev && maxvec > 0 && lane_supported(c) && f32_ok;
   const int keep_variant = c.spmv_variant;
-  if (regen) c.spmv_variant = pen_supported(c) && keep_variant == 6 ? 6 : 5;
-  // the pencil kernel keeps the Lanczos vectors in its own layout: the start
-  // vector is permuted in and the eigenvectors out
-  const bool pen = c.spmv_variant == 6 && pen_supported(c) && f32_ok;
-  if (!pen && c.spmv_variant == 6) c.spmv_variant = regen ? 5 : 0;
+  const bool pen_variant = keep_variant == 6 || keep_variant == 7;
+  if (regen) c.spmv_variant = pen_supported(c) && pen_variant ? keep_variant : 5;
+  // the pencil kernels keep the Lanczos vectors in their own layout: the
+  // start vector is permuted in and the eigenvectors out
+  const bool pen = (c.spmv_variant == 6 || c.spmv_variant == 7) && pen_supported(c) && f32_ok;
+  if (!pen && (c.spmv_variant == 6 || c.spmv_variant == 7)) c.spmv_variant = regen ? 5 : 0;
   const long n2_ref = c.natoms * c.nb;           // complex entries, reference order
   const long n2 = pen ? pen_length(c) : n2_ref;  // of the solver's vectors
   const size_t vbytes = sizeof(VT) * n2;        // one Lanczos vector

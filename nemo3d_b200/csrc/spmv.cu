@@ -237,7 +237,7 @@ int launch_spmv(Ctx &c, const double *x, double *y, double shift, const double *
   if (c.recompute) return launch_spmv_recompute(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
   // the warp-staged kernel has no phase support: periodic structures away
   // from Gamma take the lane-gather kernel
-  if (c.spmv_variant == 6 && pen_supported(c))
+  if ((c.spmv_variant == 6 || c.spmv_variant == 7) && pen_supported(c))
     return launch_spmv_pen(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
   if (c.spmv_variant == 5 && lane_supported(c))
     return launch_spmv_lane(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
@@ -261,7 +261,7 @@ int launch_spmv_f32(Ctx &c, const float *x, float *y, double shift, const double
   if (c.recompute)
     return launch_spmv_recompute_f32(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
   if (!c.ham_fp32) return set_error(TBGPU_E_UNSUPPORTED);
-  if (c.spmv_variant == 6 && pen_supported(c))
+  if ((c.spmv_variant == 6 || c.spmv_variant == 7) && pen_supported(c))
     return launch_spmv_pen_f32(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
   if (c.spmv_variant == 5 && lane_supported(c))
     return launch_spmv_lane_f32(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);

@@ -40,6 +40,7 @@
 #include "lanczos_step.cuh"
 #include "lane_math.cuh"
 #include "reduce.cuh"
+#include "stage.cuh"
 #include "zincblende.cuh"
 
 namespace tbgpu {
@@ -278,6 +279,268 @@ __global__ void __launch_bounds__(pen_warps<P, VT>() * 32, 1)
   if (DOT) grid_reduce<W * 32>(dot, partial, counter, alpha_out, alpha_idx, false);
 }
 
+// ---- the same product with each warp's block rows staged (H*x variant 7) ---
+//
+// k_spmv_pen keeps only a few of its contiguous block-row loads in flight per
+// warp and stalls on their latency.  Here every warp double-buffers the 50
+// block rows (10 rows x 5 column pairs, 16 k entries each) of the bond it
+// computes next in shared memory by 16-byte cp.async copies, issued while it
+// computes the current bond from the other buffer: a cation's own rows at
+// its 16-atom k range, or the rows its cation neighbour stores, from an even
+// k start two entries early when the neighbour sits at k - 1 (entries outside
+// the line are zero-filled and never read).  The arithmetic of every lane is
+// k_spmv_pen's, in the same order, so the results are bit-identical and the
+// solver's first pass and regenerating pass may use either kernel.  Float
+// store, spin-orbit models, closed z boundary and nz a multiple of 16 (each
+// 16-atom task inside one line); other contexts use k_spmv_pen.
+constexpr int kStgK = 18;                       // staged k entries per row
+constexpr int kStgRows = 50;                    // rows of one bond's block
+constexpr int kStgBytes = kStgRows * kStgK * 8;  // one buffer (float pairs)
+
+template <int P>
+__host__ __device__ constexpr int pen_stg_warps() {
+  return P == 1 ? 12 : 8;
+}
+
+template <int P, typename VT, bool DOT, bool UPD>
+__global__ void __launch_bounds__(pen_stg_warps<P>() * 32, 1)
+    k_spmv_pen_stg(PenGeo G, const unsigned char *__restrict__ ok, const float *__restrict__ ons,
+                   const float2 *__restrict__ blk, PenCols<VT, P> A,
+                   const double *__restrict__ bet, const double *__restrict__ alpha,
+                   double shift_d, double *partial, unsigned int *counter, double *alpha_out,
+                   int alpha_idx) {
+  using RT = typename RealOf<VT>::T;
+  using HT = float;
+  constexpr int NSPIN = 2;
+  constexpr int W = pen_stg_warps<P>();
+  constexpr int KC = 16;  // atoms per warp task
+  constexpr int NB = kNorbP * NSPIN;
+  constexpr int ONS = onsite_len(NB);
+  extern __shared__ __align__(16) unsigned char pen_stg_smem[];
+  const int nz = G.nz;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int ai = lane >> 1, s = lane & 1;
+  float2 *const buf0 = reinterpret_cast<float2 *>(pen_stg_smem + size_t(warp) * 2 * kStgBytes);
+  RT scale[P];
+  double iq[P], ip[P], al[P], bp[P];
+#pragma unroll
+  for (int c = 0; c < P; c++) {
+    const int it = A.it[c];
+    scale[c] = RT(bet ? 1.0 / bet[it] : 1.0);
+    if (UPD) {
+      al[c] = alpha[it];
+      bp[c] = bet[it];
+      iq[c] = 1.0 / bp[c];
+      ip[c] = it > 0 ? 1.0 / bet[it - 1] : 0.0;
+    }
+  }
+  const RT shift = RT(shift_d);
+  double dot = 0.0;
+  const long ntasks = (G.nline / KC) * 8;
+  const long stride = long(gridDim.x) * W;
+
+  // bond n of task t has a neighbour pencil (the same for all lanes)
+  auto bond_valid = [&](long t, int n) -> bool {
+    const int m = int(t & 7);
+    const long p = ((t >> 3) * KC) / nz;
+    const int i = int(p / G.ny), j = int(p - long(i) * G.ny);
+    return nb_pencil(G, i, j, c_nnmap[m][n][0], c_nnmap[m][n][1]) >= 0;
+  };
+  // the next bond with a neighbour pencil at or after (t, n) in this warp's
+  // task order; t >= ntasks when none is left
+  auto advance = [&](long &t, int &n) {
+    while (t < ntasks) {
+      for (; n < 4; n++)
+        if (bond_valid(t, n)) return;
+      t += stride;
+      n = 0;
+    }
+  };
+  // copy the 50 rows bond n of task t reads into buffer b (cooperative)
+  auto issue = [&](long t, int n, float2 *b) {
+    const int m = int(t & 7);
+    const long L0 = (t >> 3) * KC;
+    const long p = L0 / nz;
+    const int k0 = int(L0 - p * nz);
+    long pr = p;
+    int mr = m, nr = n, kst = k0, cpr = 8;
+    if (m >= 4) {
+      const int i = int(p / G.ny), j = int(p - long(i) * G.ny);
+      pr = nb_pencil(G, i, j, c_nnmap[m][n][0], c_nnmap[m][n][1]);
+      mr = c_nnmap[m][n][3];
+      nr = c_rev_slot[m][n];
+      if (c_nnmap[m][n][2] < 0) {
+        kst = k0 - 2;
+        cpr = 9;
+      }
+    }
+    const int total = kStgRows * cpr;
+    for (int q = lane; q < total; q += 32) {
+      const int row = q / cpr, part = q - row * cpr;
+      const int r = row / 5, cc = row - r * 5;
+      const int e = kst + 2 * part;  // even; nz even: both entries in or both out
+      const bool in = e >= 0 && e < nz;
+      stage::cp16z(b + row * kStgK + 2 * part, blk + bidx(pr, mr, nr, r, cc, in ? e : 0, nz),
+                   in ? 16 : 0);
+    }
+  };
+
+  // the copy pipeline runs one bond ahead of the computation, across tasks
+  long jt = long(blockIdx.x) * W + warp;
+  int jn = 0;
+  advance(jt, jn);
+  int cur = 0;
+  if (jt < ntasks) issue(jt, jn, buf0);
+  stage::cp_commit();
+  for (long t = long(blockIdx.x) * W + warp; t < ntasks; t += stride) {
+    const int m = int(t & 7);
+    const long line = (t >> 3) * KC + ai;
+    const long p = line / nz;
+    const int k = int(line - p * nz);
+    const int k0 = k - ai;
+    const bool active = ok[(p * 8 + m) * nz + k] != 0;
+    const int i = int(p / G.ny), j = int(p - long(i) * G.ny);
+    VT acc[P][kNorbP];
+    if (active) {
+      RT dg[kNorbP];
+#pragma unroll
+      for (int q = 0; q < kNorbP; q++) dg[q] = RT(ons[oidx(p, m, s * kNorbP + q, k, nz, ONS)]);
+      const bool pass = ons[oidx(p, m, NB + 1, k, nz, ONS)] != HT(0);
+      RT cpl[6] = {RT(0), RT(0), RT(0), RT(0), RT(0), RT(0)};
+      if (pass) {
+#pragma unroll
+        for (int f = 0; f < 6; f++) cpl[f] = RT(ons[oidx(p, m, NB + 2 + f, k, nz, ONS)]);
+      }
+      const RT L = RT(ons[oidx(p, m, NB, k, nz, ONS)]);
+#pragma unroll
+      for (int c = 0; c < P; c++) {
+        VT xo[kNorbP];
+#pragma unroll
+        for (int q = 0; q < kNorbP; q++) xo[q] = A.x[c][vidx(p, m, q, k, s, nz, NSPIN)];
+#pragma unroll
+        for (int q = 0; q < kNorbP; q++) {
+          acc[c][q].x = mul_rn(dg[q], xo[q].x);
+          acc[c][q].y = mul_rn(dg[q], xo[q].y);
+        }
+        if (pass) {
+          const RT sx = cpl[0], sy = cpl[1], sz = cpl[2], cxy = cpl[3], cxz = cpl[4], cyz = cpl[5];
+          cfma(acc[c][1], sx, xo[2]); cfma(acc[c][1], sy, xo[3]); cfma(acc[c][1], sz, xo[4]);
+          cfma(acc[c][2], sx, xo[1]); cfma(acc[c][2], cxy, xo[3]); cfma(acc[c][2], cxz, xo[4]);
+          cfma(acc[c][3], sy, xo[1]); cfma(acc[c][3], cxy, xo[2]); cfma(acc[c][3], cyz, xo[4]);
+          cfma(acc[c][4], sz, xo[1]); cfma(acc[c][4], cxz, xo[2]); cfma(acc[c][4], cyz, xo[3]);
+        }
+        {
+          const VT o2 = A.x[c][vidx(p, m, 2, k, 1 - s, nz, NSPIN)];
+          const VT o3 = A.x[c][vidx(p, m, 3, k, 1 - s, nz, NSPIN)];
+          const VT o4 = A.x[c][vidx(p, m, 4, k, 1 - s, nz, NSPIN)];
+          if (s == 0) {
+            cfma_im(acc[c][2], -L, xo[3]); cfma(acc[c][2], L, o4);
+            cfma_im(acc[c][3], L, xo[2]);  cfma_im(acc[c][3], -L, o4);
+            cfma(acc[c][4], -L, o2);       cfma_im(acc[c][4], L, o3);
+          } else {
+            cfma_im(acc[c][2], L, xo[3]);  cfma(acc[c][2], -L, o4);
+            cfma_im(acc[c][3], -L, xo[2]); cfma_im(acc[c][3], -L, o4);
+            cfma(acc[c][4], L, o2);        cfma_im(acc[c][4], L, o3);
+          }
+        }
+      }
+    }
+#pragma unroll 1
+    for (int n = 0; n < 4; n++) {
+      if (!bond_valid(t, n)) continue;  // warp-uniform; this bond's rows are in buffer `cur`
+      long nt = jt;
+      int nn = jn + 1;
+      advance(nt, nn);
+      if (nt < ntasks) issue(nt, nn, buf0 + (cur ^ 1) * (kStgBytes / 8));
+      stage::cp_commit();
+      stage::cp_wait<1>();
+      __syncwarp();
+      const float2 *b0 = buf0 + cur * (kStgBytes / 8);
+      const long p2 = nb_pencil(G, i, j, c_nnmap[m][n][0], c_nnmap[m][n][1]);
+      const int k2 = nb_k(G, k, c_nnmap[m][n][2]);
+      if (active && k2 >= 0) {
+        if (m < 4) {
+          const int m2 = c_nnmap[m][n][3];
+          VT xn[P][kNorbP];
+#pragma unroll
+          for (int c = 0; c < P; c++)
+#pragma unroll
+            for (int q = 0; q < kNorbP; q++) xn[c][q] = A.x[c][vidx(p2, m2, q, k2, s, nz, NSPIN)];
+#pragma unroll
+          for (int r = 0; r < kNorbP; r++) {
+            float2 b[5];
+#pragma unroll
+            for (int cc = 0; cc < 5; cc++) b[cc] = b0[(r * 5 + cc) * kStgK + ai];
+#pragma unroll
+            for (int c = 0; c < P; c++)
+#pragma unroll
+              for (int cc = 0; cc < 5; cc++) {
+                cfma(acc[c][r], RT(b[cc].x), xn[c][2 * cc]);
+                cfma(acc[c][r], RT(b[cc].y), xn[c][2 * cc + 1]);
+              }
+          }
+        } else {
+          const int mc = c_nnmap[m][n][3];
+          const int off = ai + (c_nnmap[m][n][2] < 0 ? 1 : 0);
+#pragma unroll
+          for (int r = 0; r < kNorbP; r++) {
+            float2 b[5];
+#pragma unroll
+            for (int cc = 0; cc < 5; cc++) b[cc] = b0[(r * 5 + cc) * kStgK + off];
+#pragma unroll
+            for (int c = 0; c < P; c++) {
+              const VT xc = A.x[c][vidx(p2, mc, r, k2, s, nz, NSPIN)];
+#pragma unroll
+              for (int cc = 0; cc < 5; cc++) {
+                cfma(acc[c][2 * cc], RT(b[cc].x), xc);
+                cfma(acc[c][2 * cc + 1], RT(b[cc].y), xc);
+              }
+            }
+          }
+        }
+      }
+      __syncwarp();  // the buffer is refilled two bonds on
+      cur ^= 1;
+      jt = nt;
+      jn = nn;
+    }
+    (void)k0;
+    if (active) {
+#pragma unroll
+      for (int c = 0; c < P; c++) {
+#pragma unroll
+        for (int q = 0; q < kNorbP; q++) {
+          const long e = vidx(p, m, q, k, s, nz, NSPIN);
+          const VT xv = A.x[c][e];
+          VT xs, out;
+          xs.x = mul_rn(scale[c], xv.x);
+          xs.y = mul_rn(scale[c], xv.y);
+          out.x = fma_rn(scale[c], acc[c][q].x, -mul_rn(shift, xs.x));
+          out.y = fma_rn(scale[c], acc[c][q].y, -mul_rn(shift, xs.y));
+          if (UPD) {
+            VT rpv;
+            if (A.rp[c]) rpv = A.rp[c][e];
+            else rpv.x = rpv.y = RT(0);
+            const double2 rr = lanczos_update_entry(
+                make_double2(double(out.x), double(out.y)),
+                make_double2(double(xv.x), double(xv.y)),
+                make_double2(double(rpv.x), double(rpv.y)), al[c], bp[c], iq[c], ip[c]);
+            VT rv;
+            rv.x = RT(rr.x);
+            rv.y = RT(rr.y);
+            A.y[c][e] = rv;
+          } else {
+            A.y[c][e] = out;
+          }
+          if (DOT) dot += double(xs.x) * double(out.x) + double(xs.y) * double(out.y);
+        }
+      }
+    }
+  }
+  stage::cp_wait<0>();
+  if (DOT) grid_reduce<W * 32>(dot, partial, counter, alpha_out, alpha_idx, false);
+}
+
 // ---- layout builders -------------------------------------------------------
 __device__ __forceinline__ void site_coords(int site, int nz, long &p, int &k, int &m) {
   m = site & 7;
@@ -369,6 +632,12 @@ bool pen_supported(const Ctx &c) {
 
 long pen_length(const Ctx &c) { return c.nsites * c.nb; }
 
+// variant 7: the staged pencil kernel where it applies (float store,
+// spin-orbit, closed z, nz a multiple of 16)
+bool pen_staged(const Ctx &c) {
+  return c.spmv_variant == 7 && c.ham_fp32 && c.nspin == 2 && c.nz % 16 == 0 && !c.periodic[2];
+}
+
 // the pencil layout of the stored Hamiltonian (built on first use)
 static int build_pen(Ctx &c) {
   if (c.d_pen_blk && c.pen_fp32 == c.ham_fp32) return TBGPU_OK;
@@ -437,6 +706,20 @@ static int launch_pen_t(Ctx &c, const PenCols<VT, P> &A, const double *bet, cons
     if (rc) return rc;
   }
   using HT2 = typename PairOf<HT>::T;
+  if constexpr (NSPIN == 2 && sizeof(HT) == sizeof(float)) {
+    if (pen_staged(c)) {
+      constexpr int smem = pen_stg_warps<P>() * 2 * kStgBytes;
+      static std::atomic<unsigned long long> attr_done{0};
+      if (ensure_smem_attr(attr_done, c.device, k_spmv_pen_stg<P, VT, DOT, UPD>, smem))
+        return TBGPU_E_CUDA;
+      k_spmv_pen_stg<P, VT, DOT, UPD><<<grid, pen_stg_warps<P>() * 32, smem, s>>>(
+          pen_geo(c), c.d_pen_ok, static_cast<const float *>(c.d_pen_ons),
+          static_cast<const float2 *>(c.d_pen_blk), A, bet, alpha, shift,
+          DOT ? c.d_partial : nullptr, DOT ? c.d_counter : nullptr, alpha_out, aidx);
+      TB_CUDA(cudaGetLastError());
+      return TBGPU_OK;
+    }
+  }
   k_spmv_pen<NSPIN, P, HT, VT, DOT, UPD><<<grid, pen_warps<P, VT>() * 32, 0, s>>>(
       pen_geo(c), c.d_pen_ok, static_cast<const HT *>(c.d_pen_ons),
       static_cast<const HT2 *>(c.d_pen_blk), A, bet, alpha, shift, DOT ? c.d_partial : nullptr,

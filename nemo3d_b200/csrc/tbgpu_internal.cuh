@@ -246,6 +246,7 @@ int launch_lane_regen(Ctx &c, int p, const VT *const *x, VT *const *y, const VT 
 // spmv_pen.cu: pencil-interleaved layout (variant 6), 10-orbital models,
 // stored blocks, Gamma point, no skip mask
 bool pen_supported(const Ctx &c);
+bool pen_staged(const Ctx &c);
 long pen_length(const Ctx &c);  // complex entries of a pencil-layout vector
 int launch_spmv_pen(Ctx &c, const double *x, double *y, double shift, const double *xscale_dev,
                     int scale_index, double *alpha_out, int alpha_index, cudaStream_t s);

@@ -12,7 +12,14 @@ Bars:
   eigenvector residuals ||H v - lambda v|| < 1e-4 eV through the oracle;
 * eigenvector pass by regeneration on the pencil kernel: every segment end
   bit-identical to its checkpoint (vec_mismatch == 0), eigenvalues identical
-  to the second-run pass on the same kernel, eigenvectors equal to rounding.
+  to the second-run pass on the same kernel, eigenvectors equal to rounding;
+* variant 7 (block rows double-buffered through shared memory by cp.async)
+  gives variant 6's y bit for bit on the float store, with float and with
+  double vectors, on boxes whose pencils are 16 and 32 cells long (every
+  task at a line end reads zero-filled entries), with vacancies; the mixed
+  solve on it regenerates its segments bit for bit and finds the values of
+  the solve on variant 6 to 1e-9 eV; where it does not apply (periodic z, nz
+  not a multiple of 16) variant 7 runs variant 6.
 """
 import numpy as np
 import pytest
@@ -151,3 +158,96 @@ def test_pen_regenerated_eigenvectors(bits, columns, segment):
             assert np.abs(v0 - v1).max() < 1e-10 * np.abs(v0).max()
     else:  # refined through the recompute product: equal to the refinement's rounding
         assert np.abs(a["values"] - b["values"]).max() < 1e-9
+
+
+def _dome16(cells=(6, 5, 16), seed=4, vacancies=0.0):
+    st = workloads.dome_in_box(cells=cells, base_nm=2.4, height_nm=1.0, wl_z_nm=1.2,
+                               sigma_frac=0.02, seed=seed)
+    if vacancies:
+        rng = np.random.default_rng(seed)
+        t = st.types.reshape(-1).copy()
+        t[rng.random(t.size) < vacancies] = 0
+        st.types = t.reshape(st.types.shape)
+    return st
+
+
+@pytest.mark.parametrize("cells,vac", [((6, 5, 16), 0.0), ((4, 3, 32), 0.0), ((6, 5, 16), 0.03)])
+def test_pen_staged_bit_identical(cells, vac):
+    import torch
+    from nemo3d_b200.tbgpu import Hamiltonian
+    st = _dome16(cells, vacancies=vac)
+    # float vectors over the float store
+    g = Hamiltonian(st, "sp3d5s*_so", MATS, ham_bits=32, lanczos_bits=32)
+    x = workloads.random_start(g.n, seed=9)
+    xf = torch.from_numpy(x.astype(np.float32)).cuda()
+    y6, y7 = torch.empty_like(xf), torch.empty_like(xf)
+    g.set_spmv_variant(6)
+    g.hx_dev_f32(xf.data_ptr(), y6.data_ptr(), shift=0.3)
+    g.set_spmv_variant(7)
+    g.hx_dev_f32(xf.data_ptr(), y7.data_ptr(), shift=0.3)
+    torch.cuda.synchronize()
+    assert torch.equal(y6, y7)
+    assert y7.abs().max().item() > 0.0
+    # double vectors over the float store, against the oracle as well
+    g2 = Hamiltonian(st, "sp3d5s*_so", MATS, ham_bits=32)
+    g2.set_spmv_variant(6)
+    a6 = g2.matvect_mult(x, 0.4)
+    g2.set_spmv_variant(7)
+    a7 = g2.matvect_mult(x, 0.4)
+    np.testing.assert_array_equal(a6, a7)
+    o32 = _rounded(oracle.OracleHamiltonian(st, 10, 2, MATS))
+    yo = o32.hx(x, 0.4)
+    assert np.abs(a7 - yo).max() <= 1e-12 * np.abs(yo).max()
+
+
+def test_pen_staged_solve():
+    """The mixed solve with the regenerating pass on variant 7 against the same
+    solve on variant 6.  The products are bit-identical, but the fused alpha
+    dot sums its per-thread parts over another thread layout (12 warps per
+    block instead of 16), so the recurrences differ in the last bits: the
+    bar is the regenerated segments bit-identical to the first pass, every
+    value both solves find equal to 1e-9 eV, and FP64 residuals of the
+    refined pairs below 1e-3 eV."""
+    from nemo3d_b200.tbgpu import Hamiltonian
+    st = _dome16((8, 8, 16), seed=2)
+    out = {}
+    for v in (6, 7):
+        g = Hamiltonian(st, "sp3d5s*_so", MATS, ham_bits=32, lanczos_bits=32)
+        g.set_spmv_variant(v)
+        g.set_eigenvector_pass(1, 4, 64)
+        g.set_mixed_acceptance(-1.0)
+        res = g.eigensolve_lanczos(workloads.random_start(g.n, seed=0), vectors=4, **KW)
+        s = g.stats()
+        assert s["vec_segments"] >= 2 and s["vec_mismatch"] == 0, s
+        res["resid"] = g.state_errors()[0]
+        out[v] = res
+    print("variant 6:", out[6]["iterations"], out[6]["values"], "variant 7:",
+          out[7]["iterations"], out[7]["values"], "residuals", out[7]["resid"])
+    assert len(out[7]["values"]) >= 2
+    common = 0
+    for lam in out[7]["values"]:
+        d = np.abs(out[6]["values"] - lam).min() if len(out[6]["values"]) else 1.0
+        if d < 1e-6:
+            assert d < 1e-9, (lam, d)
+            common += 1
+    assert common >= 2
+    assert np.max(out[7]["resid"]) < 1e-3
+
+
+@pytest.mark.parametrize("cells,periodic", [((6, 5, 5), (False, False, False)),
+                                            ((4, 4, 16), (False, False, True))])
+def test_pen_staged_falls_back(cells, periodic):
+    import torch
+    from nemo3d_b200.tbgpu import Hamiltonian
+    st = _dome16(cells)
+    st.periodic = periodic
+    g = Hamiltonian(st, "sp3d5s*_so", MATS, ham_bits=32, lanczos_bits=32)
+    x = workloads.random_start(g.n, seed=3)
+    xf = torch.from_numpy(x.astype(np.float32)).cuda()
+    y6, y7 = torch.empty_like(xf), torch.empty_like(xf)
+    g.set_spmv_variant(6)
+    g.hx_dev_f32(xf.data_ptr(), y6.data_ptr(), shift=0.1)
+    g.set_spmv_variant(7)
+    g.hx_dev_f32(xf.data_ptr(), y7.data_ptr(), shift=0.1)
+    torch.cuda.synchronize()
+    assert torch.equal(y6, y7)
