@@ -320,7 +320,7 @@ def run_ours(args, rank, world, local_rank):
         H.set_stream(stream.cuda_stream)
         if precision == 32:
             H.set_spmv_variant(args.mixed_variant)
-            H.set_eigenvector_pass(*MIXED_VEC_PASS)
+            H.set_eigenvector_pass(1, args.mixed_columns, MIXED_VEC_PASS[2])
             H.set_mixed_acceptance(args.mixed_accept)
         else:
             H.set_spmv_variant(args.spmv_variant)
@@ -411,7 +411,7 @@ def run_ours(args, rank, world, local_rank):
             H = tbgpu.Hamiltonian(st, "sp3d5s*_so", MATS, **opts)   # host geometry in
             if mixed:
                 H.set_spmv_variant(args.mixed_variant)
-                H.set_eigenvector_pass(*MIXED_VEC_PASS)
+                H.set_eigenvector_pass(1, args.mixed_columns, MIXED_VEC_PASS[2])
                 H.set_mixed_acceptance(args.mixed_accept)
             else:
                 H.set_spmv_variant(args.spmv_variant)
@@ -510,6 +510,20 @@ def run_profile_case(args):
         torch.cuda.synchronize()
         print(json.dumps({"profile_case": "vff", "natoms": st.nsites, "iterations": its,
                           "energy": e}), flush=True)
+        return
+    if args.profile_mixed:  # the headline's solver configuration on this dot
+        H = tbgpu.Hamiltonian(st, "sp3d5s*_so", MATS, ham_bits=32, lanczos_bits=32)
+        H.set_spmv_variant(args.mixed_variant)
+        H.set_eigenvector_pass(1, args.mixed_columns, MIXED_VEC_PASS[2])
+        H.set_mixed_acceptance(args.mixed_accept)
+        r0 = workloads.random_start(H.n, seed=0)
+        res = H.eigensolve_lanczos(r0, vectors=2, requested1=1, requested2=1, emin1=0.4,
+                                   emax1=1.25, emin2=1.25, emax2=2.2, tolerance=1e-7,
+                                   imax=20000)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_case": "mixed", "natoms": H.natoms, "dimension": H.n,
+                          "values": [float(v) for v in res["values"]],
+                          "iterations": res["iterations"], "stats": H.stats()}), flush=True)
         return
     opts = {}
     if args.profile_storage == "recompute":
@@ -886,6 +900,9 @@ def main():
                     help="with --profile-case: stored blocks or blocks recomputed in H*x")
     ap.add_argument("--profile-precision", type=int, default=64, choices=[64, 32],
                     help="with --profile-case: FP64 or the mixed-precision Lanczos")
+    ap.add_argument("--profile-mixed", action="store_true",
+                    help="with --profile-case: the headline's mixed solve (kernel, "
+                         "regenerating pass, acceptance floor) for 1 hole + 1 electron state")
     ap.add_argument("--profile-vectors", action="store_true",
                     help="with --profile-case: a converging solve with the eigenvector pass")
     ap.add_argument("--profile-vff", action="store_true",
@@ -895,6 +912,8 @@ def main():
     ap.add_argument("--mixed-variant", type=int, default=MIXED_VARIANT, choices=[5, 6, 7],
                     help="H*x kernel of the mixed solve (its columns must compute as one-column "
                          "launches for the regenerating pass: 5, 6 or 7)")
+    ap.add_argument("--mixed-columns", type=int, default=MIXED_VEC_PASS[1], choices=[1, 2, 3, 4],
+                    help="eigenvector pass of the mixed solve: segments regenerated per launch")
     ap.add_argument("--mixed-accept", type=float, default=-1.0,
                     help="mixed solve: floor of the convergence test's bound on the last "
                          "components of a tridiagonal eigenvector (0: the tolerance; "
