@@ -318,6 +318,17 @@ int tbgpu_set_block_dots(tbgpu_ctx *ctx, int mode);
  * TBGPU_E_ARG for floor >= 1, NaN or -infinity. */
 int tbgpu_set_mixed_acceptance(tbgpu_ctx *ctx, double floor);
 
+/* The Lanczos solves take their per-solve device buffers (the recurrence's
+ * vectors, the eigenvector pass's checkpoints and segment rings: tens of GB
+ * for a 2M-atom dot) from one memory pool per device that keeps its memory
+ * mapped after the solve, so that later solves in the process reuse it
+ * instead of mapping and unmapping it again (which took up to seconds of
+ * host time per solve).  This returns the memory the pools hold but no
+ * solve uses to the device; call it once the solves' streams have
+ * finished.  No counterpart in the reference (its buffers come from
+ * malloc). */
+int tbgpu_release_solver_memory(void);
+
 /* Tridiagonal matrix of the last solve: alpha[n], beta[n] (n <= cap). */
 int tbgpu_get_tridiagonal(const tbgpu_ctx *ctx, double *alpha, double *beta,
                           int cap);

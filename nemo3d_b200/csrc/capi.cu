@@ -3,6 +3,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -26,6 +27,57 @@ int take_status(Ctx &c) {
   if (!st) return TBGPU_OK;
   if (cudaMemset(c.d_status, 0, sizeof(int)) != cudaSuccess) return set_error(TBGPU_E_CUDA);
   return set_error(st);
+}
+
+// The solver's per-solve buffers (Lanczos rings, checkpoints, segment rings)
+// come from one memory pool per device that keeps its memory mapped between
+// solves: through a pool that returns memory at every synchronisation, the
+// tens of gigabytes a large solve takes and gives back cost up to seconds of
+// host time per solve, long enough to drain the work queued on the GPU.
+namespace {
+constexpr int kMaxPoolDevices = 64;
+std::mutex g_pool_mu;
+cudaMemPool_t g_pool[kMaxPoolDevices];
+bool g_pool_made[kMaxPoolDevices];
+bool g_pool_failed[kMaxPoolDevices];
+}  // namespace
+
+cudaMemPool_t solver_pool(int device) {
+  if (device < 0 || device >= kMaxPoolDevices) return nullptr;
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  if (g_pool_made[device]) return g_pool[device];
+  if (g_pool_failed[device]) return nullptr;
+  cudaMemPoolProps props{};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.handleTypes = cudaMemHandleTypeNone;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = device;
+  cudaMemPool_t pool = nullptr;
+  unsigned long long keep = ~0ull;
+  if (cudaMemPoolCreate(&pool, &props) != cudaSuccess ||
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess) {
+    cudaGetLastError();
+    if (pool) cudaMemPoolDestroy(pool);
+    g_pool_failed[device] = true;  // the solver falls back to the default pool
+    return nullptr;
+  }
+  g_pool[device] = pool;
+  g_pool_made[device] = true;
+  return pool;
+}
+
+size_t solver_pool_spare(int device) {
+  cudaMemPool_t pool = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (device < 0 || device >= kMaxPoolDevices || !g_pool_made[device]) return 0;
+    pool = g_pool[device];
+  }
+  unsigned long long reserved = 0, used = 0;
+  if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) != cudaSuccess ||
+      cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) != cudaSuccess)
+    return 0;
+  return reserved > used ? size_t(reserved - used) : 0;
 }
 
 
@@ -716,6 +768,19 @@ int tbgpu_set_eigenvector_pass(tbgpu_ctx *ctx, int mode, int columns, int segmen
   c.vec_columns = columns;
   c.vec_segment = segment;
   return TBGPU_OK;
+}
+
+int tbgpu_release_solver_memory(void) {
+  int rc = TBGPU_OK;
+  for (int d = 0; d < kMaxPoolDevices; d++) {
+    cudaMemPool_t pool = nullptr;
+    {
+      std::lock_guard<std::mutex> lk(g_pool_mu);
+      if (g_pool_made[d]) pool = g_pool[d];
+    }
+    if (pool && cudaMemPoolTrimTo(pool, 0) != cudaSuccess) rc = set_error(TBGPU_E_CUDA);
+  }
+  return rc;
 }
 
 int tbgpu_set_mixed_acceptance(tbgpu_ctx *ctx, double floor) {

@@ -171,8 +171,8 @@ static int rayleigh_quotients(Ctx &c, const double *V, int nv, std::vector<doubl
   const long n2 = c.natoms * c.nb;
   double *y = nullptr, *d = nullptr;
   out.assign(nv, 0.0);
-  if (cudaMallocAsync(&y, sizeof(double2) * n2, s) != cudaSuccess ||
-      cudaMallocAsync(&d, sizeof(double) * 2 * std::max(nv, 1), s) != cudaSuccess) {
+  if (solver_alloc(c.device, &y, sizeof(double2) * n2, s) != cudaSuccess ||
+      solver_alloc(c.device, &d, sizeof(double) * 2 * std::max(nv, 1), s) != cudaSuccess) {
     if (y) cudaFreeAsync(y, s);
     return set_error(TBGPU_E_NOMEM);
   }
@@ -631,11 +631,11 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
     if (Tf) cudaFreeAsync(Tf, s);
     Tf = nullptr;
     for (int i = 0; i <= kMaxChunk; i++)
-      if (ring[i]) cudaFree(ring[i]);
-    if (W) cudaFree(W);
-    if (d_alpha) cudaFree(d_alpha);
-    if (d_bet) cudaFree(d_bet);
-    if (d_tmp) cudaFree(d_tmp);
+      if (ring[i]) cudaFreeAsync(ring[i], s);
+    if (W) cudaFreeAsync(W, s);
+    if (d_alpha) cudaFreeAsync(d_alpha, s);
+    if (d_bet) cudaFreeAsync(d_bet, s);
+    if (d_tmp) cudaFreeAsync(d_tmp, s);
     if (h_alpha) cudaFreeHost(h_alpha);
     if (h_bet) cudaFreeHost(h_bet);
     for (auto e : spmv_ev) cudaEventDestroy(e);
@@ -656,12 +656,14 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
       return rc_;             \
     }                         \
   } while (0)
-  for (int i = 0; i < S1; i++) SOLVE_CUDA(cudaMalloc(&ring[i], vbytes));
-  SOLVE_CUDA(cudaMalloc(&W, vbytes));
-  if (fold) SOLVE_CUDA(cudaMallocAsync(&Tf, vbytes, s));
-  SOLVE_CUDA(cudaMalloc(&d_alpha, sizeof(double) * (A.imax + 1)));
-  SOLVE_CUDA(cudaMalloc(&d_bet, sizeof(double) * (A.imax + 2)));
-  SOLVE_CUDA(cudaMalloc(&d_tmp, sizeof(double) * 4));
+  // per-solve buffers from the solver's pool (memory kept between solves)
+  const int dev = c.device;
+  for (int i = 0; i < S1; i++) SOLVE_CUDA(solver_alloc(dev, &ring[i], vbytes, s));
+  SOLVE_CUDA(solver_alloc(dev, &W, vbytes, s));
+  if (fold) SOLVE_CUDA(solver_alloc(dev, &Tf, vbytes, s));
+  SOLVE_CUDA(solver_alloc(dev, &d_alpha, sizeof(double) * (A.imax + 1), s));
+  SOLVE_CUDA(solver_alloc(dev, &d_bet, sizeof(double) * (A.imax + 2), s));
+  SOLVE_CUDA(solver_alloc(dev, &d_tmp, sizeof(double) * 4, s));
   SOLVE_CUDA(cudaMallocHost(&h_alpha, sizeof(double) * (A.imax + 2) * (kAhead + 1)));
   SOLVE_CUDA(cudaMallocHost(&h_bet, sizeof(double) * (A.imax + 2) * (kAhead + 1)));
   Timers tm;
@@ -671,7 +673,7 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
   cudaEventCreate(&tm.t3);
 
   if (pen) {
-    SOLVE_CUDA(cudaMallocAsync(&r0_pen, ebytes, s));
+    SOLVE_CUDA(solver_alloc(dev, &r0_pen, ebytes, s));
     SOLVE_RC(pen_permute<double2>(c, reinterpret_cast<const double2 *>(r0_dev),
                                   reinterpret_cast<double2 *>(r0_pen), true, s));
     r0_dev = r0_pen;
@@ -790,13 +792,14 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
     if (!ck_budget_read) {
       size_t fre = 0, tot = 0;
       cudaMemGetInfo(&fre, &tot);
+      fre += solver_pool_spare(dev);  // the pool's memory kept from earlier solves
       ck_budget = fre > ring_need ? fre - ring_need : 0;
       ck_budget_read = true;
     }
     const size_t need = (it > 0 ? 2 : 1) * vbytes;
     VT *a = nullptr, *b = nullptr;
-    bool ok = ck_budget > 2 * vbytes && cudaMallocAsync(&a, vbytes, s) == cudaSuccess;
-    if (ok && it > 0) ok = cudaMallocAsync(&b, vbytes, s) == cudaSuccess;
+    bool ok = ck_budget > 2 * vbytes && solver_alloc(dev, &a, vbytes, s) == cudaSuccess;
+    if (ok && it > 0) ok = solver_alloc(dev, &b, vbytes, s) == cudaSuccess;
     if (ok) ck_budget -= need;
     if (!ok) {
       cudaGetLastError();  // a failed allocation is not an error of the solve
@@ -943,7 +946,7 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
   double *Vacc = V_dev;
   auto vec_target = [&]() -> int {
     if (pen) {
-      if (cudaMallocAsync(&V_pen, ebytes * nvec, s) != cudaSuccess) return set_error(TBGPU_E_NOMEM);
+      if (solver_alloc(dev, &V_pen, ebytes * nvec, s) != cudaSuccess) return set_error(TBGPU_E_NOMEM);
       Vacc = V_pen;
     }
     return cudaMemsetAsync(Vacc, 0, ebytes * nvec, s) == cudaSuccess ? TBGPU_OK
@@ -993,8 +996,8 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
     const int K = kRegenRows / P;  // accumulation rows per column
     const int R = K + 2;           // ring per column: K inputs, the previous r, the output
     rr.assign(size_t(P) * R, nullptr);
-    for (auto &q : rr) SOLVE_CUDA(cudaMallocAsync(&q, vbytes, s));
-    SOLVE_CUDA(cudaMallocAsync(&d_diff, sizeof(unsigned long long) * std::max(nseg, 1), s));
+    for (auto &q : rr) SOLVE_CUDA(solver_alloc(dev, &q, vbytes, s));
+    SOLVE_CUDA(solver_alloc(dev, &d_diff, sizeof(unsigned long long) * std::max(nseg, 1), s));
     SOLVE_CUDA(cudaMemsetAsync(d_diff, 0, sizeof(unsigned long long) * std::max(nseg, 1), s));
     SOLVE_RC(vec_target());
     cudaEventRecord(tm.t2, s);
@@ -1095,10 +1098,11 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
     // chunk size limited by free memory
     size_t fre = 0, tot = 0;
     cudaMemGetInfo(&fre, &tot);
+    fre += solver_pool_spare(dev);
     int K = kMaxChunk;
     while (K > 2 && size_t(K + 1 - S1) * vbytes + (256ull << 20) > fre) K /= 2;
     const int S2 = K + 1;
-    for (int i = S1; i < S2; i++) SOLVE_CUDA(cudaMalloc(&ring[i], vbytes));
+    for (int i = S1; i < S2; i++) SOLVE_CUDA(solver_alloc(dev, &ring[i], vbytes, s));
     SOLVE_RC(vec_target());
     cudaEventRecord(tm.t2, s);
     SOLVE_RC(start(d_bet));
@@ -1165,6 +1169,9 @@ static int solve_t(Ctx &c, const SolveArgs &A, const double *r0_dev, double *val
   cudaEventDestroy(tm.t2);
   cudaEventDestroy(tm.t3);
   cleanup();
+  // the solve returns with its work done (the buffers go back to the pool
+  // in stream order)
+  if (cudaStreamSynchronize(s) != cudaSuccess) return set_error(TBGPU_E_CUDA);
 #undef SOLVE_CUDA
 #undef SOLVE_RC
   return ne;

@@ -166,6 +166,19 @@ int set_error(int code);
 // out, a bad species id): read after the context's stream drained, cleared,
 // and returned as the call's status (TBGPU_OK when clear).
 int take_status(Ctx &c);
+// the solver's per-device memory pool (memory kept mapped between solves;
+// nullptr if it could not be made) and its reserved but unused bytes
+cudaMemPool_t solver_pool(int device);
+size_t solver_pool_spare(int device);
+template <typename T>
+inline cudaError_t solver_alloc(int device, T **p, size_t bytes, cudaStream_t s) {
+  cudaMemPool_t pool = solver_pool(device);
+  void *q = nullptr;
+  const cudaError_t e =
+      pool ? cudaMallocFromPoolAsync(&q, bytes, pool, s) : cudaMallocAsync(&q, bytes, s);
+  *p = static_cast<T *>(q);
+  return e;
+}
 
 // Dynamic shared memory above 48 KB is allowed per kernel and per device
 // context.  `done` (one per kernel instance) records the devices already

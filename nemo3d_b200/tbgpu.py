@@ -87,6 +87,7 @@ def _lib():
         L.tbgpu_block_dots_dev.argtypes = [vp, ip, vp, vp, C.c_long, vp]
         L.tbgpu_set_block_dots.argtypes = [vp, ip]
         L.tbgpu_set_mixed_acceptance.argtypes = [vp, dp]
+        L.tbgpu_release_solver_memory.argtypes = []
         L.tbgpu_eigensolve_blk_lanczos.argtypes = [vp, ip, ip, ip, ip, ip, dp, dp, dp, dp, dp,
                                                    ip, ip, vp, vp, vp, vp, vp, vp, ip]
         L.tbgpu_ctx_create.argtypes = [C.POINTER(_Geom), C.POINTER(_Model), C.POINTER(vp)]
@@ -127,6 +128,14 @@ def _lib():
 
 def _p(a):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def release_solver_memory():
+    """Return the device memory the solver's pools keep between solves
+    (tbgpu_release_solver_memory); call once the solves have finished."""
+    rc = _lib().tbgpu_release_solver_memory()
+    if rc:
+        raise TbgpuError(rc, "tbgpu_release_solver_memory")
 
 
 def write_eigenvalues(path: str, mode: str, k, E):
