@@ -370,45 +370,36 @@ int tbgpu_eigensolve_lanczos(tbgpu_ctx *ctx, int ConvCheckStartIter, int ConvChe
   Ctx &c = *C(ctx);
   if (!c.built) return set_error(TBGPU_E_STATE);
   const size_t bytes = sizeof(double) * 2 * size_t(c.natoms) * c.nb;
+  // the device copies come from the solver's pool (kept mapped between
+  // solves) and go back to it in stream order
+  cudaStream_t s = c.stream;
   double *r0 = nullptr, *V = nullptr;
-  if (!r_0) {  // the vector set by tbgpu_set_start_vector
-    int nv = (vectors && max_vectors > 0) ? max_vectors : 0;
-    if (nv && cudaMalloc(&V, bytes * nv) != cudaSuccess) return set_error(TBGPU_E_NOMEM);
-    int ne = tbgpu_eigensolve_lanczos_dev(ctx, ConvCheckStartIter, ConvCheckSkipRate, imax,
-                                          requested1, requested2, emin1, emax1, emin2, emax2,
-                                          tolerance, nullptr, values, conv_iterations, iterations,
-                                          V, nv);
-    if (ne > 0 && nv) {
-      const int got = ne < nv ? ne : nv;
-      if (cudaMemcpyAsync(vectors, V, bytes * got, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
-          cudaStreamSynchronize(c.stream) != cudaSuccess)
-        ne = set_error(TBGPU_E_CUDA);
-    }
-    if (V) cudaFree(V);
-    return ne;
-  }
-  if (cudaMalloc(&r0, bytes) != cudaSuccess) return set_error(TBGPU_E_NOMEM);
-  int nv = (vectors && max_vectors > 0) ? max_vectors : 0;
-  if (nv && cudaMalloc(&V, bytes * nv) != cudaSuccess) {
-    cudaFree(r0);
+  const int nv = (vectors && max_vectors > 0) ? max_vectors : 0;
+  if (nv && solver_alloc(c.device, &V, bytes * nv, s) != cudaSuccess) {
+    cudaGetLastError();
     return set_error(TBGPU_E_NOMEM);
   }
-  int rc = TBGPU_OK;
-  if (cudaMemcpyAsync(r0, r_0, bytes, cudaMemcpyHostToDevice, c.stream) != cudaSuccess)
-    rc = set_error(TBGPU_E_CUDA);
-  int ne = rc;
-  if (rc == TBGPU_OK)
+  if (r_0 && solver_alloc(c.device, &r0, bytes, s) != cudaSuccess) {
+    cudaGetLastError();
+    if (V) cudaFreeAsync(V, s);
+    return set_error(TBGPU_E_NOMEM);
+  }
+  int ne = TBGPU_OK;
+  if (r_0 && cudaMemcpyAsync(r0, r_0, bytes, cudaMemcpyHostToDevice, s) != cudaSuccess)
+    ne = set_error(TBGPU_E_CUDA);
+  // without r_0: the vector set by tbgpu_set_start_vector
+  if (ne == TBGPU_OK)
     ne = tbgpu_eigensolve_lanczos_dev(ctx, ConvCheckStartIter, ConvCheckSkipRate, imax,
                                       requested1, requested2, emin1, emax1, emin2, emax2,
                                       tolerance, r0, values, conv_iterations, iterations, V, nv);
   if (ne > 0 && nv) {
     const int got = ne < nv ? ne : nv;
-    if (cudaMemcpyAsync(vectors, V, bytes * got, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
-        cudaStreamSynchronize(c.stream) != cudaSuccess)
+    if (cudaMemcpyAsync(vectors, V, bytes * got, cudaMemcpyDeviceToHost, s) != cudaSuccess)
       ne = set_error(TBGPU_E_CUDA);
   }
-  cudaFree(r0);
-  if (V) cudaFree(V);
+  if (r0) cudaFreeAsync(r0, s);
+  if (V) cudaFreeAsync(V, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess && ne >= 0) ne = set_error(TBGPU_E_CUDA);
   return ne;
 }
 

@@ -342,7 +342,10 @@ class Hamiltonian:
         vals = np.zeros(imax)
         cit = np.zeros(imax, np.int32)
         its = np.zeros(1, np.int32)
-        V = np.zeros((vectors, 2 * self.n)) if vectors else None
+        # the library writes interleaved (re, im) doubles: the layout of
+        # complex128, so the result is a view of this array (no zero fill,
+        # no second copy of what can be gigabytes)
+        V = np.empty((vectors, 2 * self.n)) if vectors else None
         ne = _lib().tbgpu_eigensolve_lanczos(
             self._ctx, ConvCheckStartIter, ConvCheckSkipRate, imax, requested1, requested2,
             emin1, emax1, emin2, emax2, tolerance, _p(r0), _p(vals), _p(cit), _p(its),
@@ -353,8 +356,7 @@ class Hamiltonian:
                    iterations=int(its[0]))
         if vectors:
             k = min(ne, vectors)
-            v = V[:k].reshape(k, self.n, 2)
-            out["vectors"] = v[..., 0] + 1j * v[..., 1]
+            out["vectors"] = V[:k].view(np.complex128)
         return out
 
     def eigensolve_lanczos_batched(self, r_0, dot_cells, emin1, emax1, emin2, emax2,
@@ -391,8 +393,8 @@ class Hamiltonian:
         out = dict(values=[vals[d * vs:d * vs + found[d]].copy() for d in range(nd)],
                    iterations=its.copy())
         if vectors:
-            v = V.cpu().numpy().reshape(vectors, self.n, 2)
-            out["vectors"] = v[..., 0] + 1j * v[..., 1]
+            out["vectors"] = np.ascontiguousarray(V.cpu().numpy()).reshape(
+                vectors, 2 * self.n).view(np.complex128)
         return out
 
     def eigensolve_lanczos_dev(self, r0_ptr: int, vectors_ptr: int = 0, max_vectors: int = 0,
@@ -463,8 +465,7 @@ class Hamiltonian:
                "iterations": it.value}
         if nv > 0:
             k = min(rc, nv)
-            v = vec[:2 * self.n * k].reshape(k, self.n, 2)
-            out["vectors"] = v[..., 0] + 1j * v[..., 1]
+            out["vectors"] = vec[:2 * self.n * k].reshape(k, 2 * self.n).view(np.complex128)
         return out
 
     def write_eigenvector(self, path: str, vec, crystal_structure: int = 2):
