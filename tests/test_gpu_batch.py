@@ -6,7 +6,15 @@ iteration count (to one check interval) and the eigenvectors
 segment of the start vector; the
 mixed-precision batch refines each dot's states to within 1e-6 eV of the
 FP64 batch, the error printed per state; packings whose dots touch, and
-boundaries outside the grid, are refused.
+boundaries outside the grid, are refused; on a sample of three dots, each
+dot of the batch against the oracle's Lanczos (the restatement pinned to the
+reference's compiled lanczos.c) from the same start vector: every value the
+batch returns is one of the oracle's within 1e-6 eV (or the reverse), each
+window holds its requested count, iterations within four check intervals.
+The batch forms alpha from the unnormalised product, so its tridiagonal
+matrix differs from the oracle's by rounding, and a value whose eigenvector
+tail sits at the tolerance can be accepted at one check in one and not the
+other: the counts beyond the requested ones may differ.
 """
 import numpy as np
 import pytest
@@ -91,6 +99,39 @@ def test_mixed_batch_per_state():
         print(opts, "mixed batch error per dot (eV):", err, "residual:", resid)
         assert err.max() < 1e-6
         assert resid.max() < 1e-3
+
+
+def test_batch_matches_oracle():
+    import oracle
+    from nemo3d_b200.tbgpu import Hamiltonian
+    dots = [workloads.alloy_dot(n, x, seed=20 + i)
+            for i, (n, x) in enumerate(zip([300, 500, 900], [0.5, 0.8, 0.6]))]
+    mats = [materials.MATERIALS[m] for m in SPS]
+    packed, cells = workloads.pack_dots(dots)
+    gb = Hamiltonian(packed, "sp3s*_so", mats)
+    singles = [Hamiltonian(d, "sp3s*_so", mats) for d in dots]
+    starts = [workloads.random_start(g.n, seed=30 + i) for i, g in enumerate(singles)]
+    res = gb.eigensolve_lanczos_batched(np.concatenate(starts), cells, **_windows(len(dots)),
+                                        **KW)
+    for d, (dot, st0) in enumerate(zip(dots, starts)):
+        o = oracle.OracleHamiltonian(dot, 5, 2, mats)
+        ref = o.lanczos(st0, imax=KW["imax"], req=(KW["requested1"], KW["requested2"]),
+                        erange1=(-0.8, 0.4), erange2=(1.0, 3.5), tol=KW["tolerance"],
+                        conv_start=KW["ConvCheckStartIter"], conv_skip=KW["ConvCheckSkipRate"])
+        vb, vr = np.sort(res["values"][d]), np.sort(ref["evals"])
+        print("dot", d, "batch", res["iterations"][d], vb, "oracle", ref["iterations"], vr)
+        # these small alloy dots have closely spaced levels whose acceptance
+        # flips between neighbouring checks with rounding (measured: the same
+        # dot alone on the GPU 1301, the oracle 1251, the batch 1401)
+        assert abs(res["iterations"][d] - ref["iterations"]) <= 4 * KW["ConvCheckSkipRate"]
+        assert len(vb) >= 2 and len(vr) >= 2
+        # a borderline check may accept one value more or less: every value
+        # of the shorter set is in the longer one
+        short, long_ = (vb, vr) if len(vb) <= len(vr) else (vr, vb)
+        for v in short:
+            assert np.abs(long_ - v).min() < 1e-6, (d, v)
+        # each window holds at least its requested count
+        assert np.sum(vb <= 0.4) >= KW["requested1"] and np.sum(vb > 1.0) >= KW["requested2"]
 
 
 def test_batch_refusals():
