@@ -67,6 +67,10 @@ BYTES_PER_ATOM = {64: 2504, 32: 1256}
 # and scaled by atoms: the float lane kernel 488.6 MB, the FP64 default
 # kernel 3054 B/atom at full size.
 NCU_TRAFFIC_PER_ATOM = {32: 1272, 64: 3054}
+# one complex vector per atom (20 entries: FP64 320 B, complex float 160 B) and
+# the stored blocks + on-site records + neighbour columns per atom (B_H)
+VEC_PER_ATOM = {64: 320, 32: 160}
+H_PER_ATOM = {64: 1864, 32: 936}
 
 # band-edge windows of the dome: 4 highest hole and 4 lowest electron states
 # (Erange_vb / Erange_cb of the reference's Lanczos deck)
@@ -278,6 +282,17 @@ def max_over_ranks(value, dist, device):
     return float(t.item())
 
 
+def per_iteration(bits, natoms, stats, res):
+    its = max(int(res["iterations"]), 1)
+    ms = stats["solve_ms"] / its
+    alg = (BYTES_PER_ATOM[bits] + VEC_PER_ATOM[bits]) * natoms
+    moved = (H_PER_ATOM[bits] + 6 * VEC_PER_ATOM[bits]) * natoms
+    pk = peaks()[0]["hbm_gbs"]
+    return {"ms": ms, "algorithmic_gb": alg / 1e9, "moved_gb": moved / 1e9,
+            "algorithmic_frac": alg / (ms * 1e-3) / 1e9 / pk,
+            "moved_frac": moved / (ms * 1e-3) / 1e9 / pk}
+
+
 def _match_states(a, b):
     """Per-state |a_i - b_j| pairing each value of a with the nearest of b."""
     b = np.asarray(b)
@@ -448,6 +463,12 @@ def run_ours(args, rank, world, local_rank):
                "vectors_ms": last["vectors_ms"], "refine_ms": last["refine_ms"],
                "vec_segments": last["vec_segments"], "vec_mismatch": last["vec_mismatch"],
                "hx_avg_ms": spmv_ms,
+               # one first-pass iteration: the algorithmic bytes (B_SpMV + one
+               # vector read, the recurrence's minimum) and the bytes this
+               # design moves (B_H + 6 vector passes: the product's x and y,
+               # the update's three reads and one write), over the measured
+               # time per iteration (first pass / iterations)
+               "per_iteration": per_iteration(bits, natoms, last, res),
                "update_avg_ms": last["update_ms"] / max(last["spmv_launches"], 1),
                "host_check_ms": last["check_ms"], "host_wait_ms": last["wait_ms"],
                "residual_per_state_ev": resid, "tolerance": solve_kw["tolerance"]}
