@@ -104,15 +104,37 @@ __global__ void __launch_bounds__(kRedThreads)
   const double iq = 1.0 / bprev;
   const double ip = it > 0 ? 1.0 / bet[it - 1] : 0.0;
   double s = 0.0;
-  for (long j = blockIdx.x * (long)blockDim.x + threadIdx.x; j < n2;
-       j += (long)gridDim.x * blockDim.x) {
-    const double2 wv = widen(w[j]), cv = widen(rc[j]);
-    const double2 pv = it > 0 ? widen(rp[j]) : make_double2(0.0, 0.0);
-    const double2 rr = lanczos_update_entry(wv, cv, pv, al, bprev, iq, ip);
+  auto entry = [&](const VT wj, const VT cj, const VT pj) {
+    const double2 pv = it > 0 ? widen(pj) : make_double2(0.0, 0.0);
+    const double2 rr = lanczos_update_entry(widen(wj), widen(cj), pv, al, bprev, iq, ip);
     const VT r = narrow<VT>(rr.x, rr.y);
-    rout[j] = r;
     const double2 rw = widen(r);  // the norm of the vector as stored
     s += rw.x * rw.x + rw.y * rw.y;
+    return r;
+  };
+  const long tid = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const long nth = (long)gridDim.x * blockDim.x;
+  if constexpr (sizeof(VT) == sizeof(float2)) {
+    // complex floats two at a time: 16-byte loads and stores (the vectors
+    // start on 16-byte boundaries); each entry computes as one at a time
+    const long n4 = n2 / 2;
+    const float4 *w4 = reinterpret_cast<const float4 *>(w);
+    const float4 *c4 = reinterpret_cast<const float4 *>(rc);
+    const float4 *p4 = reinterpret_cast<const float4 *>(rp);
+    float4 *o4 = reinterpret_cast<float4 *>(rout);
+    for (long j = tid; j < n4; j += nth) {
+      const float4 a = w4[j], c = c4[j];
+      const float4 p = it > 0 ? p4[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+      const VT r0 = entry(VT{a.x, a.y}, VT{c.x, c.y}, VT{p.x, p.y});
+      const VT r1 = entry(VT{a.z, a.w}, VT{c.z, c.w}, VT{p.z, p.w});
+      o4[j] = make_float4(r0.x, r0.y, r1.x, r1.y);
+    }
+    if ((n2 & 1) && tid == 0) {  // an odd length's last entry
+      const long j = n2 - 1;
+      rout[j] = entry(w[j], rc[j], it > 0 ? rp[j] : VT{});
+    }
+  } else {
+    for (long j = tid; j < n2; j += nth) rout[j] = entry(w[j], rc[j], it > 0 ? rp[j] : VT{});
   }
   grid_reduce<kRedThreads>(s, partial, counter, bet, it + 1, true);
 }
