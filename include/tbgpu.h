@@ -411,16 +411,20 @@ int tbgpu_hx_dot_noalloc(tbgpu_ctx *ctx, double shift, const double *x_dev,
  * in batched solves, else as 0), 7 = variant 6 with each warp's next bond's
  * block rows double-buffered in shared memory by 16-byte cp.async copies
  * while it computes the current one (32-bit store, spin-orbit models, closed
- * z boundary and nz a multiple of 16; else as 6).  Variants 0, 2, 3 and 4
- * give the same y bit for bit, and so do 6 and 7; 1, 5 and 6 sum in their
- * own orders (equal to rounding). */
+ * z boundary and nz a multiple of 16; else as 6), 8 and 9 = the
+ * lane-gather kernel of variant 1 with 4 and 2 warps per block instead of
+ * 8 (the block size sets each block's staging array and so the blocks and
+ * warps an SM holds), for every model.  Variants 0, 2, 3 and 4 give the same
+ * y bit for bit, and so do 6 and 7, and 1, 8 and 9; 1, 5 and 6 sum in their
+ * own orders (equal to rounding).  For 5-orbital models and Bloch phases,
+ * 0 to 7 all run the lane-gather kernel with 8 warps per block. */
 int tbgpu_set_spmv_variant(tbgpu_ctx *ctx, int variant);
 
 /* Autotuner: times the H*x variants that are distinct kernels for the built
- * context (0 to 6 for the 10-orbital models with the 64-bit store at the
- * Gamma point, 0, 1, 5, 6 and, where it applies, 7 with the 32-bit store,
- * only 0 for 5-orbital models,
- * Bloch phases and recompute storage), reps launches each with the fused
+ * context (0 to 6, 8 and 9 for the 10-orbital models with the 64-bit store
+ * at the Gamma point; 0, 1, 5, 6, 8, 9 and, where it applies, 7 with the
+ * 32-bit store; 0, 8 and 9 for 5-orbital models and Bloch phases; only 0
+ * with recompute storage), reps launches each with the fused
  * Lanczos dot after two untimed ones (CUDA events on the context stream;
  * two temporary device vectors), selects the fastest (ties: the lower
  * number) and returns it with its time per launch.  Synchronous. */

@@ -533,7 +533,7 @@ int tbgpu_export_hamiltonian(const tbgpu_ctx *ctx, double *onsite, double *block
 }
 
 int tbgpu_set_spmv_variant(tbgpu_ctx *ctx, int variant) {
-  if (!ctx || variant < 0 || variant > 7) return set_error(TBGPU_E_ARG);
+  if (!ctx || variant < 0 || variant > 9) return set_error(TBGPU_E_ARG);
   C(ctx)->spmv_variant = variant;
   return TBGPU_OK;
 }
@@ -544,24 +544,26 @@ int tbgpu_set_spmv_variant(tbgpu_ctx *ctx, int variant) {
 // kernel with the float store; one kernel otherwise (5-orbital models, Bloch
 // phases, recompute storage).
 static int distinct_variants(const Ctx &c, int *v) {
-  if (c.norb != 10 || c.bloch || c.recompute) {
+  if (c.recompute) {
     v[0] = 0;
     return 1;
   }
-  if (c.ham_fp32) {
-    v[0] = 0;
-    v[1] = 1;
-    v[2] = 5;
-    v[3] = 6;
+  int n = 0;
+  if (c.norb != 10 || c.bloch) {  // the lane-gather kernel at three block sizes
+    v[n++] = 0;
+  } else if (c.ham_fp32) {
+    v[n++] = 0;
+    v[n++] = 1;
+    v[n++] = 5;
+    v[n++] = 6;
     // the staged pencil kernel where it applies (otherwise 7 runs 6's)
-    if (c.nspin == 2 && c.nz % 16 == 0 && !c.periodic[2]) {
-      v[4] = 7;
-      return 5;
-    }
-    return 4;
+    if (c.nspin == 2 && c.nz % 16 == 0 && !c.periodic[2]) v[n++] = 7;
+  } else {
+    for (int i = 0; i < 7; i++) v[n++] = i;
   }
-  for (int i = 0; i < 7; i++) v[i] = i;
-  return 7;
+  v[n++] = 8;
+  v[n++] = 9;
+  return n;
 }
 
 // Times the context's distinct H*x variants (the product with the fused
@@ -587,7 +589,7 @@ int tbgpu_autotune_spmv(tbgpu_ctx *ctx, int reps, int *variant_out, double *ms_o
              cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
     rc = TBGPU_E_CUDA;
   }
-  int cand[7];
+  int cand[12];
   const int ncand = distinct_variants(c, cand);
   for (int ci = 0; ci < ncand && rc == TBGPU_OK; ci++) {
     const int v = cand[ci];

@@ -188,10 +188,39 @@ __global__ void __launch_bounds__(WPB * 32)
 
 constexpr int kWPB = 8;
 
+// warps per block of the lane-gather kernel: 8 (variants 0 and 1), 4
+// (variant 8) or 2 (variant 9).  The block size sets each block's staging
+// array (warps x atoms per warp x 5 segments) and so how many blocks and
+// warps an SM holds; every atom computes the same either way.
+inline int lane_gather_wpb(const Ctx &c) {
+  return c.spmv_variant == 8 ? 4 : c.spmv_variant == 9 ? 2 : kWPB;
+}
+
+template <int NORB, int NSPIN, typename HT, typename VT = double2, int WPB = kWPB>
+static int launch_ht_w(Ctx &c, const void *x, void *y, double shift,
+                       const double *xnorm, int xidx, double *alpha_out, int aidx,
+                       cudaStream_t s);
+
 template <int NORB, int NSPIN, typename HT, typename VT = double2>
 static int launch_ht(Ctx &c, const void *x, void *y, double shift,
                      const double *xnorm, int xidx, double *alpha_out, int aidx,
                      cudaStream_t s) {
+  switch (lane_gather_wpb(c)) {
+    case 4:
+      return launch_ht_w<NORB, NSPIN, HT, VT, 4>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
+    case 2:
+      return launch_ht_w<NORB, NSPIN, HT, VT, 2>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
+    default:
+      return launch_ht_w<NORB, NSPIN, HT, VT, kWPB>(c, x, y, shift, xnorm, xidx, alpha_out, aidx,
+                                                   s);
+  }
+}
+
+template <int NORB, int NSPIN, typename HT, typename VT, int WPB>
+static int launch_ht_w(Ctx &c, const void *x, void *y, double shift,
+                       const double *xnorm, int xidx, double *alpha_out, int aidx,
+                       cudaStream_t s) {
+  constexpr int kWPB = WPB;  // this launch's block size
   constexpr int APW = 32 / NORB;
   const long per_block = long(kWPB) * APW;
   const unsigned grid = unsigned((c.natoms + per_block - 1) / per_block);
@@ -243,7 +272,8 @@ int launch_spmv(Ctx &c, const double *x, double *y, double shift, const double *
     return launch_spmv_lane(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
   if (c.norb == 10 && c.spmv_variant == 3 && !c.bloch)
     return launch_spmv_tile(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
-  if (c.norb == 10 && c.spmv_variant != 1 && !c.bloch)
+  if (c.norb == 10 && c.spmv_variant != 1 && c.spmv_variant != 8 && c.spmv_variant != 9 &&
+      !c.bloch)
     return launch_spmv_async(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
   if (c.norb == 10 && c.nspin == 2) return launch_t<10, 2>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);
   if (c.norb == 10 && c.nspin == 1) return launch_t<10, 1>(c, x, y, shift, xnorm, xidx, alpha_out, aidx, s);

@@ -491,7 +491,8 @@ class Hamiltonian:
         """0: warp-staged cp.async kernel (default, 10 orbitals); 1: lane-gather; 2: 2-stage;
         3: two-cell units; 4: all cp.async; 5: lane per (atom, spin); 6: the same lanes
         on the pencil-interleaved layout; 7: 6 with block rows double-buffered in
-        shared memory (32-bit store, spin-orbit, closed z, nz a multiple of 16)."""
+        shared memory (32-bit store, spin-orbit, closed z, nz a multiple of 16); 8, 9: the
+        lane-gather kernel of variant 1 with 4 and 2 warps per block (every model)."""
         rc = _lib().tbgpu_set_spmv_variant(self._ctx, int(variant))
         if rc:
             raise TbgpuError(rc, "tbgpu_set_spmv_variant")

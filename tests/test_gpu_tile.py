@@ -137,25 +137,63 @@ def test_autotune_selects_a_variant_with_the_same_product():
     g.set_spmv_variant(0)
     y0 = g.matvect_mult(x, 0.3)
     v, ms = g.autotune_spmv(reps=5)
-    assert v in range(5) and ms > 0.0
+    assert v in (0, 1, 2, 3, 4, 5, 6, 8, 9) and ms > 0.0
     y = g.matvect_mult(x, 0.3)
-    if v == 1:  # the lane-gather kernel sums in its own order
+    if v in (1, 5, 6, 8, 9):  # kernels that sum in their own orders
         ons, blk = g.export_hamiltonian()
         assert np.abs(y - y0).max() <= 1e-13 * max(np.abs(ons).max(), np.abs(blk).max())
     else:
         np.testing.assert_array_equal(y, y0)
-    # a model with one H*x kernel: nothing to choose
+    # a 5-orbital model: the lane-gather kernel at 8, 4 or 2 warps per block,
+    # one product
     h, _ = _ham(STRUCTURES["dome_7x6x5"](), "sp3s*_so", fam="sps")
+    h.set_spmv_variant(0)
+    z0 = h.matvect_mult(x[:2 * h.n], 0.3)
     v, ms = h.autotune_spmv(reps=3)
-    assert v == 0 and ms > 0.0
+    assert v in (0, 8, 9) and ms > 0.0
+    np.testing.assert_array_equal(h.matvect_mult(x[:2 * h.n], 0.3), z0)
+
+
+@pytest.mark.parametrize("model,fam,bloch", [("sp3s*_so", "sps", False), ("sp3s*", "sps", False),
+                                             ("sp3d5s*_so", "spds", False),
+                                             ("sp3d5s*_so", "spds", True)])
+def test_lane_gather_block_sizes_same_product(model, fam, bloch):
+    """Variants 1, 8 and 9 (the lane-gather kernel with 8, 4 and 2 warps per
+    block) give y bit for bit, with and without Bloch phases; a Lanczos solve
+    on variant 9 finds the values of variant 1 to 1e-9 eV (the fused alpha
+    dot sums its block partials over another block count)."""
+    g, _ = _ham(STRUCTURES["periodic_3x4x3" if bloch else "dome_7x6x5"](), model, fam=fam)
+    if bloch:
+        g.set_bloch_k([0.11, -0.07, 0.05])
+    x = np.random.default_rng(5).uniform(-1, 1, 2 * g.n)
+    ys = []
+    for v in (1, 8, 9):
+        g.set_spmv_variant(v)
+        ys.append(g.matvect_mult(x, 0.2))
+    np.testing.assert_array_equal(ys[0], ys[1])
+    np.testing.assert_array_equal(ys[0], ys[2])
+    if bloch:
+        return
+    r0 = workloads.random_start(g.n, seed=0)
+    kw = dict(imax=3000, requested1=2, requested2=2, emin1=-0.6, emax1=0.4, emin2=1.0,
+              emax2=2.6, tolerance=1e-7)
+    g.set_spmv_variant(1)
+    a = g.eigensolve_lanczos(r0, **kw)
+    g.set_spmv_variant(9)
+    b = g.eigensolve_lanczos(r0, **kw)
+    assert len(a["values"]) > 0 and len(b["values"]) > 0
+    for u, w in ((a["values"], b["values"]), (b["values"], a["values"])):
+        assert max(np.abs(w - t).min() for t in u) < 1e-9
 
 
 def test_tile_variant_range():
     from nemo3d_b200.tbgpu import TbgpuError
     g, _ = _ham(STRUCTURES["dome_7x6x5"](), "sp3d5s*")
     g.set_spmv_variant(7)  # the staged pencil kernel (the pencil kernel where it does not apply)
+    g.set_spmv_variant(8)  # the lane-gather kernel with 4 and 2 warps per block
+    g.set_spmv_variant(9)
     with pytest.raises(TbgpuError):
-        g.set_spmv_variant(8)
+        g.set_spmv_variant(10)
     with pytest.raises(TbgpuError):
         g.set_spmv_variant(-1)
 
